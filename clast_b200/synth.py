@@ -1,0 +1,207 @@
+"""Seeded synthetic DNA workloads with the shapes of the benchmark configurations.
+
+There is no public dataset behind these workloads; every target and read set
+is generated from a fixed seed, so the same call gives the same bytes on any
+machine.  Shapes:
+
+* ``small``  -- one 1 Mbp target record of uniform ACGT with 0.1 % of bases in
+  N runs (geometric length, mean 10); 1,000 reads of 150 bp sampled uniformly
+  from it with 2 % substitutions and 0.5 % indel events (geometric length,
+  mean 2), half reverse-complemented, 5 % uniform random decoys.
+* ``medium`` -- 100 Mbp in 200 contigs with log-normal lengths (median 300 kbp),
+  10 % of bases in 500 repeat families of 300 bp - 6 kbp copied at 85-99 %
+  identity; 1,000,000 reads of 150 bp from the same error model.
+* ``uneven`` -- the medium target; 200,000 reads with log-uniform lengths in
+  50 bp - 10 kbp, per-read error rate uniform in 1-12 % (70 % substitutions,
+  30 % indels).
+
+Reads carry labels ``r<i>``; targets ``ctg<i>``.  Sizes scale with the
+arguments so tests can use small versions of each shape.
+"""
+from __future__ import annotations
+
+import dataclasses
+import numpy as np
+
+ACGT = np.frombuffer(b"ACGT", dtype=np.uint8)
+_COMP = np.zeros(256, dtype=np.uint8)
+_COMP[:] = ord("N")
+for a, b in (("A", "T"), ("C", "G"), ("G", "C"), ("T", "A")):
+    _COMP[ord(a)] = ord(b)
+
+
+def revcomp(seq: np.ndarray) -> np.ndarray:
+    """Reverse complement of an uint8 ASCII array (non-ACGT -> N)."""
+    return _COMP[seq[::-1]]
+
+
+@dataclasses.dataclass
+class SeqSet:
+    """Concatenated sequences: ``bases[offsets[i]:offsets[i+1]]`` is record i."""
+    labels: list
+    bases: np.ndarray      # uint8 ASCII, no separators
+    offsets: np.ndarray    # int64, len(labels)+1
+
+    def __len__(self):
+        return len(self.labels)
+
+    def seq(self, i: int) -> np.ndarray:
+        return self.bases[self.offsets[i]:self.offsets[i + 1]]
+
+    @property
+    def lengths(self) -> np.ndarray:
+        return np.diff(self.offsets)
+
+    def to_fasta(self, path: str, width: int = 60) -> None:
+        """Writes FASTA with ``width``-column sequence lines."""
+        with open(path, "wb") as f:
+            for i, lab in enumerate(self.labels):
+                s = self.seq(i).tobytes()
+                f.write(b">" + lab.encode() + b"\n")
+                for k in range(0, len(s), width):
+                    f.write(s[k:k + width] + b"\n")
+
+
+def _rand_bases(rng, n):
+    return ACGT[rng.integers(0, 4, size=n)]
+
+
+def make_target(rng, total_bp: int, n_contigs: int = 1, median: float | None = None,
+                n_frac: float = 0.001, n_run_mean: float = 10.0, repeat_frac: float = 0.0,
+                n_families: int = 0, fam_len=(300, 6000), fam_ident=(0.85, 0.99)) -> SeqSet:
+    """Random contigs (log-normal lengths when ``n_contigs > 1``) with N runs
+    and optional repeat families."""
+    if n_contigs == 1:
+        lens = np.array([total_bp], dtype=np.int64)
+    else:
+        mean = total_bp / n_contigs
+        med = median if median else mean * 0.6
+        sigma = float(np.sqrt(max(2.0 * np.log(mean / med), 1e-6)))
+        raw = rng.lognormal(np.log(med), sigma, size=n_contigs)
+        lens = np.maximum((raw / raw.sum() * total_bp).astype(np.int64), 1000)
+        lens[int(np.argmax(lens))] += total_bp - lens.sum()
+    bases = _rand_bases(rng, int(lens.sum()))
+    offsets = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    total = len(bases)
+    # repeat families: consensus copies at per-copy identity, substitutions only
+    if repeat_frac > 0 and n_families > 0:
+        budget = int(repeat_frac * total)
+        per_fam = budget // n_families
+        for _ in range(n_families):
+            flen = int(np.exp(rng.uniform(np.log(fam_len[0]), np.log(fam_len[1]))))
+            cons = _rand_bases(rng, flen)
+            ncopy = max(2, per_fam // flen)
+            for _ in range(ncopy):
+                ident = rng.uniform(*fam_ident)
+                copy = cons.copy()
+                mut = rng.random(flen) > ident
+                copy[mut] = _rand_bases(rng, int(mut.sum()))
+                c = int(rng.integers(0, len(lens)))
+                if lens[c] <= flen:
+                    continue
+                at = offsets[c] + int(rng.integers(0, lens[c] - flen))
+                bases[at:at + flen] = copy
+    # N runs
+    if n_frac > 0:
+        n_runs = int(n_frac * total / n_run_mean)
+        starts = rng.integers(0, total, size=n_runs)
+        runs = rng.geometric(1.0 / n_run_mean, size=n_runs)
+        for s, r in zip(starts, runs):
+            bases[s:s + r] = ord("N")
+    labels = ["ctg%d" % i for i in range(len(lens))]
+    return SeqSet(labels, bases, offsets)
+
+
+def _mutate(rng, src: np.ndarray, out_len: int, sub: float, indel: float, indel_mean: float) -> np.ndarray:
+    """Applies substitutions and indel events to ``src`` and returns the first
+    ``out_len`` bases of the mutated sequence (``src`` is long enough)."""
+    n = len(src)
+    ev = np.flatnonzero(rng.random(n) < indel)
+    if len(ev) == 0:
+        seq = src.copy()
+    else:
+        parts, prev = [], 0
+        for e in ev:
+            if e < prev:
+                continue
+            ln = int(rng.geometric(1.0 / indel_mean))
+            parts.append(src[prev:e])
+            if rng.random() < 0.5:   # insertion before e
+                parts.append(_rand_bases(rng, ln))
+                prev = e
+            else:                    # deletion of e .. e+ln-1
+                prev = e + ln
+        parts.append(src[prev:])
+        seq = np.concatenate(parts)
+    seq = seq[:out_len].copy()
+    m = rng.random(len(seq)) < sub
+    if m.any():
+        # a substitution always changes the base
+        cur = seq[m]
+        shift = rng.integers(1, 4, size=int(m.sum()))
+        idx = np.searchsorted(ACGT, cur)
+        valid = (idx < 4) & (ACGT[np.minimum(idx, 3)] == cur)
+        new = ACGT[(np.where(valid, idx, 0) + shift) % 4]
+        seq[m] = new
+    return seq
+
+
+def make_reads(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, indel=0.005,
+               indel_mean=2.0, rev_frac=0.5, decoy_frac=0.05, log_uniform=None,
+               err_range=None) -> SeqSet:
+    """Reads sampled uniformly from the target (by base), with errors,
+    reverse-complemented with probability ``rev_frac`` and replaced by random
+    decoys with probability ``decoy_frac``.  ``log_uniform=(lo, hi)`` draws
+    read lengths log-uniformly; ``err_range=(lo, hi)`` draws a per-read error
+    rate split 70/30 between substitutions and indels."""
+    tl = target.lengths
+    cum = np.concatenate([[0], np.cumsum(tl)])
+    seqs = []
+    for i in range(n_reads):
+        L = length if log_uniform is None else int(np.exp(rng.uniform(np.log(log_uniform[0]),
+                                                                     np.log(log_uniform[1]))))
+        s_rate, i_rate = sub, indel
+        if err_range is not None:
+            e = rng.uniform(*err_range)
+            s_rate, i_rate = 0.7 * e, 0.3 * e / indel_mean
+        if rng.random() < decoy_frac:
+            seqs.append(_rand_bases(rng, L))
+            continue
+        need = L + 8 * int(np.ceil(L * i_rate * indel_mean)) + 16
+        for _ in range(100):
+            g = int(rng.integers(0, cum[-1]))
+            c = int(np.searchsorted(cum, g, side="right") - 1)
+            if tl[c] >= need:
+                break
+        else:
+            c = int(np.argmax(tl))
+        start = int(rng.integers(0, tl[c] - need + 1))
+        src = target.bases[target.offsets[c] + start: target.offsets[c] + start + need]
+        r = _mutate(rng, src, L, s_rate, i_rate, indel_mean)
+        if rng.random() < rev_frac:
+            r = revcomp(r)
+        seqs.append(r)
+    lens = np.array([len(s) for s in seqs], dtype=np.int64)
+    offsets = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    bases = np.concatenate(seqs) if seqs else np.zeros(0, dtype=np.uint8)
+    return SeqSet(["r%d" % i for i in range(n_reads)], bases, offsets)
+
+
+def workload(name: str, seed: int = 0xC1A57, scale: float = 1.0):
+    """(target, reads) for a named shape; ``scale`` shrinks sizes for tests."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    if name == "small":
+        t = make_target(rng, int(1_000_000 * scale))
+        q = make_reads(rng, t, max(1, int(1000 * scale)))
+    elif name == "medium":
+        t = make_target(rng, int(100_000_000 * scale), n_contigs=max(1, int(200 * min(1.0, scale * 10))),
+                        median=300_000 * scale, repeat_frac=0.10, n_families=max(1, int(500 * scale)))
+        q = make_reads(rng, t, max(1, int(1_000_000 * scale)))
+    elif name == "uneven":
+        t = make_target(rng, int(100_000_000 * scale), n_contigs=max(1, int(200 * min(1.0, scale * 10))),
+                        median=300_000 * scale, repeat_frac=0.10, n_families=max(1, int(500 * scale)))
+        q = make_reads(rng, t, max(1, int(200_000 * scale)), log_uniform=(50, 10_000),
+                       err_range=(0.01, 0.12), decoy_frac=0.0)
+    else:
+        raise ValueError("unknown workload %r" % name)
+    return t, q
