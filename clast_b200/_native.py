@@ -1,0 +1,78 @@
+"""ctypes binding of libclast_b200.so (declarations: include/clast_gpu.h).
+
+The library is built in-tree (``clast_b200/libclast_b200.so``).  Loading it
+fails loudly when it is missing: there is no CPU fallback for the device path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libclast_b200.so")
+CLI_PATH = os.path.join(_HERE, "bin", "clast")
+
+
+class clast_params(C.Structure):
+    _fields_ = [("lmer", C.c_int32), ("stride", C.c_int32), ("cut_repeat", C.c_int32),
+                ("width", C.c_int32), ("gap", C.c_int32), ("local", C.c_int32),
+                ("cutoff", C.c_double), ("total_db", C.c_double), ("K", C.c_double),
+                ("lambda_", C.c_double)]
+
+
+class clast_hits(C.Structure):
+    _fields_ = [("n", C.c_int64)] + [(f, C.POINTER(C.c_int32)) for f in
+                                     ("t_id", "t_idx", "q_id", "q_idx", "t_len", "q_len", "match", "score")] + \
+               [("evalue", C.POINTER(C.c_double))]
+
+
+class clast_seqs(C.Structure):
+    _fields_ = [("n_seqs", C.c_int64), ("bases", C.c_char_p), ("offsets", C.POINTER(C.c_int64))]
+
+
+class clast_map_result(C.Structure):
+    _fields_ = [("n", C.c_int64), ("load_offsets", C.POINTER(C.c_int64))] + \
+               [(f, C.POINTER(C.c_int32)) for f in ("read", "strand", "t_load", "t_seq", "t_idx", "q_idx",
+                                                   "t_len", "q_len", "match", "score")] + \
+               [("evalue", C.POINTER(C.c_double))]
+
+
+# symbol name -> (restype, argtypes); the full export list of include/clast_gpu.h
+# plus the command-line entry of clast_host.h
+SIGNATURES = {
+    "clast_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "clast_ctx_destroy": (None, [C.c_void_p]),
+    "clast_last_error": (C.c_char_p, [C.c_void_p]),
+    "clast_index_build": (C.c_int, [C.c_void_p, C.POINTER(clast_params), C.c_void_p, C.c_int64, C.c_void_p,
+                                    C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "clast_index_free": (None, [C.c_void_p]),
+    "clast_search": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(clast_params), C.c_void_p, C.c_int64,
+                               C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(clast_hits)]),
+    "clast_hits_free": (None, [C.POINTER(clast_hits)]),
+    "clast_targets_create": (C.c_int, [C.c_void_p, C.POINTER(clast_params), C.c_int32, C.POINTER(clast_seqs),
+                                       C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "clast_targets_free": (None, [C.c_void_p]),
+    "clast_map": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(clast_params), C.c_int32, C.POINTER(clast_seqs),
+                            C.c_int32, C.c_void_p, C.POINTER(clast_map_result)]),
+    "clast_map_result_free": (None, [C.POINTER(clast_map_result)]),
+    "clast_last_map_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "clast_cli_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), C.c_char_p, C.c_int]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads the in-tree library once; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libclast_b200.so is not built (run __graft_entry__.build() or "
+                               "make -C clast_b200/csrc); the device path has no fallback")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib

@@ -1,0 +1,267 @@
+"""Host-side mirror of the reference's in-process interface for the search path.
+
+The reference (masayano/CLAST) drives its device work through four classes,
+constructed by its scheduler for every (target window, query window) pair
+(CHostSchedular.cu:141,169,187,196):
+
+=====================================  ==========================================
+reference                              here
+=====================================  ==========================================
+CHostSetting (CHostSetting.cuh:29-49)  :class:`Setting`
+CHostSeqList_target / _query           :class:`SeqList` (``add_targets`` / ``add_queries``)
+CDeviceHashTable(s, t, tb, te)         :meth:`Engine.hash_table`
+CDeviceHitList(s, h, q, tb, 2*qb)      :meth:`Engine.hit_list` (+ ``getResult``)
+CHostMapper/CHostSchedular/Holder      :meth:`Engine.targets` + :meth:`Engine.map`
+``clast`` command line                 :func:`run_clast`
+=====================================  ==========================================
+
+All device work goes through libclast_b200.so (include/clast_gpu.h); a call
+that fails raises :class:`ClastError` with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+
+import numpy as np
+
+from . import _native as N
+
+HIT_FIELDS = ("t_id", "t_idx", "q_id", "q_idx", "t_len", "q_len", "match", "score", "evalue")
+MAP_FIELDS = ("read", "strand", "t_load", "t_seq", "t_idx", "q_idx", "t_len", "q_len", "match", "score", "evalue")
+
+
+class ClastError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("clast error %d: %s" % (code, msg))
+        self.code = code
+
+
+@dataclasses.dataclass
+class Setting:
+    """The search settings of CHostSetting; defaults of common.hpp:12-43."""
+    lmer: int = 15
+    stride: int = 5
+    cut_repeat: int = 20
+    width: int = 100
+    gap: int = 8
+    local: int = 0
+    cutoff: float = 10.0
+    total_db: float = 0.0
+    K: float = 0.71
+    lambda_: float = 1.37
+
+    def c(self) -> N.clast_params:
+        return N.clast_params(self.lmer, self.stride, self.cut_repeat, self.width, self.gap, self.local,
+                              float(self.cutoff), float(self.total_db), float(self.K), float(self.lambda_))
+
+
+def _comp(seq: bytes) -> bytes:
+    """utilReverseSeq.cpp:3-19: reverse complement, non-ACGT -> N."""
+    table = bytes.maketrans(b"ACGT", b"TGCA")
+    out = seq[::-1].translate(table)
+    return bytes(c if c in b"ACGT" else ord("N") for c in out) if any(c not in b"ACGT" for c in out) else out
+
+
+class SeqList:
+    """CHostSeqList: concatenated sequences, each followed by its first l-1
+    bases (the joint, utilAddSequence.cu:6-47), with gateway prefix sums."""
+
+    def __init__(self, lmer: int):
+        self.l = lmer
+        self.labels: list = []
+        self.start_idx: list = []
+        self._parts: list = []
+        self.lengths: list = []
+        self.gateway: list = []
+
+    def _add(self, label, seq: bytes, start_idx=0):
+        j = seq[: self.l - 1]
+        j = j + b"N" * (self.l - 1 - len(j))
+        self._parts.append(seq + j)
+        self.labels.append(label)
+        self.start_idx.append(start_idx)
+        self.lengths.append(len(seq))
+        if not self.gateway:
+            self.gateway.append(0)
+        self.gateway.append(self.gateway[-1] + len(seq) + self.l - 1)
+
+    def add_targets(self, seqs, labels=None, start_idx=None):
+        """CHostSeqList_target::add (CHostSeqList_target.cu:8-33)."""
+        for i, s in enumerate(seqs):
+            self._add(labels[i] if labels else "t%d" % len(self.labels), bytes(s),
+                      start_idx[i] if start_idx else 0)
+        return self
+
+    def add_queries(self, seqs, labels=None):
+        """CHostSeqList_query::add: '+' strand then the reverse complement
+        (CHostSeqList_query.cu:11-54)."""
+        for i, s in enumerate(seqs):
+            lab = labels[i] if labels else "q%d" % (len(self.labels) // 2)
+            self._add(lab, bytes(s))
+            self._add(lab, _comp(bytes(s)))
+        return self
+
+    @property
+    def bases(self) -> bytes:
+        return b"".join(self._parts)
+
+    def window(self, b: int, e: int):
+        """getBaseArray/getGateway/getLengthArray(b, e) (CHostSeqList.cu:15-70):
+        the base array of sequences b..e-1, window-relative starts, lengths."""
+        g = self.gateway
+        bases = self.bases[g[b]:g[e]]
+        gw = np.asarray([g[i] - g[b] for i in range(b, e)], dtype=np.int32)
+        ln = np.asarray(self.lengths[b:e], dtype=np.int32)
+        return bases, gw, ln
+
+
+def _hits_to_numpy(h: N.clast_hits) -> dict:
+    n = int(h.n)
+    out = {}
+    for f in HIT_FIELDS:
+        ptr = getattr(h, f)
+        dt = np.float64 if f == "evalue" else np.int32
+        out[f] = np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+    return out
+
+
+class HashTable:
+    """Resident index of one target window (CDeviceHashTable)."""
+
+    def __init__(self, engine: "Engine", handle: int, t_begin: int):
+        self.engine = engine
+        self.handle = handle
+        self.t_begin = t_begin
+
+    def close(self):
+        if self.handle:
+            N.load().clast_index_free(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+
+class Targets:
+    """Every target window of every RAM load, resident in HBM."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def close(self):
+        if self.handle:
+            N.load().clast_targets_free(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+
+class Engine:
+    """One device context (clast_ctx_create)."""
+
+    def __init__(self, device: int = 0):
+        lib = N.load()
+        h = C.c_void_p()
+        rc = lib.clast_ctx_create(device, C.byref(h))
+        if rc != 0:
+            raise ClastError(rc, "cannot create a context on device %d" % device)
+        self._lib = lib
+        self.ctx = h
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self._lib.clast_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    __del__ = close
+
+    def _check(self, rc):
+        if rc != 0:
+            raise ClastError(rc, self._lib.clast_last_error(self.ctx).decode(errors="replace"))
+
+    # -- the reference seam ------------------------------------------------
+    def hash_table_window(self, s: Setting, bases: bytes, gateway, lengths, t_begin: int) -> HashTable:
+        gw = np.ascontiguousarray(gateway, dtype=np.int32)
+        ln = np.ascontiguousarray(lengths, dtype=np.int32)
+        out = C.c_void_p()
+        p = s.c()
+        self._check(self._lib.clast_index_build(self.ctx, C.byref(p), bases, len(bases), gw.ctypes.data,
+                                                ln.ctypes.data, len(gw), t_begin, C.byref(out)))
+        return HashTable(self, out.value, t_begin)
+
+    def hash_table(self, s: Setting, targets: SeqList, t_begin: int, t_end: int) -> HashTable:
+        """CDeviceHashTable(setting, targetList, t_begin, t_end)."""
+        bases, gw, ln = targets.window(t_begin, t_end)
+        return self.hash_table_window(s, bases, gw, ln, t_begin)
+
+    def hit_list_window(self, s: Setting, ix: HashTable, q_bases: bytes, q_gateway, q_lengths,
+                        q_begin: int) -> dict:
+        gw = np.ascontiguousarray(q_gateway, dtype=np.int32)
+        ln = np.ascontiguousarray(q_lengths, dtype=np.int32)
+        h = N.clast_hits()
+        p = s.c()
+        self._check(self._lib.clast_search(self.ctx, ix.handle, C.byref(p), q_bases, len(q_bases),
+                                           gw.ctypes.data, ln.ctypes.data, len(gw), q_begin, C.byref(h)))
+        try:
+            return _hits_to_numpy(h)
+        finally:
+            self._lib.clast_hits_free(C.byref(h))
+
+    def hit_list(self, s: Setting, ix: HashTable, queries: SeqList, q_begin: int, q_end: int) -> dict:
+        """CDeviceSeqList_query(s, q, q_begin, q_end) + CDeviceHitList(s, h, q,
+        t_begin, 2*q_begin) + getResult: the window's hits as numpy arrays
+        (t_id, t_idx, q_id, q_idx, t_len, q_len, match, score, evalue)."""
+        bases, gw, ln = queries.window(2 * q_begin, 2 * q_end)
+        return self.hit_list_window(s, ix, bases, gw, ln, 2 * q_begin)
+
+    # -- whole job ----------------------------------------------------------
+    def targets(self, s: Setting, bases: np.ndarray, offsets: np.ndarray, load_sizes, t_vram: int) -> Targets:
+        b = np.ascontiguousarray(bases, dtype=np.uint8)
+        o = np.ascontiguousarray(offsets, dtype=np.int64)
+        ls = np.ascontiguousarray(load_sizes, dtype=np.int64)
+        seqs = N.clast_seqs(len(o) - 1, C.cast(b.ctypes.data, C.c_char_p), o.ctypes.data_as(C.POINTER(C.c_int64)))
+        out = C.c_void_p()
+        p = s.c()
+        self._check(self._lib.clast_targets_create(self.ctx, C.byref(p), int(t_vram), C.byref(seqs), len(ls),
+                                                   ls.ctypes.data, C.byref(out)))
+        return Targets(out.value)
+
+    def map(self, s: Setting, targets: Targets, bases: np.ndarray, offsets: np.ndarray, load_sizes,
+            q_vram: int) -> dict:
+        """Every read against every target window; hits per query load in
+        the order CHostResultHolder::fixResult leaves them."""
+        b = np.ascontiguousarray(bases, dtype=np.uint8)
+        o = np.ascontiguousarray(offsets, dtype=np.int64)
+        ls = np.ascontiguousarray(load_sizes, dtype=np.int64)
+        seqs = N.clast_seqs(len(o) - 1, C.cast(b.ctypes.data, C.c_char_p), o.ctypes.data_as(C.POINTER(C.c_int64)))
+        r = N.clast_map_result()
+        p = s.c()
+        self._check(self._lib.clast_map(self.ctx, targets.handle, C.byref(p), int(q_vram), C.byref(seqs), len(ls),
+                                        ls.ctypes.data, C.byref(r)))
+        try:
+            n = int(r.n)
+            out = {}
+            for f in MAP_FIELDS:
+                dt = np.float64 if f == "evalue" else np.int32
+                out[f] = np.ctypeslib.as_array(getattr(r, f), shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+            out["load_offsets"] = np.ctypeslib.as_array(r.load_offsets, shape=(len(ls) + 1,)).copy()
+            return out
+        finally:
+            self._lib.clast_map_result_free(C.byref(r))
+
+    def last_map_stats(self):
+        ms = C.c_double()
+        k = C.c_int64()
+        self._check(self._lib.clast_last_map_stats(self.ctx, C.byref(ms), C.byref(k)))
+        return ms.value, k.value
+
+
+def run_clast(argv) -> tuple:
+    """The reference's command line (``clast -t T.fa -q Q.fa -o out.tsv ...``)
+    on the GPU.  Returns (exit code, error message)."""
+    lib = N.load()
+    args = ["clast"] + [str(a) for a in argv]
+    arr = (C.c_char_p * len(args))(*[a.encode() for a in args])
+    err = C.create_string_buffer(1024)
+    rc = lib.clast_cli_main(len(args), arr, err, len(err))
+    return rc, err.value.decode(errors="replace")

@@ -1,0 +1,700 @@
+// clast_engine.cu -- host orchestration of the device path and the C ABI
+// declared in include/clast_gpu.h.
+//
+// One context owns one CUDA stream and a scratch pool.  An index keeps its
+// target window resident in HBM (bases with joints, padded with 'N', plus the
+// key directory, unique keys, bucket ranges and resolved entries).  A search
+// runs the whole hit pipeline of CDeviceHitList (CDeviceHitList.cu:228-423)
+// for a batch of query windows with three host synchronisations (seed total,
+// hit total, result total).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/clast_gpu.h"
+#include "clast_device.cuh"
+#include "clast_kernels.cuh"
+#include "clast_workspace.h"
+
+using namespace clast;
+
+struct clast_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Workspace ws;
+  std::string err;
+  double last_ms = 0;
+  int64_t last_launches = 0;
+};
+
+namespace {
+
+template <class T>
+struct DevArray {  // owning device allocation
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (cudaMalloc(&p, (count ? count : 1) * sizeof(T)) != cudaSuccess) {
+      (void)cudaGetLastError();
+      p = nullptr;
+      throw std::bad_alloc();
+    }
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevArray() { release(); }
+};
+
+void check_params(const clast_params* p) {
+  if (!p) throw std::invalid_argument("params is null");
+  if (p->lmer < 1 || p->lmer > 31) throw std::invalid_argument("lmer must be in 1..31");
+  if (p->stride < 1) throw std::invalid_argument("stride must be >= 1");
+  if (p->gap < 2 || p->gap > 16) throw std::invalid_argument("gap must be in 2..16");
+}
+
+// Device copy of a base array with kPad 'N' bytes on both sides.
+void upload_padded(const char* host, int64_t n, DevArray<char>& dev, cudaStream_t st) {
+  dev.alloc((size_t)n + 2 * kPad);
+  CLAST_CK(cudaMemsetAsync(dev.p, 'N', (size_t)n + 2 * kPad, st));
+  if (n > 0) CLAST_CK(cudaMemcpyAsync(dev.p + kPad, host, (size_t)n, cudaMemcpyHostToDevice, st));
+}
+
+template <class T>
+T read_scalar(const T* dev, cudaStream_t st) {
+  T v;
+  CLAST_CK(cudaMemcpyAsync(&v, dev, sizeof(T), cudaMemcpyDeviceToHost, st));
+  CLAST_CK(cudaStreamSynchronize(st));
+  return v;
+}
+
+}  // namespace
+
+struct clast_index {
+  int l = 0, stride = 0, cut = 0;
+  int32_t t_begin = 0;
+  int64_t n = 0;
+  int32_t nseqs = 0;
+  DevArray<char> bases;  // padded
+  DevArray<int32_t> gateway, lengths;
+  DevArray<uint32_t> dir;
+  DevArray<uint64_t> ukeys;
+  DevArray<int32_t> ustart, ucnt;
+  DevArray<int2> entries;
+  int64_t n_unique = 0, n_entries = 0;
+  int dir_bits = 1, shift = 0;
+
+  IndexView view() const {
+    IndexView v;
+    v.l = l;
+    v.shift = shift;
+    v.dir = dir.p;
+    v.ukeys = ukeys.p;
+    v.ustart = ustart.p;
+    v.ucnt = ucnt.p;
+    v.entries = entries.p;
+    v.n_unique = n_unique;
+    return v;
+  }
+  TargetView tview() const {
+    TargetView t;
+    t.bases = bases.p + kPad;
+    t.n = n;
+    t.gateway = gateway.p;
+    t.lengths = lengths.p;
+    t.nseqs = nseqs;
+    return t;
+  }
+};
+
+namespace {
+
+// CDeviceHashTable::CDeviceHashTable (CDeviceHashTable.cu:143-174) for the
+// window whose padded bases are already in ix->bases.
+void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix) {
+  cudaStream_t st = c->st;
+  Workspace& ws = c->ws;
+  const int l = p->lmer;
+  const int64_t n = ix->n;
+  const char* bases = ix->bases.p + kPad;
+  uint64_t* packed = ws.get<uint64_t>("ix_packed", (size_t)(n / 32 + 4));
+  uint64_t* nmask = ws.get<uint64_t>("ix_nmask", (size_t)(n / 64 + 4));
+  pack_bases(bases, n, packed, nmask, st);
+  const int64_t ns = n / p->stride;  // CDeviceHashTable.cu:34
+  uint64_t* keys = ws.get<uint64_t>("ix_keys", ns);
+  int32_t* vals = ws.get<int32_t>("ix_vals", ns);
+  uint64_t* keys2 = ws.get<uint64_t>("ix_keys2", ns);
+  int32_t* vals2 = ws.get<int32_t>("ix_vals2", ns);
+  sample_keys(packed, nmask, ns, p->stride, l, keys, vals, st);
+  radix_sort_pairs(ws, keys, vals, keys2, vals2, ns, 2 * l + 1, st);
+  int64_t* scal = ws.get<int64_t>("ix_scalar", 4);
+  int64_t nv = 0;
+  if (ns > 0) {
+    count_below(keys, ns, 1ull << (2 * l), scal, st);
+    nv = read_scalar(scal, st);
+  }
+  int32_t* head = ws.get<int32_t>("ix_head", nv);
+  int64_t* hpos = ws.get<int64_t>("ix_hpos", nv + 1);
+  index_heads(keys, nv, head, st);
+  scan_i32(ws, head, nv, hpos, st);
+  const int64_t nu = read_scalar(hpos + nv, st);
+  ix->n_unique = nu;
+  ix->ukeys.alloc(nu);
+  int64_t* ufirst = ws.get<int64_t>("ix_ufirst", nu + 1);
+  index_unique(keys, head, hpos, nv, ix->ukeys.p, ufirst, st);
+  int32_t* keep = ws.get<int32_t>("ix_keep", nv);
+  int2* resolved = ws.get<int2>("ix_resolved", nv);
+  int64_t* kpos = ws.get<int64_t>("ix_kpos", nv + 1);
+  index_keep(vals, hpos, ufirst, nv, p->stride, l, p->cut_repeat, ix->gateway.p, ix->lengths.p, ix->nseqs, keep,
+             resolved, st);
+  scan_i32(ws, keep, nv, kpos, st);
+  const int64_t ne = read_scalar(kpos + nv, st);
+  ix->n_entries = ne;
+  ix->entries.alloc(ne);
+  index_entries(keep, kpos, resolved, nv, ix->entries.p, st);
+  ix->ustart.alloc(nu);
+  ix->ucnt.alloc(nu);
+  index_buckets(ufirst, kpos, nu, ix->ustart.p, ix->ucnt.p, st);
+  int bits = 1;
+  while (bits < 26 && (1ll << bits) < nu) ++bits;
+  bits = std::min(bits, 2 * l);
+  bits = std::max(bits, 1);
+  ix->dir_bits = bits;
+  ix->shift = 2 * l - bits;
+  ix->dir.alloc(((size_t)1 << bits) + 1);
+  index_directory(ix->ukeys.p, nu, ix->shift, bits, ix->dir.p, st);
+  CLAST_CK(cudaStreamSynchronize(st));
+}
+
+clast_index* make_index(clast_ctx* c, const clast_params* p, const char* bases, int64_t n_bases,
+                        const int32_t* gateway, const int32_t* lengths, int32_t n_seqs, int32_t t_begin) {
+  std::unique_ptr<clast_index> ix(new clast_index());
+  ix->l = p->lmer;
+  ix->stride = p->stride;
+  ix->cut = p->cut_repeat;
+  ix->t_begin = t_begin;
+  ix->n = n_bases;
+  ix->nseqs = n_seqs;
+  upload_padded(bases, n_bases, ix->bases, c->st);
+  ix->gateway.alloc(n_seqs);
+  ix->lengths.alloc(n_seqs);
+  if (n_seqs > 0) {
+    CLAST_CK(cudaMemcpyAsync(ix->gateway.p, gateway, n_seqs * sizeof(int32_t), cudaMemcpyHostToDevice, c->st));
+    CLAST_CK(cudaMemcpyAsync(ix->lengths.p, lengths, n_seqs * sizeof(int32_t), cudaMemcpyHostToDevice, c->st));
+  }
+  build_index_device(c, p, ix.get());
+  return ix.release();
+}
+
+// Device-resident query strands of one batch, packed once for every index.
+struct QueryBatch {
+  DevArray<char> bases;  // padded
+  int64_t n = 0;
+  DevArray<int64_t> start;
+  DevArray<int32_t> len;
+  DevArray<uint64_t> packed, nmask;
+  int32_t nstrands = 0;
+  DevArray<int32_t> wstart;  // strand index where each window starts, plus the end
+  int32_t nwin = 0;
+  QueryView view() const {
+    QueryView q;
+    q.bases = bases.p + kPad;
+    q.n = n;
+    q.packed = packed.p;
+    q.nmask = nmask.p;
+    q.start = start.p;
+    q.len = len.p;
+    q.nstrands = nstrands;
+    return q;
+  }
+  void pack(cudaStream_t st) {
+    packed.alloc((size_t)(n / 32 + 4));
+    nmask.alloc((size_t)(n / 64 + 4));
+    pack_bases(bases.p + kPad, n, packed.p, nmask.p, st);
+  }
+};
+
+// Host copy of one batch's result (reference order within each query window).
+struct HostHits {
+  std::vector<int32_t> t_id, t_idx, q_id, q_idx, t_len, q_len, match, score;
+  std::vector<double> evalue;
+  size_t size() const { return t_id.size(); }
+};
+
+// CDeviceHitList for every query window of `qb` against one index.
+void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, const QueryBatch& qb,
+                  int32_t q_first, HostHits& out) {
+  cudaStream_t st = c->st;
+  Workspace& ws = c->ws;
+  const QueryView q = qb.view();
+  const IndexView iv = ix->view();
+  const TargetView tv = ix->tview();
+  const int64_t ns = qb.nstrands, nr = ns / 2;
+  out = HostHits();
+  if (ns == 0 || ix->n_unique == 0) return;
+  // createRawSeedList + deleteSeedsOnSequenceBoundary
+  int64_t* cnt = ws.get<int64_t>("s_cnt", ns);
+  int64_t* off = ws.get<int64_t>("s_off", ns + 1);
+  seed_count(q, iv, cnt, st);
+  scan_i64(ws, cnt, ns, off, st);
+  const int64_t S = read_scalar(off + ns, st);
+  if (S == 0) return;
+  uint64_t* skey = ws.get<uint64_t>("s_key", S);
+  uint32_t* sq = ws.get<uint32_t>("s_q", S);
+  int32_t* nvalid = ws.get<int32_t>("s_nvalid", ns);
+  seed_write(q, iv, tv, p->gap, p->local, off, skey, sq, nvalid, st);
+  int32_t* wfirst = ws.get<int32_t>("s_wfirst", qb.nwin);
+  window_first(nvalid, qb.wstart.p, qb.nwin, wfirst, st);
+  // sortSeeds, deletingIsolateSeeds, deleteDuplicateSeeds
+  int32_t* len32 = ws.get<int32_t>("s_len32", ns);
+  to_i32(cnt, ns, len32, st);
+  segmented_sort_u32(ws, skey, sq, off, len32, ns, st, 0);
+  int32_t* hcnt = ws.get<int32_t>("s_hcnt", ns);
+  seed_filter(skey, sq, off, nvalid, qb.wstart.p, qb.nwin, wfirst, p->width, p->gap, ns, hcnt, st);
+  int64_t* hoff = ws.get<int64_t>("s_hoff", ns + 1);
+  scan_i32(ws, hcnt, ns, hoff, st);
+  const int64_t H = read_scalar(hoff + ns, st);
+  if (H == 0) return;
+  uint64_t* hk = ws.get<uint64_t>("h_key", H);
+  int32_t* hq = ws.get<int32_t>("h_q", H);
+  int32_t* hs = ws.get<int32_t>("h_s", H);
+  gather_hits(skey, sq, off, hcnt, hoff, ns, hk, hq, hs, st);
+  // alignmentHits + calculateEvalue + deleteHits_lowEValue / _tooShort
+  DpOut o;
+  o.t_idx = ws.get<int32_t>("d_tidx", H);
+  o.q_idx = ws.get<int32_t>("d_qidx", H);
+  o.t_len = ws.get<int32_t>("d_tlen", H);
+  o.q_len = ws.get<int32_t>("d_qlen", H);
+  o.match = ws.get<int32_t>("d_match", H);
+  o.score = ws.get<int32_t>("d_score", H);
+  o.evalue = ws.get<double>("d_e", H);
+  o.keep = ws.get<uint8_t>("d_keep", H);
+  DpParams dp{p->lmer, p->stride, p->gap, p->local, p->cutoff, p->total_db, p->K, p->lambda};
+  banded_dp(tv, q, hk, hq, hs, H, dp, o, st);
+  // resultSorting + deleteHits_duplicateResult, per read
+  uint64_t* k1 = ws.get<uint64_t>("f_k1", H);
+  uint64_t* k2 = ws.get<uint64_t>("f_k2", H);
+  int32_t* idx = ws.get<int32_t>("f_idx", H);
+  final_keys(hk, hq, hs, o, H, k1, k2, idx, st);
+  int64_t* roff = ws.get<int64_t>("f_roff", nr);
+  int32_t* rlen = ws.get<int32_t>("f_rlen", nr);
+  read_ranges(hoff, nr, roff, rlen, st);
+  segmented_sort_u64(ws, k1, k2, idx, roff, rlen, nr, st, 1);
+  int32_t* fcnt = ws.get<int32_t>("f_cnt", nr);
+  int32_t* fsel = ws.get<int32_t>("f_sel", H);
+  final_dedupe(k1, k2, idx, hk, hs, o, roff, rlen, nr, fcnt, fsel, st);
+  int64_t* foff = ws.get<int64_t>("f_off", nr + 1);
+  scan_i32(ws, fcnt, nr, foff, st);
+  const int64_t F = read_scalar(foff + nr, st);
+  if (F == 0) return;
+  FinalOut fo;
+  fo.t_id = ws.get<int32_t>("o_tid", F);
+  fo.t_idx = ws.get<int32_t>("o_tidx", F);
+  fo.q_id = ws.get<int32_t>("o_qid", F);
+  fo.q_idx = ws.get<int32_t>("o_qidx", F);
+  fo.t_len = ws.get<int32_t>("o_tlen", F);
+  fo.q_len = ws.get<int32_t>("o_qlen", F);
+  fo.match = ws.get<int32_t>("o_match", F);
+  fo.score = ws.get<int32_t>("o_score", F);
+  fo.evalue = ws.get<double>("o_e", F);
+  final_compact(fsel, roff, fcnt, foff, nr, hk, hs, o, ix->t_begin, q_first, fo, st);
+  auto d2h = [&](std::vector<int32_t>& v, const int32_t* d) {
+    v.resize(F);
+    CLAST_CK(cudaMemcpyAsync(v.data(), d, F * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  };
+  d2h(out.t_id, fo.t_id);
+  d2h(out.t_idx, fo.t_idx);
+  d2h(out.q_id, fo.q_id);
+  d2h(out.q_idx, fo.q_idx);
+  d2h(out.t_len, fo.t_len);
+  d2h(out.q_len, fo.q_len);
+  d2h(out.match, fo.match);
+  d2h(out.score, fo.score);
+  out.evalue.resize(F);
+  CLAST_CK(cudaMemcpyAsync(out.evalue.data(), fo.evalue, F * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CLAST_CK(cudaStreamSynchronize(st));
+}
+
+template <class T>
+T* host_copy(const std::vector<T>& v) {
+  T* p = static_cast<T*>(std::malloc((v.size() ? v.size() : 1) * sizeof(T)));
+  if (!p) throw std::bad_alloc();
+  if (!v.empty()) std::memcpy(p, v.data(), v.size() * sizeof(T));
+  return p;
+}
+
+int fail(clast_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+// Runs f() and turns every exception into a status code plus message.
+template <class F>
+int guarded(clast_ctx* ctx, F&& f) {
+  try {
+    return f();
+  } catch (const CudaError& e) {
+    return fail(ctx, CLAST_ERR_CUDA, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(ctx, CLAST_ERR_NOMEM, "out of memory");
+  } catch (const std::invalid_argument& e) {
+    return fail(ctx, CLAST_ERR_ARG, e.what());
+  } catch (const std::exception& e) {
+    return fail(ctx, CLAST_ERR_INTERNAL, e.what());
+  }
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------------
+// targets / map: whole job with resident indexes
+// ----------------------------------------------------------------------------
+struct clast_targets {
+  clast_ctx* ctx = nullptr;
+  struct Win {
+    int32_t load, first;  // target load, first record within the load
+    std::unique_ptr<clast_index> ix;
+  };
+  std::vector<Win> wins;
+  int32_t n_loads = 0;
+};
+
+namespace {
+
+// One read window list per query load (moveQueryWindow, CHostSchedular.cu:12-23).
+void query_windows(const int64_t* offsets, int64_t r0, int64_t r1, int l, int32_t q_vram,
+                   std::vector<int64_t>& win_first_read) {
+  // gateway over strands: every read adds two strands of len + l - 1
+  const int64_t nreads = r1 - r0;
+  auto gw = [&](int64_t strand) -> int64_t {  // gateway(strand) relative to the load
+    const int64_t r = strand / 2;
+    int64_t v = 2 * (offsets[r0 + r] - offsets[r0]) + 2 * r * (int64_t)(l - 1);
+    if (strand & 1) v += (offsets[r0 + r + 1] - offsets[r0 + r]) + (l - 1);
+    return v;
+  };
+  for (int64_t qb = 0, qe = 1; qb < nreads; qb = qe++) {
+    const int64_t base = gw(2 * qb);
+    while (qe < nreads && gw(2 * qe + 2) - base < (int64_t)q_vram) ++qe;
+    win_first_read.push_back(r0 + qb);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int clast_ctx_create(int device, clast_ctx** out) {
+  if (!out) return CLAST_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<clast_ctx> c(new (std::nothrow) clast_ctx());
+  if (!c) return CLAST_ERR_NOMEM;
+  c->device = device;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    (void)cudaGetLastError();
+    return CLAST_ERR_CUDA;
+  }
+  if (device < 0 || device >= ndev) return CLAST_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return CLAST_ERR_CUDA;
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
+  if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) return CLAST_ERR_CUDA;
+  *out = c.release();
+  return CLAST_OK;
+}
+
+void clast_ctx_destroy(clast_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
+  ctx->ws.release_all();
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->st) cudaStreamDestroy(ctx->st);
+  delete ctx;
+}
+
+const char* clast_last_error(const clast_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int clast_index_build(clast_ctx* ctx, const clast_params* p, const char* bases, int64_t n_bases,
+                      const int32_t* gateway, const int32_t* lengths, int32_t n_seqs, int32_t t_begin,
+                      clast_index** out) {
+  if (!ctx || !out) return CLAST_ERR_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&]() -> int {
+    check_params(p);
+    if (n_bases < 0 || n_seqs < 0 || (n_bases > 0 && !bases) || (n_seqs > 0 && (!gateway || !lengths)))
+      throw std::invalid_argument("bad window arrays");
+    if (n_bases >= INT32_MAX) throw std::invalid_argument("window larger than 2^31 bases");
+    CLAST_CK(cudaSetDevice(ctx->device));
+    g_kernel_launches = 0;
+    *out = make_index(ctx, p, bases, n_bases, gateway, lengths, n_seqs, t_begin);
+    return CLAST_OK;
+  });
+}
+
+void clast_index_free(clast_index* ix) { delete ix; }
+
+int clast_search(clast_ctx* ctx, const clast_index* ix, const clast_params* p, const char* q_bases,
+                 int64_t n_qbases, const int32_t* q_gateway, const int32_t* q_lengths, int32_t n_qseqs,
+                 int32_t q_begin, clast_hits* out) {
+  if (!ctx || !out) return CLAST_ERR_ARG;
+  std::memset(out, 0, sizeof(*out));
+  return guarded(ctx, [&]() -> int {
+    check_params(p);
+    if (!ix) throw std::invalid_argument("index is null");
+    if (p->lmer != ix->l || p->stride != ix->stride || p->cut_repeat != ix->cut)
+      throw std::invalid_argument("params differ from the ones the index was built with");
+    if (n_qseqs < 0 || (n_qseqs & 1) || (q_begin & 1))
+      throw std::invalid_argument("query windows hold whole reads: n_qseqs and q_begin must be even");
+    if (n_qbases < 0 || (n_qbases > 0 && !q_bases) || (n_qseqs > 0 && (!q_gateway || !q_lengths)))
+      throw std::invalid_argument("bad query arrays");
+    CLAST_CK(cudaSetDevice(ctx->device));
+    g_kernel_launches = 0;
+    cudaStream_t st = ctx->st;
+    QueryBatch qb;
+    qb.n = n_qbases;
+    qb.nstrands = n_qseqs;
+    upload_padded(q_bases, n_qbases, qb.bases, st);
+    std::vector<int64_t> start(n_qseqs);
+    for (int32_t i = 0; i < n_qseqs; ++i) {
+      start[i] = q_gateway[i];
+      if (q_gateway[i] < 0 || q_lengths[i] < 0 || (int64_t)q_gateway[i] + q_lengths[i] > n_qbases)
+        throw std::invalid_argument("query sequence outside the base array");
+    }
+    qb.start.alloc(n_qseqs);
+    qb.len.alloc(n_qseqs);
+    if (n_qseqs) {
+      CLAST_CK(cudaMemcpyAsync(qb.start.p, start.data(), n_qseqs * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+      CLAST_CK(cudaMemcpyAsync(qb.len.p, q_lengths, n_qseqs * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    }
+    const int32_t ws2[2] = {0, n_qseqs};
+    qb.nwin = 1;
+    qb.wstart.alloc(2);
+    CLAST_CK(cudaMemcpyAsync(qb.wstart.p, ws2, sizeof(ws2), cudaMemcpyHostToDevice, st));
+    qb.pack(st);
+    HostHits h;
+    search_batch(ctx, ix, p, qb, q_begin, h);
+    out->n = (int64_t)h.size();
+    out->t_id = host_copy(h.t_id);
+    out->t_idx = host_copy(h.t_idx);
+    out->q_id = host_copy(h.q_id);
+    out->q_idx = host_copy(h.q_idx);
+    out->t_len = host_copy(h.t_len);
+    out->q_len = host_copy(h.q_len);
+    out->match = host_copy(h.match);
+    out->score = host_copy(h.score);
+    out->evalue = host_copy(h.evalue);
+    ctx->last_launches = g_kernel_launches;
+    return CLAST_OK;
+  });
+}
+
+void clast_hits_free(clast_hits* h) {
+  if (!h) return;
+  std::free(h->t_id); std::free(h->t_idx); std::free(h->q_id); std::free(h->q_idx);
+  std::free(h->t_len); std::free(h->q_len); std::free(h->match); std::free(h->score);
+  std::free(h->evalue);
+  std::memset(h, 0, sizeof(*h));
+}
+
+int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, const clast_seqs* targets,
+                         int32_t n_loads, const int64_t* load_sizes, clast_targets** out) {
+  if (!ctx || !out) return CLAST_ERR_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&]() -> int {
+    check_params(p);
+    if (!targets || n_loads < 0 || (n_loads > 0 && !load_sizes)) throw std::invalid_argument("bad targets");
+    int64_t total = 0;
+    for (int32_t k = 0; k < n_loads; ++k) total += load_sizes[k];
+    if (total != targets->n_seqs) throw std::invalid_argument("load sizes do not add up to n_seqs");
+    CLAST_CK(cudaSetDevice(ctx->device));
+    g_kernel_launches = 0;
+    const int l = p->lmer;
+    std::unique_ptr<clast_targets> T(new clast_targets());
+    T->ctx = ctx;
+    T->n_loads = n_loads;
+    int64_t rec = 0;
+    std::vector<char> wb;
+    std::vector<int32_t> gw, ln;
+    for (int32_t k = 0; k < n_loads; ++k) {
+      const int64_t r0 = rec, r1 = rec + load_sizes[k];
+      rec = r1;
+      // load-relative gateway: prefix sums of len + l - 1 (CHostSeqList_target.cu:8-33)
+      std::vector<int64_t> lg(r1 - r0 + 1, 0);
+      for (int64_t i = r0; i < r1; ++i)
+        lg[i - r0 + 1] = lg[i - r0] + (targets->offsets[i + 1] - targets->offsets[i]) + (l - 1);
+      const int64_t tEnd = r1 - r0;
+      for (int64_t tb = 0, te = 1; tb < tEnd; tb = te++) {  // moveTargetWindow
+        while (te < tEnd && lg[te + 1] - lg[tb] < (int64_t)t_vram) ++te;
+        wb.clear();
+        gw.clear();
+        ln.clear();
+        for (int64_t i = r0 + tb; i < r0 + te; ++i) {
+          const char* s = targets->bases + targets->offsets[i];
+          const int64_t len = targets->offsets[i + 1] - targets->offsets[i];
+          gw.push_back((int32_t)wb.size());
+          ln.push_back((int32_t)len);
+          wb.insert(wb.end(), s, s + len);
+          for (int j = 0; j < l - 1; ++j) wb.push_back(j < len ? s[j] : 'N');  // joint
+        }
+        if (wb.size() >= (size_t)INT32_MAX) throw std::invalid_argument("target window larger than 2^31 bases");
+        clast_targets::Win w;
+        w.load = k;
+        w.first = (int32_t)tb;
+        w.ix.reset(make_index(ctx, p, wb.data(), (int64_t)wb.size(), gw.data(), ln.data(), (int32_t)gw.size(),
+                              (int32_t)tb));
+        T->wins.push_back(std::move(w));
+      }
+    }
+    *out = T.release();
+    return CLAST_OK;
+  });
+}
+
+void clast_targets_free(clast_targets* t) { delete t; }
+
+int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int32_t q_vram,
+              const clast_seqs* reads, int32_t n_loads, const int64_t* load_sizes, clast_map_result* out) {
+  if (!ctx || !out) return CLAST_ERR_ARG;
+  std::memset(out, 0, sizeof(*out));
+  return guarded(ctx, [&]() -> int {
+    check_params(p);
+    if (!T || !reads || n_loads < 0 || (n_loads > 0 && !load_sizes)) throw std::invalid_argument("bad arguments");
+    int64_t total = 0;
+    for (int32_t k = 0; k < n_loads; ++k) total += load_sizes[k];
+    if (total != reads->n_seqs) throw std::invalid_argument("load sizes do not add up to n_seqs");
+    for (const auto& w : T->wins)
+      if (p->lmer != w.ix->l || p->stride != w.ix->stride || p->cut_repeat != w.ix->cut)
+        throw std::invalid_argument("params differ from the ones the targets were built with");
+    CLAST_CK(cudaSetDevice(ctx->device));
+    g_kernel_launches = 0;
+    cudaStream_t st = ctx->st;
+    CLAST_CK(cudaEventRecord(ctx->ev0, st));
+    const int64_t nreads = reads->n_seqs;
+    // query windows of every load, in read order
+    std::vector<int64_t> wfirst;
+    std::vector<int64_t> load_first(n_loads + 1, 0);
+    for (int32_t k = 0; k < n_loads; ++k) load_first[k + 1] = load_first[k] + load_sizes[k];
+    for (int32_t k = 0; k < n_loads; ++k)
+      query_windows(reads->offsets, load_first[k], load_first[k + 1], p->lmer, q_vram, wfirst);
+    wfirst.push_back(nreads);
+    // upload every read once; strands built on the device
+    const int64_t nb = reads->offsets[nreads] - reads->offsets[0];
+    DevArray<char> draw;
+    DevArray<int64_t> doff;
+    draw.alloc((size_t)nb + 64);
+    doff.alloc((size_t)nreads + 1);
+    std::vector<int64_t> off0(nreads + 1);
+    for (int64_t i = 0; i <= nreads; ++i) off0[i] = reads->offsets[i] - reads->offsets[0];
+    if (nb) CLAST_CK(cudaMemcpyAsync(draw.p, reads->bases + reads->offsets[0], nb, cudaMemcpyHostToDevice, st));
+    CLAST_CK(cudaMemcpyAsync(doff.p, off0.data(), (nreads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    QueryBatch qb;
+    qb.n = 2 * nb;
+    qb.nstrands = (int32_t)(2 * nreads);
+    qb.bases.alloc((size_t)qb.n + 2 * kPad);
+    CLAST_CK(cudaMemsetAsync(qb.bases.p, 'N', (size_t)qb.n + 2 * kPad, st));
+    qb.start.alloc(2 * nreads);
+    qb.len.alloc(2 * nreads);
+    build_strands(draw.p, doff.p, nreads, nb, qb.bases.p + kPad, qb.start.p, qb.len.p, st);
+    std::vector<int32_t> wstart(wfirst.size());
+    for (size_t i = 0; i < wfirst.size(); ++i) wstart[i] = (int32_t)(2 * wfirst[i]);
+    qb.nwin = (int32_t)wfirst.size() - 1;
+    qb.wstart.alloc(wstart.size());
+    CLAST_CK(cudaMemcpyAsync(qb.wstart.p, wstart.data(), wstart.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                             st));
+    qb.pack(st);
+    // every target window, in holder order (target load, window)
+    std::vector<HostHits> per_win(T->wins.size());
+    for (size_t w = 0; w < T->wins.size(); ++w) search_batch(ctx, T->wins[w].ix.get(), p, qb, 0, per_win[w]);
+    CLAST_CK(cudaEventRecord(ctx->ev1, st));
+    CLAST_CK(cudaEventSynchronize(ctx->ev1));
+    float ms = 0;
+    CLAST_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->last_ms = ms;
+    ctx->last_launches = g_kernel_launches;
+    // fixResult: per read, stable merge by score desc over the windows in holder order
+    std::vector<std::vector<std::pair<int64_t, int64_t>>> ranges(T->wins.size());
+    std::vector<int64_t> per_read(nreads + 1, 0);
+    for (size_t w = 0; w < T->wins.size(); ++w) {
+      const HostHits& h = per_win[w];
+      for (size_t i = 0; i < h.size(); ++i) per_read[h.q_id[i] / 2 + 1]++;
+    }
+    for (int64_t r = 0; r < nreads; ++r) per_read[r + 1] += per_read[r];
+    const int64_t F = per_read[nreads];
+    clast_map_result res;
+    std::memset(&res, 0, sizeof(res));
+    res.n = F;
+    auto alloc32 = [&](int32_t*& q) {
+      q = static_cast<int32_t*>(std::malloc((F ? F : 1) * sizeof(int32_t)));
+      if (!q) throw std::bad_alloc();
+    };
+    alloc32(res.read); alloc32(res.strand); alloc32(res.t_load); alloc32(res.t_seq); alloc32(res.t_idx);
+    alloc32(res.q_idx); alloc32(res.t_len); alloc32(res.q_len); alloc32(res.match); alloc32(res.score);
+    res.evalue = static_cast<double*>(std::malloc((F ? F : 1) * sizeof(double)));
+    res.load_offsets = static_cast<int64_t*>(std::malloc((n_loads + 1) * sizeof(int64_t)));
+    if (!res.evalue || !res.load_offsets) throw std::bad_alloc();
+    for (int32_t k = 0; k <= n_loads; ++k) res.load_offsets[k] = per_read[load_first[k]];
+    std::vector<int64_t> fill(per_read.begin(), per_read.end() - 1);
+    struct Ref { int32_t w; int64_t i; };
+    std::vector<Ref> refs(F);
+    for (size_t w = 0; w < T->wins.size(); ++w) {
+      const HostHits& h = per_win[w];
+      for (size_t i = 0; i < h.size(); ++i) refs[fill[h.q_id[i] / 2]++] = Ref{(int32_t)w, (int64_t)i};
+    }
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t r = 0; r < nreads; ++r) {
+      const int64_t a = per_read[r], b = per_read[r + 1];
+      if (b - a > 1)
+        std::stable_sort(refs.begin() + a, refs.begin() + b, [&](const Ref& x, const Ref& y) {
+          return per_win[x.w].score[x.i] > per_win[y.w].score[y.i];
+        });
+      for (int64_t j = a; j < b; ++j) {
+        const HostHits& h = per_win[refs[j].w];
+        const int64_t i = refs[j].i;
+        const auto& win = T->wins[refs[j].w];
+        res.read[j] = h.q_id[i] / 2;
+        res.strand[j] = h.q_id[i] & 1;
+        res.t_load[j] = win.load;
+        res.t_seq[j] = h.t_id[i];
+        res.t_idx[j] = h.t_idx[i];
+        res.q_idx[j] = h.q_idx[i];
+        res.t_len[j] = h.t_len[i];
+        res.q_len[j] = h.q_len[i];
+        res.match[j] = h.match[i];
+        res.score[j] = h.score[i];
+        res.evalue[j] = h.evalue[i];
+      }
+    }
+    *out = res;
+    return CLAST_OK;
+  });
+}
+
+void clast_map_result_free(clast_map_result* r) {
+  if (!r) return;
+  std::free(r->load_offsets); std::free(r->read); std::free(r->strand); std::free(r->t_load);
+  std::free(r->t_seq); std::free(r->t_idx); std::free(r->q_idx); std::free(r->t_len); std::free(r->q_len);
+  std::free(r->match); std::free(r->score); std::free(r->evalue);
+  std::memset(r, 0, sizeof(*r));
+}
+
+int clast_last_map_stats(const clast_ctx* ctx, double* device_ms, int64_t* kernel_launches) {
+  if (!ctx) return CLAST_ERR_ARG;
+  if (device_ms) *device_ms = ctx->last_ms;
+  if (kernel_launches) *kernel_launches = ctx->last_launches;
+  return CLAST_OK;
+}
+
+}  // extern "C"

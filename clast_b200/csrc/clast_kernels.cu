@@ -1,0 +1,1133 @@
+// clast_kernels.cu -- sm_100a kernels of the CLAST seed-and-extend path.
+//
+// Reference (masayano/CLAST) stages and the kernels that replace them:
+//   SRead2bit/SRepelHasOddBase + CDeviceSeqList_query::createHashIndex -> pack_bases, kmer_at
+//   CDeviceHashTable (sort_by_key, unique, reduce_by_key, scan, cut)   -> sample_keys,
+//       radix_sort_pairs, index_* (directory for O(1) lookups)
+//   createRawSeedList (binarySearch, writeSeedList)                     -> seed_count, seed_write
+//   deleteSeedsOnSequenceBoundary                                       -> folded into seed_write
+//   sortSeeds / deletingIsolateSeeds / deleteDuplicateSeeds             -> segmented_sort, seed_filter
+//   globalAlign* / localAlign* + calculateEvalue + deleteBadHits        -> banded_dp
+//   resultSorting + deleteHits_duplicateResult                          -> final_* (per read)
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+#include "clast_device.cuh"
+#include "clast_kernels.cuh"
+#include "clast_workspace.h"
+
+namespace clast {
+
+thread_local int64_t g_kernel_launches = 0;
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+inline int blocks_for(int64_t n, int threads) { return (int)((n + threads - 1) / threads); }
+inline int grid_cap(int64_t want) { return (int)(want < 1 ? 1 : (want > 1048576 ? 1048576 : want)); }
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// ------------------------------------------------------------------------
+// exclusive scan
+// ------------------------------------------------------------------------
+constexpr int kScanThreads = 256, kScanItems = 8, kScanTile = kScanThreads * kScanItems;
+
+template <class T>
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const T* __restrict__ in, int64_t n_in,
+                                                             int64_t n_out, int64_t* __restrict__ out,
+                                                             int64_t* __restrict__ tile_sums) {
+  __shared__ int64_t warp_tot[kScanThreads / 32];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int64_t v[kScanItems];
+  int64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int64_t idx = base + i;
+    v[i] = (idx < n_in) ? (int64_t)in[idx] : 0;
+    s += v[i];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  int64_t wpre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < kScanThreads / 32; ++w) {
+    const int64_t t = warp_tot[w];
+    if (w < warp) wpre += t;
+    tot += t;
+  }
+  int64_t run = wpre + incl - s;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int64_t idx = base + i;
+    if (idx < n_out) out[idx] = run;
+    run += v[i];
+  }
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_add(int64_t* __restrict__ out, int64_t n_out, const int64_t* __restrict__ tile_pre) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_out) out[i] += tile_pre[i / kScanTile];
+}
+
+template <class T>
+void scan_impl(Workspace& ws, const T* in, int64_t n, int64_t* out, cudaStream_t st, int level) {
+  const int64_t n_out = n + 1;
+  const int64_t tiles = (n_out + kScanTile - 1) / kScanTile;
+  const std::string tag = "scan" + std::to_string(level);
+  int64_t* sums = ws.get<int64_t>(tag + "s", tiles);
+  k_scan_tiles<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, n_out, out, sums);
+  CLAST_LAUNCHED();
+  if (tiles > 1) {
+    int64_t* pre = ws.get<int64_t>(tag + "p", tiles + 1);
+    scan_impl<int64_t>(ws, sums, tiles, pre, st, level + 1);
+    k_scan_add<<<blocks_for(n_out, 256), 256, 0, st>>>(out, n_out, pre);
+    CLAST_LAUNCHED();
+  }
+}
+
+// ------------------------------------------------------------------------
+// packing and query strands
+// ------------------------------------------------------------------------
+__global__ void k_pack(const char* __restrict__ bases, int64_t n, uint64_t* __restrict__ packed,
+                       uint64_t* __restrict__ nmask, int64_t nwords) {
+  const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nwords) return;
+  uint64_t m = 0, p0 = 0, p1 = 0;
+  const int64_t f0 = w * 64;
+#pragma unroll 8
+  for (int i = 0; i < 64; ++i) {
+    const int64_t f = f0 + i;
+    const char c = (f < n) ? bases[f] : 'N';
+    uint64_t code = 0, isn = 0;
+    switch (c) {
+      case 'A': code = 0; break;
+      case 'C': code = 1; break;
+      case 'G': code = 2; break;
+      case 'T': code = 3; break;
+      default: isn = 1;
+    }
+    m |= isn << (63 - i);
+    if (i < 32) p0 |= code << (62 - 2 * i);
+    else p1 |= code << (62 - 2 * (i - 32));
+  }
+  nmask[w] = m;
+  packed[2 * w] = p0;
+  packed[2 * w + 1] = p1;
+}
+
+__device__ __forceinline__ char complement(char c) {
+  switch (c) {
+    case 'A': return 'T';
+    case 'T': return 'A';
+    case 'G': return 'C';
+    case 'C': return 'G';
+    default: return 'N';
+  }
+}
+
+__global__ void k_strand_meta(const int64_t* __restrict__ off, int64_t n_reads, int64_t* __restrict__ sstart,
+                              int32_t* __restrict__ slen) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_reads) return;
+  const int64_t a = off[r], len = off[r + 1] - a;
+  sstart[2 * r] = 2 * a;
+  sstart[2 * r + 1] = 2 * a + len;
+  slen[2 * r] = (int32_t)len;
+  slen[2 * r + 1] = (int32_t)len;
+}
+
+__global__ void k_strands(const char* __restrict__ reads, const int64_t* __restrict__ off, int64_t n_reads,
+                          int64_t n_bases, char* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_bases) return;
+  int64_t lo = 0, hi = n_reads;  // last read with off[r] <= i
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (off[mid] <= i) lo = mid;
+    else hi = mid;
+  }
+  const int64_t a = off[lo], len = off[lo + 1] - a, j = i - a;
+  const char c = reads[i];
+  out[2 * a + j] = c;
+  out[2 * a + len + (len - 1 - j)] = complement(c);
+}
+
+// ------------------------------------------------------------------------
+// index build
+// ------------------------------------------------------------------------
+__global__ void k_sample_keys(const uint64_t* __restrict__ packed, const uint64_t* __restrict__ nmask,
+                              int64_t ns, int stride, int l, uint64_t* __restrict__ keys,
+                              int32_t* __restrict__ vals) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  uint64_t key;
+  if (!kmer_at(packed, nmask, j * stride, l, key)) key = 1ull << (2 * l);
+  keys[j] = key;
+  vals[j] = (int32_t)j;
+}
+
+constexpr int kRsThreads = 256, kRsItems = 16, kRsTile = kRsThreads * kRsItems;
+
+__global__ void __launch_bounds__(kRsThreads) k_radix_hist(const uint64_t* __restrict__ keys, int64_t n,
+                                                           int shift, uint32_t* __restrict__ hist,
+                                                           int nblocks) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kRsTile;
+#pragma unroll 4
+  for (int r = 0; r < kRsItems; ++r) {
+    const int64_t idx = base + r * kRsThreads + threadIdx.x;
+    if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 255], 1u);
+  }
+  __syncthreads();
+  hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kRsThreads) k_radix_scatter(const uint64_t* __restrict__ kin,
+                                                              const int32_t* __restrict__ vin,
+                                                              uint64_t* __restrict__ kout,
+                                                              int32_t* __restrict__ vout, int64_t n, int shift,
+                                                              const int64_t* __restrict__ offs, int nblocks) {
+  __shared__ uint32_t wcnt[kRsThreads / 32][256];
+  __shared__ uint32_t run[256];
+  __shared__ int64_t goff[256];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  goff[tid] = offs[(int64_t)tid * nblocks + blockIdx.x];
+  run[tid] = 0;
+#pragma unroll
+  for (int w = 0; w < kRsThreads / 32; ++w) wcnt[w][tid] = 0;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kRsTile;
+  const unsigned lt = lanemask_lt();
+  for (int r = 0; r < kRsItems; ++r) {
+    const int64_t idx = base + r * kRsThreads + tid;
+    const bool valid = idx < n;
+    const uint64_t k = valid ? kin[idx] : 0;
+    const int32_t v = valid ? vin[idx] : 0;
+    const unsigned d = valid ? (unsigned)((k >> shift) & 255) : 256u;
+    const unsigned peers = __match_any_sync(kFull, d);
+    const unsigned rank = __popc(peers & lt);
+    if (valid && lane == __ffs(peers) - 1) wcnt[warp][d] = __popc(peers);
+    __syncthreads();
+    {
+      uint32_t acc = run[tid];
+#pragma unroll
+      for (int w = 0; w < kRsThreads / 32; ++w) {
+        const uint32_t c = wcnt[w][tid];
+        wcnt[w][tid] = acc;
+        acc += c;
+      }
+      run[tid] = acc;
+    }
+    __syncthreads();
+    if (valid) {
+      const int64_t pos = goff[d] + wcnt[warp][d] + rank;
+      kout[pos] = k;
+      vout[pos] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int w = 0; w < kRsThreads / 32; ++w) wcnt[w][tid] = 0;
+    __syncthreads();
+  }
+}
+
+__global__ void k_count_below(const uint64_t* __restrict__ keys, int64_t n, uint64_t bound,
+                              int64_t* __restrict__ out) {
+  int64_t lo = 0, hi = n;  // first key >= bound in a sorted array
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (keys[mid] < bound) lo = mid + 1;
+    else hi = mid;
+  }
+  *out = lo;
+}
+
+__global__ void k_index_heads(const uint64_t* __restrict__ k, int64_t nv, int32_t* __restrict__ head) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nv) head[i] = (i == 0 || k[i] != k[i - 1]) ? 1 : 0;
+}
+
+__global__ void k_index_unique(const uint64_t* __restrict__ k, const int32_t* __restrict__ head,
+                               const int64_t* __restrict__ hpos, int64_t nv, uint64_t* __restrict__ ukeys,
+                               int64_t* __restrict__ ufirst) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nv && head[i]) {
+    ukeys[hpos[i]] = k[i];
+    ufirst[hpos[i]] = i;
+  }
+  if (i == 0) ufirst[hpos[nv]] = nv;
+}
+
+__global__ void k_index_keep(const int32_t* __restrict__ vals, const int64_t* __restrict__ hpos,
+                             const int64_t* __restrict__ ufirst, int64_t nv, int stride, int l, int cut,
+                             const int32_t* __restrict__ gw, const int32_t* __restrict__ len, int nseqs,
+                             int32_t* __restrict__ keep, int2* __restrict__ resolved) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  const int64_t u = hpos[i + 1] - 1;
+  const int64_t cnt = ufirst[u + 1] - ufirst[u];
+  const bool pass = (cut == -1) || (cnt < (int64_t)cut);  // removeRepeatedSequence
+  const int64_t pos = (int64_t)vals[i] * stride;
+  int lo = 0, hi = nseqs;  // last sequence starting at or before pos
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if ((int64_t)gw[mid] <= pos) lo = mid;
+    else hi = mid;
+  }
+  const int tidx = (int)(pos - gw[lo]);
+  const bool joint = (int64_t)tidx + l > (int64_t)len[lo];  // onTargetBoundary
+  keep[i] = (pass && !joint) ? 1 : 0;
+  resolved[i] = make_int2(lo, tidx);
+}
+
+__global__ void k_index_entries(const int32_t* __restrict__ keep, const int64_t* __restrict__ kpos,
+                                const int2* __restrict__ resolved, int64_t nv, int2* __restrict__ entries) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nv && keep[i]) entries[kpos[i]] = resolved[i];
+}
+
+__global__ void k_index_buckets(const int64_t* __restrict__ ufirst, const int64_t* __restrict__ kpos,
+                                int64_t nu, int32_t* __restrict__ ustart, int32_t* __restrict__ ucnt) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nu) return;
+  const int64_t a = kpos[ufirst[k]], b = kpos[ufirst[k + 1]];
+  ustart[k] = (int32_t)a;
+  ucnt[k] = (int32_t)(b - a);
+}
+
+__global__ void k_index_dir(const uint64_t* __restrict__ ukeys, int64_t nu, int shift, int64_t nslots,
+                            uint32_t* __restrict__ dir) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p > nslots) return;
+  const uint64_t target = (uint64_t)p << shift;
+  int64_t lo = 0, hi = nu;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (ukeys[mid] < target) lo = mid + 1;
+    else hi = mid;
+  }
+  dir[p] = (uint32_t)lo;
+}
+
+// ------------------------------------------------------------------------
+// seeds
+// ------------------------------------------------------------------------
+__global__ void k_seed_count(QueryView q, IndexView ix, int64_t* __restrict__ cnt) {
+  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (s >= q.nstrands) return;
+  const int64_t st = q.start[s];
+  const int nk = q.len[s] - ix.l + 1;
+  int64_t sum = 0;
+  for (int qi = lane; qi < nk; qi += 32) {
+    uint64_t key;
+    if (kmer_at(q.packed, q.nmask, st + qi, ix.l, key)) {
+      const int64_t u = index_lookup(ix, key);
+      if (u >= 0) sum += ix.ucnt[u];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+  if (lane == 0) cnt[s] = sum;
+}
+
+__global__ void k_seed_write(QueryView q, IndexView ix, TargetView t, int gap, int local,
+                             const int64_t* __restrict__ off, uint64_t* __restrict__ skey,
+                             uint32_t* __restrict__ sq, int32_t* __restrict__ nvalid) {
+  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (s >= q.nstrands) return;
+  const int64_t st = q.start[s];
+  const int qlen = q.len[s];
+  const int nk = qlen - ix.l + 1;
+  int64_t base = off[s];
+  int valid = 0;
+  for (int c0 = 0; c0 < nk; c0 += 32) {
+    const int qi = c0 + lane;
+    int c = 0, us = 0;
+    if (qi < nk) {
+      uint64_t key;
+      if (kmer_at(q.packed, q.nmask, st + qi, ix.l, key)) {
+        const int64_t u = index_lookup(ix, key);
+        if (u >= 0) {
+          c = ix.ucnt[u];
+          us = ix.ustart[u];
+        }
+      }
+    }
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(kFull, incl, 31);
+    const int64_t w0 = base + incl - c;
+    for (int i = 0; i < c; ++i) {
+      const int2 e = ix.entries[us + i];
+      const int s0 = e.y - qi;  // tHitStartIdx, is_onCorner
+      const bool drop = !local && ((s0 + gap < 0) || (s0 + qlen - gap > t.lengths[e.x]));
+      skey[w0 + i] = drop ? kDroppedSeed : (((uint64_t)(uint32_t)e.x << 32) | ((uint32_t)s0 ^ 0x80000000u));
+      sq[w0 + i] = (uint32_t)qi;
+      valid += drop ? 0 : 1;
+    }
+    base += total;
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) valid += __shfl_xor_sync(kFull, valid, o);
+  if (lane == 0) nvalid[s] = valid;
+}
+
+__global__ void k_window_first(const int32_t* __restrict__ nvalid, const int32_t* __restrict__ wstart, int nwin,
+                               int32_t* __restrict__ wfirst) {
+  const int w = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= nwin) return;
+  const int a = wstart[w], b = wstart[w + 1];
+  int first = -1;
+  for (int c = a; c < b && first < 0; c += 32) {
+    const int s = c + lane;
+    const unsigned m = __ballot_sync(kFull, s < b && nvalid[s] > 0);
+    if (m) first = c + __ffs(m) - 1;
+  }
+  if (lane == 0) wfirst[w] = first;
+}
+
+// ---- segmented sort (ascending compare-exchange network, safe with a ragged tail) ----
+template <class K2>
+__device__ __forceinline__ bool less2(uint64_t a1, K2 a2, uint64_t b1, K2 b2) {
+  return a1 < b1 || (a1 == b1 && a2 < b2);
+}
+
+template <class K2, bool PAY>
+__global__ void k_classify(const int32_t* __restrict__ len, int64_t nseg, int32_t* __restrict__ lists,
+                           int32_t* __restrict__ counts) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nseg) return;
+  const int n = len[i];
+  if (n <= 1) return;
+  const int tier = (n <= 32) ? 0 : (n <= 2048 ? 1 : 2);
+  const int slot = atomicAdd(&counts[tier], 1);
+  lists[(int64_t)tier * nseg + slot] = (int32_t)i;
+}
+
+template <class K2, bool PAY>
+__global__ void k_sort_warp(uint64_t* __restrict__ k1, K2* __restrict__ k2, int32_t* __restrict__ pay,
+                            const int64_t* __restrict__ off, const int32_t* __restrict__ len,
+                            const int32_t* __restrict__ list, const int32_t* __restrict__ count) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int total = *count;
+  for (int64_t li = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; li < total; li += nwarps) {
+    const int seg = list[li];
+    const int64_t o = off[seg];
+    const int n = len[seg];
+    uint64_t a1 = ~0ull;
+    K2 a2 = (K2)~(K2)0;
+    int32_t ap = 0;
+    if (lane < n) {
+      a1 = k1[o + lane];
+      a2 = k2[o + lane];
+      if (PAY) ap = pay[o + lane];
+    }
+    for (int size = 2; size <= 32; size <<= 1) {
+      {
+        const int partner = lane ^ (size - 1);
+        const uint64_t b1 = __shfl_sync(kFull, a1, partner);
+        const K2 b2 = __shfl_sync(kFull, a2, partner);
+        const int32_t bp = __shfl_sync(kFull, ap, partner);
+        const bool lower = lane < partner;
+        const bool b_less = less2(b1, b2, a1, a2);
+        if (lower ? b_less : !b_less && (b1 != a1 || b2 != a2)) { a1 = b1; a2 = b2; ap = bp; }
+      }
+      for (int stride = size >> 2; stride > 0; stride >>= 1) {
+        const int partner = lane ^ stride;
+        const uint64_t b1 = __shfl_sync(kFull, a1, partner);
+        const K2 b2 = __shfl_sync(kFull, a2, partner);
+        const int32_t bp = __shfl_sync(kFull, ap, partner);
+        const bool lower = lane < partner;
+        const bool b_less = less2(b1, b2, a1, a2);
+        if (lower ? b_less : !b_less && (b1 != a1 || b2 != a2)) { a1 = b1; a2 = b2; ap = bp; }
+      }
+    }
+    if (lane < n) {
+      k1[o + lane] = a1;
+      k2[o + lane] = a2;
+      if (PAY) pay[o + lane] = ap;
+    }
+  }
+}
+
+template <class K2, bool PAY>
+__device__ __forceinline__ void cta_network(uint64_t* s1, K2* s2, int32_t* sp, int n) {
+  int np = 1;
+  while (np < n) np <<= 1;
+  for (int size = 2; size <= np; size <<= 1) {
+    for (int i = threadIdx.x; i < np / 2; i += blockDim.x) {  // flip stage
+      const int blk = i / (size / 2), r = i % (size / 2);
+      const int a = blk * size + r, b = blk * size + size - 1 - r;
+      if (b < n && less2(s1[b], s2[b], s1[a], s2[a])) {
+        const uint64_t t1 = s1[a]; s1[a] = s1[b]; s1[b] = t1;
+        const K2 t2 = s2[a]; s2[a] = s2[b]; s2[b] = t2;
+        if (PAY) { const int32_t tp = sp[a]; sp[a] = sp[b]; sp[b] = tp; }
+      }
+    }
+    __syncthreads();
+    for (int stride = size >> 2; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < np / 2; i += blockDim.x) {
+        const int blk = i / stride, r = i % stride;
+        const int a = blk * 2 * stride + r, b = a + stride;
+        if (b < n && less2(s1[b], s2[b], s1[a], s2[a])) {
+          const uint64_t t1 = s1[a]; s1[a] = s1[b]; s1[b] = t1;
+          const K2 t2 = s2[a]; s2[a] = s2[b]; s2[b] = t2;
+          if (PAY) { const int32_t tp = sp[a]; sp[a] = sp[b]; sp[b] = tp; }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+constexpr int kCtaSortCap = 2048;
+
+template <class K2, bool PAY>
+__global__ void __launch_bounds__(256) k_sort_cta(uint64_t* __restrict__ k1, K2* __restrict__ k2,
+                                                  int32_t* __restrict__ pay, const int64_t* __restrict__ off,
+                                                  const int32_t* __restrict__ len, const int32_t* __restrict__ list,
+                                                  const int32_t* __restrict__ count) {
+  __shared__ uint64_t s1[kCtaSortCap];
+  __shared__ K2 s2[kCtaSortCap];
+  __shared__ int32_t sp[PAY ? kCtaSortCap : 1];
+  const int total = *count;
+  for (int li = blockIdx.x; li < total; li += gridDim.x) {
+    const int seg = list[li];
+    const int64_t o = off[seg];
+    const int n = len[seg];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      s1[i] = k1[o + i];
+      s2[i] = k2[o + i];
+      if (PAY) sp[i] = pay[o + i];
+    }
+    __syncthreads();
+    cta_network<K2, PAY>(s1, s2, sp, n);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      k1[o + i] = s1[i];
+      k2[o + i] = s2[i];
+      if (PAY) pay[o + i] = sp[i];
+    }
+    __syncthreads();
+  }
+}
+
+template <class K2, bool PAY>
+__global__ void __launch_bounds__(1024) k_sort_global(uint64_t* __restrict__ k1, K2* __restrict__ k2,
+                                                      int32_t* __restrict__ pay, const int64_t* __restrict__ off,
+                                                      const int32_t* __restrict__ len,
+                                                      const int32_t* __restrict__ list,
+                                                      const int32_t* __restrict__ count) {
+  const int total = *count;
+  for (int li = blockIdx.x; li < total; li += gridDim.x) {
+    const int seg = list[li];
+    const int64_t o = off[seg];
+    cta_network<K2, PAY>(k1 + o, k2 + o, PAY ? pay + o : pay, len[seg]);
+    __syncthreads();
+  }
+}
+
+template <class K2, bool PAY>
+void seg_sort(Workspace& ws, uint64_t* k1, K2* k2, int32_t* pay, const int64_t* off, const int32_t* len,
+              int64_t nseg, cudaStream_t st, int tag) {
+  if (nseg <= 0) return;
+  const std::string t = "segsort" + std::to_string(tag);
+  int32_t* lists = ws.get<int32_t>(t + "l", 3 * nseg);
+  int32_t* counts = ws.get<int32_t>(t + "c", 3);
+  CLAST_CK(cudaMemsetAsync(counts, 0, 3 * sizeof(int32_t), st));
+  k_classify<K2, PAY><<<blocks_for(nseg, 256), 256, 0, st>>>(len, nseg, lists, counts);
+  CLAST_LAUNCHED();
+  k_sort_warp<K2, PAY><<<grid_cap((nseg * 32 + 255) / 256), 256, 0, st>>>(k1, k2, pay, off, len, lists, counts);
+  CLAST_LAUNCHED();
+  k_sort_cta<K2, PAY><<<grid_cap(nseg < 4096 ? nseg : 4096), 256, 0, st>>>(k1, k2, pay, off, len, lists + nseg,
+                                                                           counts + 1);
+  CLAST_LAUNCHED();
+  k_sort_global<K2, PAY><<<grid_cap(nseg < 1024 ? nseg : 1024), 1024, 0, st>>>(k1, k2, pay, off, len,
+                                                                                lists + 2 * nseg, counts + 2);
+  CLAST_LAUNCHED();
+}
+
+__global__ void k_to_i32(const int64_t* __restrict__ in, int64_t n, int32_t* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (int32_t)in[i];
+}
+
+// is "s" near its predecessor "p" (hasNotNearPair / hasNearPair, same strand)
+__device__ __forceinline__ bool near_pred(int tid, int tidx, int diag, int ptid, int ptidx, int pdiag,
+                                          int width, int gap) {
+  return tid == ptid && width >= tidx - ptidx && width >= ptidx - tidx && gap >= pdiag - diag;
+}
+
+__global__ void k_seed_filter(uint64_t* __restrict__ skey, uint32_t* __restrict__ sq,
+                              const int64_t* __restrict__ off, const int32_t* __restrict__ nvalid,
+                              const int32_t* __restrict__ wstart, int nwin, const int32_t* __restrict__ wfirst,
+                              int width, int gap, int64_t nstrands, int32_t* __restrict__ hcnt) {
+  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (s >= nstrands) return;
+  const int n = nvalid[s];
+  if (n == 0) {
+    if (lane == 0) hcnt[s] = 0;
+    return;
+  }
+  int lo = 0, hi = nwin;  // window of strand s
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (wstart[mid] <= s) lo = mid;
+    else hi = mid;
+  }
+  const bool wf = (wfirst[lo] == (int32_t)s);
+  const int64_t o = off[s];
+  const unsigned lt = lanemask_lt();
+  int ptid = 0, ptidx = 0, pdiag = 0;          // element j-1 of the previous chunk
+  bool have_surv = false;
+  int stid = 0, stidx = 0, sdiag = 0;          // last A8 survivor so far
+  int64_t out = o;
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    const int j = c0 + lane;
+    const bool in = j < n;
+    uint64_t k = 0;
+    uint32_t qi = 0;
+    if (in) {
+      k = skey[o + j];
+      qi = sq[o + j];
+    }
+    const int tid = (int)(k >> 32);
+    const int diag = (int)((uint32_t)k ^ 0x80000000u);
+    const int tidx = diag + (int)qi;
+    int ptid_l = __shfl_up_sync(kFull, tid, 1);
+    int ptidx_l = __shfl_up_sync(kFull, tidx, 1);
+    int pdiag_l = __shfl_up_sync(kFull, diag, 1);
+    if (lane == 0) { ptid_l = ptid; ptidx_l = ptidx; pdiag_l = pdiag; }
+    bool keep8 = false;
+    if (in) keep8 = (j == 0) ? wf : near_pred(tid, tidx, diag, ptid_l, ptidx_l, pdiag_l, width, gap);
+    const unsigned b8 = __ballot_sync(kFull, keep8);
+    const unsigned below = b8 & lt;
+    const int src = below ? 31 - __clz(below) : 0;
+    const int qtid = __shfl_sync(kFull, tid, src);
+    const int qtidx = __shfl_sync(kFull, tidx, src);
+    const int qdiag = __shfl_sync(kFull, diag, src);
+    bool keep9 = keep8;
+    if (keep8) {
+      if (below) keep9 = !near_pred(tid, tidx, diag, qtid, qtidx, qdiag, width, gap);
+      else if (have_surv) keep9 = !near_pred(tid, tidx, diag, stid, stidx, sdiag, width, gap);
+    }
+    const unsigned b9 = __ballot_sync(kFull, keep9);
+    if (keep9) {
+      const int64_t w = out + __popc(b9 & lt);
+      skey[w] = k;
+      sq[w] = qi;
+    }
+    out += __popc(b9);
+    ptid = __shfl_sync(kFull, tid, 31);
+    ptidx = __shfl_sync(kFull, tidx, 31);
+    pdiag = __shfl_sync(kFull, diag, 31);
+    if (b8) {
+      const int last = 31 - __clz(b8);
+      stid = __shfl_sync(kFull, tid, last);
+      stidx = __shfl_sync(kFull, tidx, last);
+      sdiag = __shfl_sync(kFull, diag, last);
+      have_surv = true;
+    }
+  }
+  if (lane == 0) hcnt[s] = (int32_t)(out - o);
+}
+
+__global__ void k_gather_hits(const uint64_t* __restrict__ skey, const uint32_t* __restrict__ sq,
+                              const int64_t* __restrict__ off, const int32_t* __restrict__ hcnt,
+                              const int64_t* __restrict__ hoff, int64_t nstrands, uint64_t* __restrict__ hk,
+                              int32_t* __restrict__ hq, int32_t* __restrict__ hs) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nstrands) return;
+  const int n = hcnt[s];
+  const int64_t a = off[s], b = hoff[s];
+  for (int i = 0; i < n; ++i) {
+    hk[b + i] = skey[a + i];
+    hq[b + i] = (int32_t)sq[a + i];
+    hs[b + i] = (int32_t)s;
+  }
+}
+
+// ------------------------------------------------------------------------
+// banded DP
+// ------------------------------------------------------------------------
+// POINT_MATRIX / MATCH_COUNTER (krnlMatrix.cuh:11-67) as a rule over letter
+// classes, packed as (point << 16) | (match & 0xffff) at [target*32 + query].
+__device__ __forceinline__ int letter_group(int c) {  // 0..3 ACGT, 4 scored letter, 5 "-1" letter, 6 X
+  switch (c) {
+    case 0: return 0;   // A
+    case 2: return 1;   // C
+    case 6: return 2;   // G
+    case 19: return 3;  // T
+    case 23: return 6;  // X
+    case 4: case 5: case 8: case 9: case 11: case 14: case 15: case 16: case 25: return 5;  // E F I J L O P Q Z
+    default: return 4;
+  }
+}
+
+__device__ __forceinline__ int packed_score(int t, int q) {
+  const int a = letter_group(t < 26 ? t : kNClass), b = letter_group(q < 26 ? q : kNClass);
+  int point, match;
+  if (a == 6 || b == 6) { point = -1000; match = -1000; }
+  else if (a == 5 || b == 5) { point = -1; match = -1; }
+  else if (a == b && a < 4) { point = 1; match = 1; }
+  else { point = -3; match = 0; }
+  return (int)((unsigned)point << 16) | (match & 0xffff);
+}
+
+template <int GAP, bool LOCAL, bool BACKWARD>
+__device__ __forceinline__ void dp_pass(const int* __restrict__ tab, const char* __restrict__ tb, int64_t tstart,
+                                        int tlen, const char* __restrict__ qb, int64_t qfirst, int rows, int tidx,
+                                        int l, int& move, int& endp, int& best, int& best_m) {
+  constexpr int W = 2 * GAP + 1;
+  constexpr int kBotS = (GAP + 1) * kGapExtend + kGapOpen;
+  constexpr int kBotV = kBotS + kGapOpen;
+  int S[W], V[W], M[W], tc[W];
+#pragma unroll
+  for (int c = 0; c < W; ++c) {  // initTempNodeArray, krnlAlignment.cu:6-38 (band rows 1..W)
+    const int r = c + 1;
+    if (r < GAP + 1) { S[c] = kMarginScore; V[c] = kMarginScore; M[c] = kMarginScore; }
+    else if (r == GAP + 1) { S[c] = 0; V[c] = kGapOpen; M[c] = 0; }
+    else { S[c] = (r - GAP - 1) * kGapExtend + kGapOpen; V[c] = S[c] + kGapOpen; M[c] = 0; }
+    const int64_t ib = BACKWARD ? (int64_t)tidx + l - GAP + c : (int64_t)tidx + GAP - c - 1;
+    const bool bad = BACKWARD ? (ib >= tlen) : (ib < 0);
+    tc[c] = (bad ? kBadClass : base_class(tb[tstart + ib])) << 5;
+  }
+  int bs = 0, bm = 0, calc = -1, ep = GAP;
+  for (int q = 0; q < rows; ++q) {
+    const int qc = base_class(BACKWARD ? qb[qfirst + q] : qb[qfirst - q]);
+    int hS = kMarginScore, hH = kMarginScore, hM = kMarginScore;
+#pragma unroll
+    for (int c = 0; c < W; ++c) {  // calcutlateCell, krnlAlignment.cu:42-77
+      const int vS = (c + 1 < W) ? S[(c + 1) % W] : kBotS;
+      const int vV = (c + 1 < W) ? V[(c + 1) % W] : kBotV;
+      const int vM = (c + 1 < W) ? M[(c + 1) % W] : 0;
+      const int nV = max(vS + (kGapOpen + kGapExtend), vV + kGapExtend);
+      const int nH = max(hS + (kGapOpen + kGapExtend), hH + kGapExtend);
+      const int w = tab[tc[c] | qc];
+      const int pt = S[c] + (w >> 16);
+      const int mx = max(nV, nH);
+      const int side_m = (nV > nH) ? vM : hM;
+      const int nM = (pt > mx) ? (M[c] + ((w << 16) >> 16)) : side_m;
+      const int nS = max(pt, mx);
+      S[c] = nS;
+      V[c] = nV;
+      M[c] = nM;
+      hS = nS;
+      hH = nH;
+      hM = nM;
+      if (LOCAL) {
+        if (bs < nS) { bs = nS; bm = nM; calc = q; ep = c; }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < W - 1; ++c) tc[c] = tc[c + 1];
+    const int64_t ib = BACKWARD ? (int64_t)tidx + l + GAP + q + 1 : (int64_t)tidx - GAP - q - 2;
+    const bool bad = BACKWARD ? (ib >= tlen) : (ib < 0);
+    tc[W - 1] = (bad ? kBadClass : base_class(tb[tstart + ib])) << 5;
+  }
+  if (!LOCAL) {  // select end node, krnlAlignment.cu:170-185
+    bs = kMarginScore;
+    bm = kMarginScore;
+    ep = -1;
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+      if (bs < S[c]) { bs = S[c]; bm = M[c]; ep = c; }
+    move = rows;
+  } else {
+    move = calc + 1;
+  }
+  endp = ep - GAP;
+  best = bs;
+  best_m = bm;
+}
+
+struct DpKernelArgs {
+  TargetView t;
+  QueryView q;
+  const uint64_t* hk;
+  const int32_t* hq;
+  const int32_t* hs;
+  int64_t n;
+  DpParams p;
+  DpOut o;
+};
+
+template <int GAP, bool LOCAL>
+__global__ void __launch_bounds__(128) k_banded_dp(DpKernelArgs a) {
+  __shared__ int tab[32 * 32];
+  for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) tab[i] = packed_score(i >> 5, i & 31);
+  __syncthreads();
+  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= a.n) return;
+  const uint64_t k = a.hk[h];
+  const int qidx = a.hq[h];
+  const int s = a.hs[h];
+  const int tid = (int)(k >> 32);
+  const int tidx = (int)((uint32_t)k ^ 0x80000000u) + qidx;
+  const int64_t tstart = a.t.gateway[tid];
+  const int tlen = a.t.lengths[tid];
+  const int64_t qstart = a.q.start[s];
+  const int qlen = a.q.len[s];
+  const int l = a.p.l;
+  int t_hl = l, q_hl = l, match = l, score = l;  // CDeviceHitList.cu:283-286
+  int o_tidx = tidx, o_qidx = qidx;
+  int move, endp, best, best_m;
+  const int rows_b = qlen - (qidx + l);  // globalAlignBackward / localAlignBackward
+  dp_pass<GAP, LOCAL, true>(tab, a.t.bases, tstart, tlen, a.q.bases, qstart + qidx + l, rows_b, tidx, l, move,
+                            endp, best, best_m);
+  if (rows_b != 0) {
+    t_hl += move + endp;
+    q_hl += move;
+    match += best_m;
+    score += best;
+  }
+  const int rows_f = qidx;  // globalAlignForward / localAlignForward
+  dp_pass<GAP, LOCAL, false>(tab, a.t.bases, tstart, tlen, a.q.bases, qstart + qidx - 1, rows_f, tidx, l, move,
+                             endp, best, best_m);
+  if (rows_f != 0) {
+    o_tidx -= move + endp;
+    o_qidx -= move;
+    t_hl += move + endp;
+    q_hl += move;
+    match += best_m;
+    score += best;
+  }
+  // calculateEvalue, krnlCalculateEvalue.cu:21 (same operation order)
+  const double e = a.p.K * a.p.total_db * (double)qlen * exp(-a.p.lambda * (double)score);
+  const bool keep = !(a.p.cutoff != -1.0 && a.p.cutoff < e) && !(l + a.p.stride > q_hl);
+  a.o.t_idx[h] = o_tidx;
+  a.o.q_idx[h] = o_qidx;
+  a.o.t_len[h] = t_hl;
+  a.o.q_len[h] = q_hl;
+  a.o.match[h] = match;
+  a.o.score[h] = score;
+  a.o.evalue[h] = e;
+  a.o.keep[h] = keep ? 1 : 0;
+}
+
+template <int GAP>
+void launch_dp_gap(const DpKernelArgs& a, bool local, cudaStream_t st) {
+  const int threads = 128;
+  const unsigned grid = (unsigned)((a.n + threads - 1) / threads);
+  if (local) k_banded_dp<GAP, true><<<grid, threads, 0, st>>>(a);
+  else k_banded_dp<GAP, false><<<grid, threads, 0, st>>>(a);
+  CLAST_LAUNCHED();
+}
+
+// ------------------------------------------------------------------------
+// final per-read order
+// ------------------------------------------------------------------------
+__global__ void k_final_keys(const uint64_t* __restrict__ hk, const int32_t* __restrict__ hq,
+                             const int32_t* __restrict__ hs, DpOut o, int64_t n, uint64_t* __restrict__ k1,
+                             uint64_t* __restrict__ k2, int32_t* __restrict__ idx) {
+  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= n) return;
+  if (!o.keep[h]) {  // filtered hits sort after every kept one
+    k1[h] = ~0ull;
+    k2[h] = ~0ull;
+    idx[h] = (int32_t)h;
+    return;
+  }
+  const uint64_t k = hk[h];
+  const int qidx = hq[h];
+  const int tid = (int)(k >> 32);
+  const int tidx = (int)((uint32_t)k ^ 0x80000000u) + qidx;
+  // (score desc, seed qIdx desc, strand, target sequence, seed tIdx): the order the
+  // stable sorts of alignmentHits (by rows desc, then qIdx desc) and
+  // resultSorting (qID/2 asc, score desc) leave hits of one read in.
+  const uint32_t a1 = (uint32_t)((int64_t)INT_MAX - (int64_t)o.score[h]);
+  const uint32_t a2 = (uint32_t)((int64_t)INT_MAX - (int64_t)qidx);
+  k1[h] = ((uint64_t)a1 << 32) | a2;
+  k2[h] = ((uint64_t)(hs[h] & 1) << 62) | ((uint64_t)(uint32_t)tid << 31) | (uint64_t)(uint32_t)tidx;
+  idx[h] = (int32_t)h;
+}
+
+__global__ void k_read_ranges(const int64_t* __restrict__ hoff, int64_t n_reads, int64_t* __restrict__ roff,
+                              int32_t* __restrict__ rlen) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_reads) return;
+  roff[r] = hoff[2 * r];
+  rlen[r] = (int32_t)(hoff[2 * r + 2] - hoff[2 * r]);
+}
+
+// Duplicate removal within one read (deleteHits_duplicateResult: a hit equal
+// in (tID, tIdx, qID, qIdx) to its predecessor in result order is dropped).
+__global__ void k_final_dedupe(const uint64_t* __restrict__ k1, const int32_t* __restrict__ idx,
+                               const uint64_t* __restrict__ hk, const int32_t* __restrict__ hs, DpOut o,
+                               const int64_t* __restrict__ roff, const int32_t* __restrict__ rlen,
+                               int64_t n_reads, int32_t* __restrict__ fcnt, int32_t* __restrict__ fsel) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_reads) return;
+  const int64_t a = roff[r];
+  const int n = rlen[r];
+  int cnt = 0;
+  int ptid = 0, ptidx = 0, ps = 0, pqidx = 0;
+  for (int j = 0; j < n; ++j) {
+    if (k1[a + j] == ~0ull) break;  // the filtered hits
+    const int h = idx[a + j];
+    const int tid = (int)(hk[h] >> 32);
+    const int tidx = o.t_idx[h], qidx = o.q_idx[h], s = hs[h];
+    const bool dup = j > 0 && tid == ptid && tidx == ptidx && s == ps && qidx == pqidx;
+    if (!dup) fsel[a + cnt++] = h;
+    ptid = tid; ptidx = tidx; ps = s; pqidx = qidx;
+  }
+  fcnt[r] = cnt;
+}
+
+__global__ void k_final_compact(const int32_t* __restrict__ fsel, const int64_t* __restrict__ roff,
+                                const int32_t* __restrict__ fcnt, const int64_t* __restrict__ foff,
+                                int64_t n_reads, const uint64_t* __restrict__ hk, const int32_t* __restrict__ hs,
+                                DpOut o, int32_t t_first, int32_t q_first, FinalOut out) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_reads) return;
+  const int64_t a = roff[r], b = foff[r];
+  const int n = fcnt[r];
+  for (int j = 0; j < n; ++j) {
+    const int h = fsel[a + j];
+    const int64_t w = b + j;
+    out.t_id[w] = t_first + (int32_t)(hk[h] >> 32);
+    out.t_idx[w] = o.t_idx[h];
+    out.q_id[w] = q_first + hs[h];
+    out.q_idx[w] = o.q_idx[h];
+    out.t_len[w] = o.t_len[h];
+    out.q_len[w] = o.q_len[h];
+    out.match[w] = o.match[h];
+    out.score[w] = o.score[h];
+    out.evalue[w] = o.evalue[h];
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------
+// launch wrappers
+// ------------------------------------------------------------------------
+void scan_i32(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st, int level) {
+  scan_impl<int32_t>(ws, in, n, out, st, level);
+}
+void scan_i64(Workspace& ws, const int64_t* in, int64_t n, int64_t* out, cudaStream_t st, int level) {
+  scan_impl<int64_t>(ws, in, n, out, st, level);
+}
+
+void pack_bases(const char* bases, int64_t n, uint64_t* packed, uint64_t* nmask, cudaStream_t st) {
+  const int64_t nwords = (n + 63) / 64 + 1;  // one extra word so kmer_at may read w+1
+  k_pack<<<blocks_for(nwords, 256), 256, 0, st>>>(bases, n, packed, nmask, nwords);
+  CLAST_LAUNCHED();
+}
+
+void build_strands(const char* reads, const int64_t* offsets, int64_t n_reads, int64_t n_bases, char* strands,
+                   int64_t* strand_start, int32_t* strand_len, cudaStream_t st) {
+  if (n_reads <= 0) return;
+  k_strand_meta<<<blocks_for(n_reads, 256), 256, 0, st>>>(offsets, n_reads, strand_start, strand_len);
+  CLAST_LAUNCHED();
+  if (n_bases > 0) {
+    k_strands<<<blocks_for(n_bases, 256), 256, 0, st>>>(reads, offsets, n_reads, n_bases, strands);
+    CLAST_LAUNCHED();
+  }
+}
+
+void sample_keys(const uint64_t* packed, const uint64_t* nmask, int64_t n_samples, int stride, int l,
+                 uint64_t* keys, int32_t* vals, cudaStream_t st) {
+  if (n_samples <= 0) return;
+  k_sample_keys<<<blocks_for(n_samples, 256), 256, 0, st>>>(packed, nmask, n_samples, stride, l, keys, vals);
+  CLAST_LAUNCHED();
+}
+
+void radix_sort_pairs(Workspace& ws, uint64_t* keys, int32_t* vals, uint64_t* keys_alt, int32_t* vals_alt,
+                      int64_t n, int bits, cudaStream_t st) {
+  if (n <= 1) return;
+  const int nblocks = (int)((n + kRsTile - 1) / kRsTile);
+  uint32_t* hist = ws.get<uint32_t>("rs_hist", (size_t)256 * nblocks);
+  int64_t* offs = ws.get<int64_t>("rs_offs", (size_t)256 * nblocks + 1);
+  uint64_t* ka = keys;
+  int32_t* va = vals;
+  uint64_t* kb = keys_alt;
+  int32_t* vb = vals_alt;
+  int passes = 0;
+  for (int shift = 0; shift < bits; shift += 8) {
+    k_radix_hist<<<nblocks, kRsThreads, 0, st>>>(ka, n, shift, hist, nblocks);
+    CLAST_LAUNCHED();
+    scan_impl<uint32_t>(ws, hist, (int64_t)256 * nblocks, offs, st, 0);
+    k_radix_scatter<<<nblocks, kRsThreads, 0, st>>>(ka, va, kb, vb, n, shift, offs, nblocks);
+    CLAST_LAUNCHED();
+    std::swap(ka, kb);
+    std::swap(va, vb);
+    ++passes;
+  }
+  if (passes & 1) {
+    CLAST_CK(cudaMemcpyAsync(keys, ka, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+    CLAST_CK(cudaMemcpyAsync(vals, va, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+  }
+}
+
+void count_below(const uint64_t* keys, int64_t n, uint64_t bound, int64_t* out, cudaStream_t st) {
+  k_count_below<<<1, 1, 0, st>>>(keys, n, bound, out);
+  CLAST_LAUNCHED();
+}
+
+void index_heads(const uint64_t* keys, int64_t nv, int32_t* head, cudaStream_t st) {
+  if (nv <= 0) return;
+  k_index_heads<<<blocks_for(nv, 256), 256, 0, st>>>(keys, nv, head);
+  CLAST_LAUNCHED();
+}
+void index_unique(const uint64_t* keys, const int32_t* head, const int64_t* hpos, int64_t nv, uint64_t* ukeys,
+                  int64_t* ufirst, cudaStream_t st) {
+  k_index_unique<<<blocks_for(nv > 0 ? nv : 1, 256), 256, 0, st>>>(keys, head, hpos, nv, ukeys, ufirst);
+  CLAST_LAUNCHED();
+}
+void index_keep(const int32_t* vals, const int64_t* hpos, const int64_t* ufirst, int64_t nv, int stride, int l,
+                int cut, const int32_t* gateway, const int32_t* lengths, int nseqs, int32_t* keep, int2* resolved,
+                cudaStream_t st) {
+  if (nv <= 0) return;
+  k_index_keep<<<blocks_for(nv, 256), 256, 0, st>>>(vals, hpos, ufirst, nv, stride, l, cut, gateway, lengths,
+                                                    nseqs, keep, resolved);
+  CLAST_LAUNCHED();
+}
+void index_entries(const int32_t* keep, const int64_t* kpos, const int2* resolved, int64_t nv, int2* entries,
+                   cudaStream_t st) {
+  if (nv <= 0) return;
+  k_index_entries<<<blocks_for(nv, 256), 256, 0, st>>>(keep, kpos, resolved, nv, entries);
+  CLAST_LAUNCHED();
+}
+void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n_unique, int32_t* ustart, int32_t* ucnt,
+                   cudaStream_t st) {
+  if (n_unique <= 0) return;
+  k_index_buckets<<<blocks_for(n_unique, 256), 256, 0, st>>>(ufirst, kpos, n_unique, ustart, ucnt);
+  CLAST_LAUNCHED();
+}
+void index_directory(const uint64_t* ukeys, int64_t n_unique, int shift, int dir_bits, uint32_t* dir,
+                     cudaStream_t st) {
+  const int64_t nslots = 1ll << dir_bits;
+  k_index_dir<<<blocks_for(nslots + 1, 256), 256, 0, st>>>(ukeys, n_unique, shift, nslots, dir);
+  CLAST_LAUNCHED();
+}
+
+void seed_count(const QueryView& q, const IndexView& ix, int64_t* cnt, cudaStream_t st) {
+  if (q.nstrands <= 0) return;
+  k_seed_count<<<blocks_for((int64_t)q.nstrands * 32, 256), 256, 0, st>>>(q, ix, cnt);
+  CLAST_LAUNCHED();
+}
+void seed_write(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
+                const int64_t* off, uint64_t* skey, uint32_t* sq, int32_t* nvalid, cudaStream_t st) {
+  if (q.nstrands <= 0) return;
+  k_seed_write<<<blocks_for((int64_t)q.nstrands * 32, 256), 256, 0, st>>>(q, ix, t, gap, local, off, skey, sq,
+                                                                           nvalid);
+  CLAST_LAUNCHED();
+}
+void window_first(const int32_t* nvalid, const int32_t* win_start, int n_windows, int32_t* win_first,
+                  cudaStream_t st) {
+  if (n_windows <= 0) return;
+  k_window_first<<<blocks_for((int64_t)n_windows * 32, 256), 256, 0, st>>>(nvalid, win_start, n_windows,
+                                                                            win_first);
+  CLAST_LAUNCHED();
+}
+void segmented_sort_u32(Workspace& ws, uint64_t* k1, uint32_t* k2, const int64_t* off, const int32_t* len,
+                        int64_t n_segments, cudaStream_t st, int tag) {
+  seg_sort<uint32_t, false>(ws, k1, k2, nullptr, off, len, n_segments, st, tag);
+}
+void segmented_sort_u64(Workspace& ws, uint64_t* k1, uint64_t* k2, int32_t* payload, const int64_t* off,
+                        const int32_t* len, int64_t n_segments, cudaStream_t st, int tag) {
+  seg_sort<uint64_t, true>(ws, k1, k2, payload, off, len, n_segments, st, tag);
+}
+void to_i32(const int64_t* in, int64_t n, int32_t* out, cudaStream_t st) {
+  if (n <= 0) return;
+  k_to_i32<<<blocks_for(n, 256), 256, 0, st>>>(in, n, out);
+  CLAST_LAUNCHED();
+}
+void seed_filter(uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t* nvalid, const int32_t* win_start,
+                 int n_windows, const int32_t* win_first, int width, int gap, int64_t nstrands, int32_t* hcnt,
+                 cudaStream_t st) {
+  if (nstrands <= 0) return;
+  k_seed_filter<<<blocks_for(nstrands * 32, 256), 256, 0, st>>>(skey, sq, off, nvalid, win_start, n_windows,
+                                                                 win_first, width, gap, nstrands, hcnt);
+  CLAST_LAUNCHED();
+}
+void gather_hits(const uint64_t* skey, const uint32_t* sq, const int64_t* off, const int32_t* hcnt,
+                 const int64_t* hoff, int64_t nstrands, uint64_t* hk, int32_t* hq, int32_t* hs, cudaStream_t st) {
+  if (nstrands <= 0) return;
+  k_gather_hits<<<blocks_for(nstrands, 256), 256, 0, st>>>(skey, sq, off, hcnt, hoff, nstrands, hk, hq, hs);
+  CLAST_LAUNCHED();
+}
+
+void banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq, const int32_t* hs,
+               int64_t n_hits, const DpParams& p, const DpOut& o, cudaStream_t st) {
+  if (n_hits <= 0) return;
+  DpKernelArgs a{t, q, hk, hq, hs, n_hits, p, o};
+  const bool local = p.local != 0;
+  switch (p.gap) {
+    case 2: launch_dp_gap<2>(a, local, st); break;
+    case 3: launch_dp_gap<3>(a, local, st); break;
+    case 4: launch_dp_gap<4>(a, local, st); break;
+    case 5: launch_dp_gap<5>(a, local, st); break;
+    case 6: launch_dp_gap<6>(a, local, st); break;
+    case 7: launch_dp_gap<7>(a, local, st); break;
+    case 8: launch_dp_gap<8>(a, local, st); break;
+    case 9: launch_dp_gap<9>(a, local, st); break;
+    case 10: launch_dp_gap<10>(a, local, st); break;
+    case 11: launch_dp_gap<11>(a, local, st); break;
+    case 12: launch_dp_gap<12>(a, local, st); break;
+    case 13: launch_dp_gap<13>(a, local, st); break;
+    case 14: launch_dp_gap<14>(a, local, st); break;
+    case 15: launch_dp_gap<15>(a, local, st); break;
+    case 16: launch_dp_gap<16>(a, local, st); break;
+    default: throw std::invalid_argument("gap out of range 2..16");
+  }
+}
+
+void final_keys(const uint64_t* hk, const int32_t* hq, const int32_t* hs, const DpOut& o, int64_t n_hits,
+                uint64_t* k1, uint64_t* k2, int32_t* idx, cudaStream_t st) {
+  if (n_hits <= 0) return;
+  k_final_keys<<<blocks_for(n_hits, 256), 256, 0, st>>>(hk, hq, hs, o, n_hits, k1, k2, idx);
+  CLAST_LAUNCHED();
+}
+void read_ranges(const int64_t* hoff, int64_t n_reads, int64_t* roff, int32_t* rlen, cudaStream_t st) {
+  if (n_reads <= 0) return;
+  k_read_ranges<<<blocks_for(n_reads, 256), 256, 0, st>>>(hoff, n_reads, roff, rlen);
+  CLAST_LAUNCHED();
+}
+void final_dedupe(const uint64_t* k1, const uint64_t* /*k2*/, const int32_t* idx, const uint64_t* hk,
+                  const int32_t* hs, const DpOut& o, const int64_t* roff, const int32_t* rlen, int64_t n_reads,
+                  int32_t* fcnt, int32_t* fsel, cudaStream_t st) {
+  if (n_reads <= 0) return;
+  k_final_dedupe<<<blocks_for(n_reads, 128), 128, 0, st>>>(k1, idx, hk, hs, o, roff, rlen, n_reads, fcnt, fsel);
+  CLAST_LAUNCHED();
+}
+void final_compact(const int32_t* fsel, const int64_t* roff, const int32_t* fcnt, const int64_t* foff,
+                   int64_t n_reads, const uint64_t* hk, const int32_t* hs, const DpOut& o, int32_t t_first,
+                   int32_t q_first, const FinalOut& out, cudaStream_t st) {
+  if (n_reads <= 0) return;
+  k_final_compact<<<blocks_for(n_reads, 128), 128, 0, st>>>(fsel, roff, fcnt, foff, n_reads, hk, hs, o, t_first,
+                                                             q_first, out);
+  CLAST_LAUNCHED();
+}
+
+}  // namespace clast

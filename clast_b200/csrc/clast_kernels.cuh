@@ -1,0 +1,101 @@
+// clast_kernels.cuh -- launch wrappers of the sm_100a kernels (clast_kernels.cu).
+// Every wrapper enqueues on `st` and returns immediately; sizes are element counts.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "clast_device.cuh"
+
+namespace clast {
+
+struct Workspace;  // device scratch pool (clast_engine.cu)
+
+// out[0..n] = exclusive prefix sums of in[0..n) (out[n] = total).
+void scan_i32(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st, int level = 0);
+void scan_i64(Workspace& ws, const int64_t* in, int64_t n, int64_t* out, cudaStream_t st, int level = 0);
+
+// 2-bit codes (32 bases per word) and non-ACGT mask (64 per word) of bases[0..n);
+// positions >= n count as 'N'.  packed needs ceil(n/32)+2 words, nmask ceil(n/64)+2.
+void pack_bases(const char* bases, int64_t n, uint64_t* packed, uint64_t* nmask, cudaStream_t st);
+
+// Query strands of n_reads one-strand reads: strand 2r = read r, strand 2r+1 its
+// reverse complement (utilReverseSeq.cpp:3-19), laid out back to back.
+void build_strands(const char* reads, const int64_t* offsets, int64_t n_reads, int64_t n_bases,
+                   char* strands, int64_t* strand_start, int32_t* strand_len, cudaStream_t st);
+
+// ---- index of one target window (CDeviceHashTable.cu:20-174) ----
+// Sampled keys at window positions j*stride; invalid k-mers get key 1<<(2l).
+void sample_keys(const uint64_t* packed, const uint64_t* nmask, int64_t n_samples, int stride, int l,
+                 uint64_t* keys, int32_t* vals, cudaStream_t st);
+// Stable LSD radix sort of (keys, vals) on the low `bits` key bits; the result
+// ends in (keys, vals) (alt buffers are scratch).
+void radix_sort_pairs(Workspace& ws, uint64_t* keys, int32_t* vals, uint64_t* keys_alt, int32_t* vals_alt,
+                      int64_t n, int bits, cudaStream_t st);
+// *out = number of keys < bound in the sorted array keys[0..n)
+void count_below(const uint64_t* keys, int64_t n, uint64_t bound, int64_t* out, cudaStream_t st);
+void index_heads(const uint64_t* keys, int64_t nv, int32_t* head, cudaStream_t st);
+void index_unique(const uint64_t* keys, const int32_t* head, const int64_t* hpos, int64_t nv,
+                  uint64_t* ukeys, int64_t* ufirst, cudaStream_t st);
+void index_keep(const int32_t* vals, const int64_t* hpos, const int64_t* ufirst, int64_t nv, int stride,
+                int l, int cut, const int32_t* gateway, const int32_t* lengths, int nseqs,
+                int32_t* keep, int2* resolved, cudaStream_t st);
+void index_entries(const int32_t* keep, const int64_t* kpos, const int2* resolved, int64_t nv,
+                   int2* entries, cudaStream_t st);
+void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n_unique, int32_t* ustart,
+                   int32_t* ucnt, cudaStream_t st);
+void index_directory(const uint64_t* ukeys, int64_t n_unique, int shift, int dir_bits, uint32_t* dir,
+                     cudaStream_t st);
+
+// ---- seeds (CDeviceHitList_createRawSeedList.cu, _deleteSeeds*.cu, _sortSeeds.cu) ----
+void seed_count(const QueryView& q, const IndexView& ix, int64_t* cnt, cudaStream_t st);
+void seed_write(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
+                const int64_t* off, uint64_t* skey, uint32_t* sq, int32_t* nvalid, cudaStream_t st);
+void window_first(const int32_t* nvalid, const int32_t* win_start, int n_windows, int32_t* win_first,
+                  cudaStream_t st);
+
+// Sorts every segment [off[i], off[i]+len[i]) of (k1, k2[, payload]) ascending by
+// (k1, k2).  Segments of <= 32 are sorted by one warp in registers, <= 2048 by one
+// CTA in shared memory, longer ones by one CTA in global memory.
+void segmented_sort_u32(Workspace& ws, uint64_t* k1, uint32_t* k2, const int64_t* off, const int32_t* len,
+                        int64_t n_segments, cudaStream_t st, int tag);
+void segmented_sort_u64(Workspace& ws, uint64_t* k1, uint64_t* k2, int32_t* payload, const int64_t* off,
+                        const int32_t* len, int64_t n_segments, cudaStream_t st, int tag);
+// seed counts per strand (int32) from the int64 count array
+void to_i32(const int64_t* in, int64_t n, int32_t* out, cudaStream_t st);
+
+void seed_filter(uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t* nvalid,
+                 const int32_t* win_start, int n_windows, const int32_t* win_first, int width, int gap,
+                 int64_t nstrands, int32_t* hcnt, cudaStream_t st);
+void gather_hits(const uint64_t* skey, const uint32_t* sq, const int64_t* off, const int32_t* hcnt,
+                 const int64_t* hoff, int64_t nstrands, uint64_t* hk, int32_t* hq, int32_t* hs,
+                 cudaStream_t st);
+
+// ---- banded DP + E-value (krnlAlignment.cu, krnlCalculateEvalue.cu) ----
+struct DpOut {
+  int32_t* t_idx; int32_t* q_idx; int32_t* t_len; int32_t* q_len; int32_t* match; int32_t* score;
+  double* evalue; uint8_t* keep;
+};
+struct DpParams {
+  int l, stride, gap, local;
+  double cutoff, total_db, K, lambda;
+};
+void banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq,
+               const int32_t* hs, int64_t n_hits, const DpParams& p, const DpOut& o, cudaStream_t st);
+
+// ---- per-read result order and duplicate removal (utilResultSorting.cuh, CDeviceHitList.cu:32-128) ----
+void final_keys(const uint64_t* hk, const int32_t* hq, const int32_t* hs, const DpOut& o, int64_t n_hits,
+                uint64_t* k1, uint64_t* k2, int32_t* idx, cudaStream_t st);
+void read_ranges(const int64_t* hoff, int64_t n_reads, int64_t* roff, int32_t* rlen, cudaStream_t st);
+void final_dedupe(const uint64_t* k1, const uint64_t* k2, const int32_t* idx, const uint64_t* hk,
+                  const int32_t* hs, const DpOut& o, const int64_t* roff, const int32_t* rlen,
+                  int64_t n_reads, int32_t* fcnt, int32_t* fsel, cudaStream_t st);
+struct FinalOut {
+  int32_t* t_id; int32_t* t_idx; int32_t* q_id; int32_t* q_idx; int32_t* t_len; int32_t* q_len;
+  int32_t* match; int32_t* score; double* evalue;
+};
+void final_compact(const int32_t* fsel, const int64_t* roff, const int32_t* fcnt, const int64_t* foff,
+                   int64_t n_reads, const uint64_t* hk, const int32_t* hs, const DpOut& o, int32_t t_first,
+                   int32_t q_first, const FinalOut& out, cudaStream_t st);
+
+}  // namespace clast

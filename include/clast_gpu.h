@@ -1,0 +1,156 @@
+/*
+ * clast_gpu.h -- C ABI of the B200 seed-and-extend engine (libclast_b200.so).
+ *
+ * The reference (masayano/CLAST) has no plugin API; its in-process seam is
+ * the trio of classes its scheduler constructs for every (target window,
+ * query window) pair (CHostSchedular.cu:141,169,187,196):
+ *
+ *   CDeviceHashTable(setting, targetList, t_begin, t_end)      CDeviceHashTable.cuh:17-21
+ *   CDeviceSeqList_query(setting, queryList, q_begin, q_end)    CDeviceSeqList_query.cuh:14-18
+ *   CDeviceHitList(setting, hashTable, query, t_begin, q_begin) CDeviceHitList.cuh:23-28
+ *     + CDeviceHitList::getResult(holder)                        CDeviceHitList.cuh:29
+ *
+ * clast_index_build() replaces the first, clast_search() the other two.  The
+ * whole-job entry points clast_targets_create() / clast_map() replace
+ * CHostMapper::getResult + CHostSchedular::search + CHostResultHolder::fixResult
+ * (CHostMapper.cu:53-71, CHostSchedular.cu:43-130, CHostResultHolder.cu:75-128)
+ * for every RAM load at once, keeping the target indexes resident in HBM.
+ *
+ * Conventions: every call returns 0 on success or a negative clast_status;
+ * nothing aborts or throws across the ABI; the message of the last failure is
+ * clast_last_error(ctx).  One context per host thread.  Arrays are plain host
+ * pointers; results are allocated by the library and released with
+ * clast_hits_free() / clast_map_result_free().
+ */
+#ifndef CLAST_GPU_H_
+#define CLAST_GPU_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum clast_status {
+  CLAST_OK = 0,
+  CLAST_ERR_ARG = -1,      /* invalid argument (sizes, parameter ranges) */
+  CLAST_ERR_CUDA = -2,     /* a CUDA runtime call failed */
+  CLAST_ERR_NOMEM = -3,    /* device or host allocation failed */
+  CLAST_ERR_INTERNAL = -4  /* internal consistency check failed */
+} clast_status;
+
+typedef struct clast_ctx clast_ctx;
+typedef struct clast_index clast_index;
+typedef struct clast_targets clast_targets;
+
+/* The search settings of CHostSetting (CHostSetting.cuh:29-49) that the
+ * device path reads.  Defaults (common.hpp:12-43): lmer 15, stride 5,
+ * cut_repeat 20, width 100, gap 8, local 0, cutoff 10, K 0.71, lambda 1.37. */
+typedef struct clast_params {
+  int32_t lmer;        /* 1..31                               */
+  int32_t stride;      /* >= 1                                */
+  int32_t cut_repeat;  /* -1 = unlimited                      */
+  int32_t width;       /* seed-seed distance for the filters  */
+  int32_t gap;         /* 2..16: band = 2*gap+1 diagonals     */
+  int32_t local;       /* 0 = global alignment, else local    */
+  double cutoff;       /* E-value cut-off, -1 = none          */
+  double total_db;     /* totalDatabaseSize (CHostSetting.cu:46-58) */
+  double K;
+  double lambda;
+} clast_params;
+
+/* Hit list, structure of arrays (the nine device_vectors of CDeviceHitList,
+ * CDeviceHitList.cuh:13-21), in the order the reference produces. */
+typedef struct clast_hits {
+  int64_t n;
+  int32_t* t_id;
+  int32_t* t_idx;
+  int32_t* q_id;
+  int32_t* q_idx;
+  int32_t* t_len;
+  int32_t* q_len;
+  int32_t* match;
+  int32_t* score;
+  double* evalue;
+} clast_hits;
+
+int clast_ctx_create(int device, clast_ctx** out);
+void clast_ctx_destroy(clast_ctx* ctx);
+const char* clast_last_error(const clast_ctx* ctx);
+
+/* Index of one target window (replaces CDeviceHashTable's constructor).
+ * bases: the window's base array exactly as CHostSeqList::getBaseArray(
+ * t_begin, t_end) builds it -- every sequence followed by its first l-1
+ * bases; gateway: window-relative sequence starts (n_seqs values, first 0);
+ * lengths: sequence lengths; t_begin: id of the window's first sequence. */
+int clast_index_build(clast_ctx* ctx, const clast_params* p, const char* bases, int64_t n_bases,
+                      const int32_t* gateway, const int32_t* lengths, int32_t n_seqs,
+                      int32_t t_begin, clast_index** out);
+void clast_index_free(clast_index* ix);
+
+/* Hits of one query window against one index (replaces CDeviceSeqList_query
+ * + CDeviceHitList + getResult).  q_bases/q_gateway/q_lengths describe the
+ * query window as CHostSeqList::getBaseArray(2*qb, 2*qe) does: '+' and '-'
+ * strand of every read, each followed by its joint.  q_begin = 2*qb (even). */
+int clast_search(clast_ctx* ctx, const clast_index* ix, const clast_params* p,
+                 const char* q_bases, int64_t n_qbases, const int32_t* q_gateway,
+                 const int32_t* q_lengths, int32_t n_qseqs, int32_t q_begin, clast_hits* out);
+void clast_hits_free(clast_hits* h);
+
+/* ---- whole job: resident target indexes, every query RAM load at once ---- */
+
+/* One set of sequences, one strand, no joints: record i is
+ * bases[offsets[i] .. offsets[i+1]). */
+typedef struct clast_seqs {
+  int64_t n_seqs;
+  const char* bases;
+  const int64_t* offsets; /* n_seqs + 1 values */
+} clast_seqs;
+
+/* Builds and keeps in HBM the index of every target window.  The target
+ * records are split into RAM loads (load_sizes[k] records each, in order, as
+ * CFASTALoader hands them out) and each load into windows by the rule of
+ * moveTargetWindow (CHostSchedular.cu:25-35) with budget t_vram (bases). */
+int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram,
+                         const clast_seqs* targets, int32_t n_loads, const int64_t* load_sizes,
+                         clast_targets** out);
+void clast_targets_free(clast_targets* t);
+
+/* Result of clast_map: hits of every query load in the order
+ * CHostResultHolder::fixResult leaves them (load by load).  read = record
+ * index in the query set; strand 0 '+', 1 '-'; t_load / t_seq locate the
+ * target record (t_seq counts within its load). */
+typedef struct clast_map_result {
+  int64_t n;
+  int64_t* load_offsets; /* n_qloads + 1 values: hits of query load k */
+  int32_t* read;
+  int32_t* strand;
+  int32_t* t_load;
+  int32_t* t_seq;
+  int32_t* t_idx;
+  int32_t* q_idx;
+  int32_t* t_len;
+  int32_t* q_len;
+  int32_t* match;
+  int32_t* score;
+  double* evalue;
+} clast_map_result;
+
+/* Maps every read against every target window.  The reads are split into RAM
+ * loads (load_sizes[k] records each) and each load into windows by the rule
+ * of moveQueryWindow (CHostSchedular.cu:12-23) with budget q_vram (bases,
+ * both strands and joints counted). */
+int clast_map(clast_ctx* ctx, const clast_targets* t, const clast_params* p, int32_t q_vram,
+              const clast_seqs* reads, int32_t n_loads, const int64_t* load_sizes,
+              clast_map_result* out);
+void clast_map_result_free(clast_map_result* r);
+
+/* Device-side timing of the last clast_map call in milliseconds (kernels and
+ * copies on the context's stream), and how many kernels it launched. */
+int clast_last_map_stats(const clast_ctx* ctx, double* device_ms, int64_t* kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
