@@ -27,7 +27,8 @@ class clast_hits(C.Structure):
 
 
 class clast_seqs(C.Structure):
-    _fields_ = [("n_seqs", C.c_int64), ("bases", C.c_char_p), ("offsets", C.POINTER(C.c_int64))]
+    _fields_ = [("n_seqs", C.c_int64), ("bases", C.c_void_p), ("offsets", C.POINTER(C.c_int64)),
+                ("bases_on_device", C.c_int32)]
 
 
 class clast_map_result(C.Structure):
@@ -35,6 +36,15 @@ class clast_map_result(C.Structure):
                [(f, C.POINTER(C.c_int32)) for f in ("read", "strand", "t_load", "t_seq", "t_idx", "q_idx",
                                                    "t_len", "q_len", "match", "score")] + \
                [("evalue", C.POINTER(C.c_double))]
+
+
+class clast_stats(C.Structure):
+    _fields_ = [("index_ms", C.c_double), ("index_upload_ms", C.c_double), ("map_ms", C.c_double),
+                ("map_upload_ms", C.c_double), ("index_launches", C.c_int64), ("map_launches", C.c_int64),
+                ("query_bases", C.c_int64), ("query_kmers", C.c_int64), ("seeds", C.c_int64), ("hits", C.c_int64),
+                ("results", C.c_int64), ("dp_cells", C.c_int64), ("seed_ms", C.c_double),
+                ("seed_launches", C.c_int64), ("dp_ms", C.c_double), ("dp_launches", C.c_int64),
+                ("sort_ms", C.c_double), ("final_ms", C.c_double)]
 
 
 # symbol name -> (restype, argtypes); the full export list of include/clast_gpu.h
@@ -56,6 +66,7 @@ SIGNATURES = {
                             C.c_int32, C.c_void_p, C.POINTER(clast_map_result)]),
     "clast_map_result_free": (None, [C.POINTER(clast_map_result)]),
     "clast_last_map_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "clast_get_stats": (C.c_int, [C.c_void_p, C.POINTER(clast_stats)]),
     "clast_cli_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), C.c_char_p, C.c_int]),
 }
 

@@ -56,6 +56,31 @@ class Setting:
                               float(self.cutoff), float(self.total_db), float(self.K), float(self.lambda_))
 
 
+def ram_loads(lengths, budget: int):
+    """RAM loads of CFASTALoader (CFASTALoader.cpp:43-87) for records of the
+    given lengths: a record joins the current load while sum + length <
+    budget, a record longer than the budget is skipped.  Returns (kept mask,
+    records per load).  A record exactly as long as the budget would make the
+    reference loop forever; that raises ValueError."""
+    lengths = np.asarray(lengths, dtype=np.int64)
+    keep = lengths <= budget
+    loads, cur, tot = [], 0, 0
+    for L in lengths[keep].tolist():
+        if tot + L < budget:
+            tot += L
+            cur += 1
+            continue
+        if cur == 0:
+            raise ValueError("a record is exactly as long as the RAM budget; the reference never terminates")
+        loads.append(cur)
+        cur, tot = 1, L
+        if L == budget:
+            raise ValueError("a record is exactly as long as the RAM budget; the reference never terminates")
+    if cur:
+        loads.append(cur)
+    return keep, loads
+
+
 def _comp(seq: bytes) -> bytes:
     """utilReverseSeq.cpp:3-19: reverse complement, non-ACGT -> N."""
     table = bytes.maketrans(b"ACGT", b"TGCA")
@@ -215,25 +240,35 @@ class Engine:
         return self.hit_list_window(s, ix, bases, gw, ln, 2 * q_begin)
 
     # -- whole job ----------------------------------------------------------
-    def targets(self, s: Setting, bases: np.ndarray, offsets: np.ndarray, load_sizes, t_vram: int) -> Targets:
-        b = np.ascontiguousarray(bases, dtype=np.uint8)
+    @staticmethod
+    def _seqs(bases, offsets):
+        """clast_seqs over a numpy array (host) or an object with a
+        ``data_ptr()`` method on the context's GPU (e.g. a torch CUDA tensor)."""
         o = np.ascontiguousarray(offsets, dtype=np.int64)
+        if hasattr(bases, "data_ptr"):
+            dev = 1 if getattr(bases, "is_cuda", False) else 0
+            ptr, keep = bases.data_ptr(), bases
+        else:
+            keep = np.ascontiguousarray(bases, dtype=np.uint8)
+            dev, ptr = 0, keep.ctypes.data
+        return N.clast_seqs(len(o) - 1, ptr, o.ctypes.data_as(C.POINTER(C.c_int64)), dev), (o, keep)
+
+    def targets(self, s: Setting, bases, offsets: np.ndarray, load_sizes, t_vram: int) -> Targets:
+        """Index of every target window (``bases``: numpy uint8, pinned or
+        CUDA torch tensor)."""
         ls = np.ascontiguousarray(load_sizes, dtype=np.int64)
-        seqs = N.clast_seqs(len(o) - 1, C.cast(b.ctypes.data, C.c_char_p), o.ctypes.data_as(C.POINTER(C.c_int64)))
+        seqs, _keep = self._seqs(bases, offsets)
         out = C.c_void_p()
         p = s.c()
         self._check(self._lib.clast_targets_create(self.ctx, C.byref(p), int(t_vram), C.byref(seqs), len(ls),
                                                    ls.ctypes.data, C.byref(out)))
         return Targets(out.value)
 
-    def map(self, s: Setting, targets: Targets, bases: np.ndarray, offsets: np.ndarray, load_sizes,
-            q_vram: int) -> dict:
+    def map(self, s: Setting, targets: Targets, bases, offsets: np.ndarray, load_sizes, q_vram: int) -> dict:
         """Every read against every target window; hits per query load in
         the order CHostResultHolder::fixResult leaves them."""
-        b = np.ascontiguousarray(bases, dtype=np.uint8)
-        o = np.ascontiguousarray(offsets, dtype=np.int64)
         ls = np.ascontiguousarray(load_sizes, dtype=np.int64)
-        seqs = N.clast_seqs(len(o) - 1, C.cast(b.ctypes.data, C.c_char_p), o.ctypes.data_as(C.POINTER(C.c_int64)))
+        seqs, _keep = self._seqs(bases, offsets)
         r = N.clast_map_result()
         p = s.c()
         self._check(self._lib.clast_map(self.ctx, targets.handle, C.byref(p), int(q_vram), C.byref(seqs), len(ls),
@@ -248,6 +283,13 @@ class Engine:
             return out
         finally:
             self._lib.clast_map_result_free(C.byref(r))
+
+    def stats(self) -> dict:
+        """clast_get_stats: CUDA-event timings and counts of the last
+        targets()/map() calls."""
+        st = N.clast_stats()
+        self._check(self._lib.clast_get_stats(self.ctx, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in N.clast_stats._fields_}
 
     def last_map_stats(self):
         ms = C.c_double()

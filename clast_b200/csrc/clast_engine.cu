@@ -25,14 +25,67 @@
 
 using namespace clast;
 
+// CUDA-event timing of device stages on one stream: begin()/end() bracket
+// launches, flush() (after a stream synchronisation) adds up the intervals.
+struct StageTimer {
+  enum Stage { SEED = 0, DP = 1, SORT = 2, FINAL = 3, N_STAGES = 4 };
+  std::vector<cudaEvent_t> pool;
+  struct Pending { int stage; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  double ms[N_STAGES] = {0, 0, 0, 0};
+  int64_t n[N_STAGES] = {0, 0, 0, 0};
+  cudaEvent_t cur_a = nullptr;
+
+  cudaEvent_t take() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      CLAST_CK(cudaEventCreate(&e));
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  void begin(cudaStream_t st) {
+    cur_a = take();
+    CLAST_CK(cudaEventRecord(cur_a, st));
+  }
+  void end(int stage, cudaStream_t st, int launches = 1) {
+    cudaEvent_t b = take();
+    CLAST_CK(cudaEventRecord(b, st));
+    pending.push_back({stage, cur_a, b});
+    n[stage] += launches;
+  }
+  void flush() {
+    for (auto& p : pending) {
+      float t = 0;
+      CLAST_CK(cudaEventElapsedTime(&t, p.a, p.b));
+      ms[p.stage] += t;
+      pool.push_back(p.a);
+      pool.push_back(p.b);
+    }
+    pending.clear();
+  }
+  void reset() {
+    flush();
+    for (int i = 0; i < N_STAGES; ++i) { ms[i] = 0; n[i] = 0; }
+  }
+  ~StageTimer() {
+    for (auto e : pool) cudaEventDestroy(e);
+    for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+  }
+};
+
 struct clast_ctx {
   int device = 0;
   cudaStream_t st = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
   Workspace ws;
   std::string err;
   double last_ms = 0;
   int64_t last_launches = 0;
+  clast_stats stats{};
+  StageTimer timer;
 };
 
 namespace {
@@ -41,6 +94,20 @@ template <class T>
 struct DevArray {  // owning device allocation
   T* p = nullptr;
   size_t n = 0;
+  DevArray() = default;
+  DevArray(const DevArray&) = delete;
+  DevArray& operator=(const DevArray&) = delete;
+  DevArray(DevArray&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevArray& operator=(DevArray&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
   void alloc(size_t count) {
     release();
     n = count;
@@ -178,8 +245,10 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix) {
   CLAST_CK(cudaStreamSynchronize(st));
 }
 
-clast_index* make_index(clast_ctx* c, const clast_params* p, const char* bases, int64_t n_bases,
-                        const int32_t* gateway, const int32_t* lengths, int32_t n_seqs, int32_t t_begin) {
+// Index of a window whose padded base array is already on the device.
+clast_index* make_index_resident(clast_ctx* c, const clast_params* p, DevArray<char>&& padded, int64_t n_bases,
+                                 DevArray<int32_t>&& gateway, DevArray<int32_t>&& lengths, int32_t n_seqs,
+                                 int32_t t_begin) {
   std::unique_ptr<clast_index> ix(new clast_index());
   ix->l = p->lmer;
   ix->stride = p->stride;
@@ -187,15 +256,41 @@ clast_index* make_index(clast_ctx* c, const clast_params* p, const char* bases, 
   ix->t_begin = t_begin;
   ix->n = n_bases;
   ix->nseqs = n_seqs;
-  upload_padded(bases, n_bases, ix->bases, c->st);
-  ix->gateway.alloc(n_seqs);
-  ix->lengths.alloc(n_seqs);
-  if (n_seqs > 0) {
-    CLAST_CK(cudaMemcpyAsync(ix->gateway.p, gateway, n_seqs * sizeof(int32_t), cudaMemcpyHostToDevice, c->st));
-    CLAST_CK(cudaMemcpyAsync(ix->lengths.p, lengths, n_seqs * sizeof(int32_t), cudaMemcpyHostToDevice, c->st));
-  }
+  ix->bases = std::move(padded);
+  ix->gateway = std::move(gateway);
+  ix->lengths = std::move(lengths);
   build_index_device(c, p, ix.get());
   return ix.release();
+}
+
+// Index of a window given as host arrays (the reference's seam).
+clast_index* make_index(clast_ctx* c, const clast_params* p, const char* bases, int64_t n_bases,
+                        const int32_t* gateway, const int32_t* lengths, int32_t n_seqs, int32_t t_begin) {
+  DevArray<char> padded;
+  DevArray<int32_t> gw, ln;
+  gw.alloc(n_seqs);
+  ln.alloc(n_seqs);
+  padded.alloc((size_t)n_bases + 2 * kPad);
+  CLAST_CK(cudaEventRecord(c->ev0, c->st));
+  CLAST_CK(cudaMemsetAsync(padded.p, 'N', (size_t)n_bases + 2 * kPad, c->st));
+  if (n_bases > 0) CLAST_CK(cudaMemcpyAsync(padded.p + kPad, bases, (size_t)n_bases, cudaMemcpyHostToDevice, c->st));
+  if (n_seqs > 0) {
+    CLAST_CK(cudaMemcpyAsync(gw.p, gateway, n_seqs * sizeof(int32_t), cudaMemcpyHostToDevice, c->st));
+    CLAST_CK(cudaMemcpyAsync(ln.p, lengths, n_seqs * sizeof(int32_t), cudaMemcpyHostToDevice, c->st));
+  }
+  CLAST_CK(cudaEventRecord(c->ev1, c->st));
+  const int64_t k0 = g_kernel_launches;
+  clast_index* ix = make_index_resident(c, p, std::move(padded), n_bases, std::move(gw), std::move(ln), n_seqs,
+                                        t_begin);
+  CLAST_CK(cudaEventRecord(c->ev2, c->st));
+  CLAST_CK(cudaEventSynchronize(c->ev2));
+  float up = 0, bd = 0;
+  CLAST_CK(cudaEventElapsedTime(&up, c->ev0, c->ev1));
+  CLAST_CK(cudaEventElapsedTime(&bd, c->ev1, c->ev2));
+  c->stats.index_upload_ms += up;
+  c->stats.index_ms += bd;
+  c->stats.index_launches += g_kernel_launches - k0;
+  return ix;
 }
 
 // Device-resident query strands of one batch, packed once for every index.
@@ -247,30 +342,55 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   // createRawSeedList + deleteSeedsOnSequenceBoundary
   int64_t* cnt = ws.get<int64_t>("s_cnt", ns);
   int64_t* off = ws.get<int64_t>("s_off", ns + 1);
-  seed_count(q, iv, cnt, st);
+  unsigned long long* counters = ws.get<unsigned long long>("s_counters", 2);  // k-mers, DP cells
+  CLAST_CK(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st));
+  StageTimer& tm = c->timer;
+  tm.begin(st);
+  seed_count(q, iv, cnt, counters, st);
+  tm.end(StageTimer::SEED, st);
   scan_i64(ws, cnt, ns, off, st);
   const int64_t S = read_scalar(off + ns, st);
-  if (S == 0) return;
+  auto add_counters = [&]() {
+    unsigned long long h[2];
+    CLAST_CK(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CLAST_CK(cudaStreamSynchronize(st));
+    c->stats.query_kmers += (int64_t)h[0];
+    c->stats.dp_cells += (int64_t)h[1];
+    tm.flush();
+  };
+  c->stats.seeds += S;
+  if (S == 0) {
+    add_counters();
+    return;
+  }
   uint64_t* skey = ws.get<uint64_t>("s_key", S);
   uint32_t* sq = ws.get<uint32_t>("s_q", S);
   int32_t* nvalid = ws.get<int32_t>("s_nvalid", ns);
+  tm.begin(st);
   seed_write(q, iv, tv, p->gap, p->local, off, skey, sq, nvalid, st);
+  tm.end(StageTimer::SEED, st);
   int32_t* wfirst = ws.get<int32_t>("s_wfirst", qb.nwin);
   window_first(nvalid, qb.wstart.p, qb.nwin, wfirst, st);
   // sortSeeds, deletingIsolateSeeds, deleteDuplicateSeeds
   int32_t* len32 = ws.get<int32_t>("s_len32", ns);
+  tm.begin(st);
   to_i32(cnt, ns, len32, st);
   segmented_sort_u32(ws, skey, sq, off, len32, ns, st, 0);
   int32_t* hcnt = ws.get<int32_t>("s_hcnt", ns);
   seed_filter(skey, sq, off, nvalid, qb.wstart.p, qb.nwin, wfirst, p->width, p->gap, ns, hcnt, st);
+  tm.end(StageTimer::SORT, st, 7);
   int64_t* hoff = ws.get<int64_t>("s_hoff", ns + 1);
   scan_i32(ws, hcnt, ns, hoff, st);
   const int64_t H = read_scalar(hoff + ns, st);
-  if (H == 0) return;
+  c->stats.hits += H;
+  if (H == 0) {
+    add_counters();
+    return;
+  }
   uint64_t* hk = ws.get<uint64_t>("h_key", H);
   int32_t* hq = ws.get<int32_t>("h_q", H);
   int32_t* hs = ws.get<int32_t>("h_s", H);
-  gather_hits(skey, sq, off, hcnt, hoff, ns, hk, hq, hs, st);
+  gather_hits(skey, sq, off, hcnt, hoff, ns, hk, hq, hs, qb.len.p, p->lmer, 2 * p->gap + 1, counters + 1, st);
   // alignmentHits + calculateEvalue + deleteHits_lowEValue / _tooShort
   DpOut o;
   o.t_idx = ws.get<int32_t>("d_tidx", H);
@@ -282,12 +402,15 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   o.evalue = ws.get<double>("d_e", H);
   o.keep = ws.get<uint8_t>("d_keep", H);
   DpParams dp{p->lmer, p->stride, p->gap, p->local, p->cutoff, p->total_db, p->K, p->lambda};
+  tm.begin(st);
   banded_dp(tv, q, hk, hq, hs, H, dp, o, st);
+  tm.end(StageTimer::DP, st);
   // resultSorting + deleteHits_duplicateResult, per read
   uint64_t* k1 = ws.get<uint64_t>("f_k1", H);
   uint64_t* k2 = ws.get<uint64_t>("f_k2", H);
   int32_t* idx = ws.get<int32_t>("f_idx", H);
   final_keys(hk, hq, hs, o, H, k1, k2, idx, st);
+  tm.begin(st);
   int64_t* roff = ws.get<int64_t>("f_roff", nr);
   int32_t* rlen = ws.get<int32_t>("f_rlen", nr);
   read_ranges(hoff, nr, roff, rlen, st);
@@ -297,7 +420,10 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   final_dedupe(k1, k2, idx, hk, hs, o, roff, rlen, nr, fcnt, fsel, st);
   int64_t* foff = ws.get<int64_t>("f_off", nr + 1);
   scan_i32(ws, fcnt, nr, foff, st);
+  tm.end(StageTimer::FINAL, st, 9);
   const int64_t F = read_scalar(foff + nr, st);
+  c->stats.results += F;
+  add_counters();
   if (F == 0) return;
   FinalOut fo;
   fo.t_id = ws.get<int32_t>("o_tid", F);
@@ -409,7 +535,9 @@ int clast_ctx_create(int device, clast_ctx** out) {
   if (device < 0 || device >= ndev) return CLAST_ERR_ARG;
   if (cudaSetDevice(device) != cudaSuccess) return CLAST_ERR_CUDA;
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
-  if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) return CLAST_ERR_CUDA;
+  if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaEventCreate(&c->ev2) != cudaSuccess)
+    return CLAST_ERR_CUDA;
   *out = c.release();
   return CLAST_OK;
 }
@@ -421,6 +549,7 @@ void clast_ctx_destroy(clast_ctx* ctx) {
   ctx->ws.release_all();
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->ev2) cudaEventDestroy(ctx->ev2);
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
 }
@@ -439,6 +568,8 @@ int clast_index_build(clast_ctx* ctx, const clast_params* p, const char* bases, 
     if (n_bases >= INT32_MAX) throw std::invalid_argument("window larger than 2^31 bases");
     CLAST_CK(cudaSetDevice(ctx->device));
     g_kernel_launches = 0;
+    ctx->stats.index_ms = ctx->stats.index_upload_ms = 0;
+    ctx->stats.index_launches = 0;
     *out = make_index(ctx, p, bases, n_bases, gateway, lengths, n_seqs, t_begin);
     return CLAST_OK;
   });
@@ -521,13 +652,33 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
     if (total != targets->n_seqs) throw std::invalid_argument("load sizes do not add up to n_seqs");
     CLAST_CK(cudaSetDevice(ctx->device));
     g_kernel_launches = 0;
+    ctx->stats.index_ms = ctx->stats.index_upload_ms = 0;
+    ctx->stats.index_launches = 0;
     const int l = p->lmer;
     std::unique_ptr<clast_targets> T(new clast_targets());
     T->ctx = ctx;
     T->n_loads = n_loads;
+    cudaStream_t st = ctx->st;
+    // the raw target set on the device, uploaded once unless already resident
+    const int64_t nt = targets->n_seqs;
+    const int64_t tbytes = nt ? targets->offsets[nt] - targets->offsets[0] : 0;
+    DevArray<char> traw;
+    const char* src = targets->bases + (nt ? targets->offsets[0] : 0);
+    CLAST_CK(cudaEventRecord(ctx->ev0, st));
+    if (!targets->bases_on_device) {
+      traw.alloc((size_t)tbytes + 1);
+      if (tbytes) CLAST_CK(cudaMemcpyAsync(traw.p, src, (size_t)tbytes, cudaMemcpyHostToDevice, st));
+      src = traw.p;
+    }
+    CLAST_CK(cudaEventRecord(ctx->ev1, st));
+    CLAST_CK(cudaEventSynchronize(ctx->ev1));
+    float up = 0;
+    CLAST_CK(cudaEventElapsedTime(&up, ctx->ev0, ctx->ev1));
+    ctx->stats.index_upload_ms += up;
+    const int64_t base0 = nt ? targets->offsets[0] : 0;
     int64_t rec = 0;
-    std::vector<char> wb;
     std::vector<int32_t> gw, ln;
+    std::vector<int64_t> so;
     for (int32_t k = 0; k < n_loads; ++k) {
       const int64_t r0 = rec, r1 = rec + load_sizes[k];
       rec = r1;
@@ -536,25 +687,44 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
       for (int64_t i = r0; i < r1; ++i)
         lg[i - r0 + 1] = lg[i - r0] + (targets->offsets[i + 1] - targets->offsets[i]) + (l - 1);
       const int64_t tEnd = r1 - r0;
-      for (int64_t tb = 0, te = 1; tb < tEnd; tb = te++) {  // moveTargetWindow
+      for (int64_t tb = 0, te = 1; tb < tEnd; tb = te++) {  // moveTargetWindow, CHostSchedular.cu:25-35
         while (te < tEnd && lg[te + 1] - lg[tb] < (int64_t)t_vram) ++te;
-        wb.clear();
+        const int64_t wn = lg[te] - lg[tb];
+        if (wn >= (int64_t)INT32_MAX) throw std::invalid_argument("target window larger than 2^31 bases");
         gw.clear();
         ln.clear();
+        so.clear();
         for (int64_t i = r0 + tb; i < r0 + te; ++i) {
-          const char* s = targets->bases + targets->offsets[i];
-          const int64_t len = targets->offsets[i + 1] - targets->offsets[i];
-          gw.push_back((int32_t)wb.size());
-          ln.push_back((int32_t)len);
-          wb.insert(wb.end(), s, s + len);
-          for (int j = 0; j < l - 1; ++j) wb.push_back(j < len ? s[j] : 'N');  // joint
+          gw.push_back((int32_t)(lg[i - r0] - lg[tb]));
+          ln.push_back((int32_t)(targets->offsets[i + 1] - targets->offsets[i]));
+          so.push_back(targets->offsets[i] - base0);
         }
-        if (wb.size() >= (size_t)INT32_MAX) throw std::invalid_argument("target window larger than 2^31 bases");
+        const int32_t wseqs = (int32_t)gw.size();
+        DevArray<char> padded;
+        DevArray<int32_t> dgw, dln;
+        DevArray<int64_t> dso;
+        padded.alloc((size_t)wn + 2 * kPad);
+        dgw.alloc(wseqs);
+        dln.alloc(wseqs);
+        dso.alloc(wseqs);
+        CLAST_CK(cudaEventRecord(ctx->ev1, st));
+        const int64_t k0 = g_kernel_launches;
+        CLAST_CK(cudaMemcpyAsync(dgw.p, gw.data(), wseqs * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        CLAST_CK(cudaMemcpyAsync(dln.p, ln.data(), wseqs * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        CLAST_CK(cudaMemcpyAsync(dso.p, so.data(), wseqs * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+        CLAST_CK(cudaMemsetAsync(padded.p, 'N', (size_t)wn + 2 * kPad, st));
+        build_window(src, dso.p, dgw.p, dln.p, wseqs, wn, padded.p + kPad, st);
         clast_targets::Win w;
         w.load = k;
         w.first = (int32_t)tb;
-        w.ix.reset(make_index(ctx, p, wb.data(), (int64_t)wb.size(), gw.data(), ln.data(), (int32_t)gw.size(),
-                              (int32_t)tb));
+        w.ix.reset(make_index_resident(ctx, p, std::move(padded), wn, std::move(dgw), std::move(dln), wseqs,
+                                       (int32_t)tb));
+        CLAST_CK(cudaEventRecord(ctx->ev2, st));
+        CLAST_CK(cudaEventSynchronize(ctx->ev2));
+        float bd = 0;
+        CLAST_CK(cudaEventElapsedTime(&bd, ctx->ev1, ctx->ev2));
+        ctx->stats.index_ms += bd;
+        ctx->stats.index_launches += g_kernel_launches - k0;
         T->wins.push_back(std::move(w));
       }
     }
@@ -581,7 +751,10 @@ int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int
     CLAST_CK(cudaSetDevice(ctx->device));
     g_kernel_launches = 0;
     cudaStream_t st = ctx->st;
-    CLAST_CK(cudaEventRecord(ctx->ev0, st));
+    clast_stats& S = ctx->stats;
+    S.map_ms = S.map_upload_ms = 0;
+    S.map_launches = S.query_bases = S.query_kmers = S.seeds = S.hits = S.results = S.dp_cells = 0;
+    ctx->timer.reset();
     const int64_t nreads = reads->n_seqs;
     // query windows of every load, in read order
     std::vector<int64_t> wfirst;
@@ -590,39 +763,57 @@ int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int
     for (int32_t k = 0; k < n_loads; ++k)
       query_windows(reads->offsets, load_first[k], load_first[k + 1], p->lmer, q_vram, wfirst);
     wfirst.push_back(nreads);
-    // upload every read once; strands built on the device
+    std::vector<int32_t> wstart(wfirst.size());
+    for (size_t i = 0; i < wfirst.size(); ++i) wstart[i] = (int32_t)(2 * wfirst[i]);
+    // every read uploaded once; strands are built on the device
     const int64_t nb = reads->offsets[nreads] - reads->offsets[0];
-    DevArray<char> draw;
-    DevArray<int64_t> doff;
-    draw.alloc((size_t)nb + 64);
-    doff.alloc((size_t)nreads + 1);
     std::vector<int64_t> off0(nreads + 1);
     for (int64_t i = 0; i <= nreads; ++i) off0[i] = reads->offsets[i] - reads->offsets[0];
-    if (nb) CLAST_CK(cudaMemcpyAsync(draw.p, reads->bases + reads->offsets[0], nb, cudaMemcpyHostToDevice, st));
-    CLAST_CK(cudaMemcpyAsync(doff.p, off0.data(), (nreads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    DevArray<char> draw;
+    DevArray<int64_t> doff;
+    if (!reads->bases_on_device) draw.alloc((size_t)nb + 64);
+    doff.alloc((size_t)nreads + 1);
     QueryBatch qb;
     qb.n = 2 * nb;
     qb.nstrands = (int32_t)(2 * nreads);
     qb.bases.alloc((size_t)qb.n + 2 * kPad);
-    CLAST_CK(cudaMemsetAsync(qb.bases.p, 'N', (size_t)qb.n + 2 * kPad, st));
     qb.start.alloc(2 * nreads);
     qb.len.alloc(2 * nreads);
-    build_strands(draw.p, doff.p, nreads, nb, qb.bases.p + kPad, qb.start.p, qb.len.p, st);
-    std::vector<int32_t> wstart(wfirst.size());
-    for (size_t i = 0; i < wfirst.size(); ++i) wstart[i] = (int32_t)(2 * wfirst[i]);
     qb.nwin = (int32_t)wfirst.size() - 1;
     qb.wstart.alloc(wstart.size());
+    CLAST_CK(cudaEventRecord(ctx->ev0, st));
+    const char* rsrc = reads->bases + reads->offsets[0];
+    if (!reads->bases_on_device) {
+      if (nb) CLAST_CK(cudaMemcpyAsync(draw.p, rsrc, nb, cudaMemcpyHostToDevice, st));
+      rsrc = draw.p;
+    }
+    CLAST_CK(cudaMemcpyAsync(doff.p, off0.data(), (nreads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
     CLAST_CK(cudaMemcpyAsync(qb.wstart.p, wstart.data(), wstart.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
                              st));
+    CLAST_CK(cudaEventRecord(ctx->ev1, st));
+    CLAST_CK(cudaMemsetAsync(qb.bases.p, 'N', (size_t)qb.n + 2 * kPad, st));
+    build_strands(rsrc, doff.p, nreads, nb, qb.bases.p + kPad, qb.start.p, qb.len.p, st);
     qb.pack(st);
+    S.query_bases = qb.n;
     // every target window, in holder order (target load, window)
     std::vector<HostHits> per_win(T->wins.size());
     for (size_t w = 0; w < T->wins.size(); ++w) search_batch(ctx, T->wins[w].ix.get(), p, qb, 0, per_win[w]);
-    CLAST_CK(cudaEventRecord(ctx->ev1, st));
-    CLAST_CK(cudaEventSynchronize(ctx->ev1));
-    float ms = 0;
-    CLAST_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-    ctx->last_ms = ms;
+    CLAST_CK(cudaEventRecord(ctx->ev2, st));
+    CLAST_CK(cudaEventSynchronize(ctx->ev2));
+    float up = 0, ms = 0;
+    CLAST_CK(cudaEventElapsedTime(&up, ctx->ev0, ctx->ev1));
+    CLAST_CK(cudaEventElapsedTime(&ms, ctx->ev1, ctx->ev2));
+    ctx->timer.flush();
+    S.map_upload_ms = up;
+    S.map_ms = ms;
+    S.map_launches = g_kernel_launches;
+    S.seed_ms = ctx->timer.ms[StageTimer::SEED];
+    S.seed_launches = ctx->timer.n[StageTimer::SEED];
+    S.dp_ms = ctx->timer.ms[StageTimer::DP];
+    S.dp_launches = ctx->timer.n[StageTimer::DP];
+    S.sort_ms = ctx->timer.ms[StageTimer::SORT];
+    S.final_ms = ctx->timer.ms[StageTimer::FINAL];
+    ctx->last_ms = up + ms;
     ctx->last_launches = g_kernel_launches;
     // fixResult: per read, stable merge by score desc over the windows in holder order
     std::vector<std::vector<std::pair<int64_t, int64_t>>> ranges(T->wins.size());
@@ -688,6 +879,12 @@ void clast_map_result_free(clast_map_result* r) {
   std::free(r->t_seq); std::free(r->t_idx); std::free(r->q_idx); std::free(r->t_len); std::free(r->q_len);
   std::free(r->match); std::free(r->score); std::free(r->evalue);
   std::memset(r, 0, sizeof(*r));
+}
+
+int clast_get_stats(const clast_ctx* ctx, clast_stats* out) {
+  if (!ctx || !out) return CLAST_ERR_ARG;
+  *out = ctx->stats;
+  return CLAST_OK;
 }
 
 int clast_last_map_stats(const clast_ctx* ctx, double* device_ms, int64_t* kernel_launches) {

@@ -171,6 +171,28 @@ __global__ void k_strands(const char* __restrict__ reads, const int64_t* __restr
   out[2 * a + len + (len - 1 - j)] = complement(c);
 }
 
+// Base array of one target window: every sequence followed by its first l-1
+// bases (utilAddSequence.cu:15-46); joint bases past a sequence shorter than
+// l-1 are 'N'.
+__global__ void k_build_window(const char* __restrict__ src, const int64_t* __restrict__ src_off,
+                               const int32_t* __restrict__ gw, const int32_t* __restrict__ len, int nseqs,
+                               int64_t n, char* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int lo = 0, hi = nseqs;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if ((int64_t)gw[mid] <= i) lo = mid;
+    else hi = mid;
+  }
+  const int64_t j = i - gw[lo];
+  const int64_t L = len[lo];
+  char c;
+  if (j < L) c = src[src_off[lo] + j];
+  else c = (j - L < L) ? src[src_off[lo] + (j - L)] : 'N';
+  out[i] = c;
+}
+
 // ------------------------------------------------------------------------
 // index build
 // ------------------------------------------------------------------------
@@ -333,23 +355,32 @@ __global__ void k_index_dir(const uint64_t* __restrict__ ukeys, int64_t nu, int 
 // ------------------------------------------------------------------------
 // seeds
 // ------------------------------------------------------------------------
-__global__ void k_seed_count(QueryView q, IndexView ix, int64_t* __restrict__ cnt) {
+__global__ void k_seed_count(QueryView q, IndexView ix, int64_t* __restrict__ cnt,
+                             unsigned long long* __restrict__ n_kmers) {
   const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (s >= q.nstrands) return;
   const int64_t st = q.start[s];
   const int nk = q.len[s] - ix.l + 1;
   int64_t sum = 0;
+  int valid = 0;
   for (int qi = lane; qi < nk; qi += 32) {
     uint64_t key;
     if (kmer_at(q.packed, q.nmask, st + qi, ix.l, key)) {
+      ++valid;
       const int64_t u = index_lookup(ix, key);
       if (u >= 0) sum += ix.ucnt[u];
     }
   }
 #pragma unroll
-  for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
-  if (lane == 0) cnt[s] = sum;
+  for (int o = 16; o; o >>= 1) {
+    sum += __shfl_xor_sync(kFull, sum, o);
+    valid += __shfl_xor_sync(kFull, valid, o);
+  }
+  if (lane == 0) {
+    cnt[s] = sum;
+    if (valid) atomicAdd(n_kmers, (unsigned long long)valid);
+  }
 }
 
 __global__ void k_seed_write(QueryView q, IndexView ix, TargetView t, int gap, int local,
@@ -664,10 +695,13 @@ __global__ void k_seed_filter(uint64_t* __restrict__ skey, uint32_t* __restrict_
 __global__ void k_gather_hits(const uint64_t* __restrict__ skey, const uint32_t* __restrict__ sq,
                               const int64_t* __restrict__ off, const int32_t* __restrict__ hcnt,
                               const int64_t* __restrict__ hoff, int64_t nstrands, uint64_t* __restrict__ hk,
-                              int32_t* __restrict__ hq, int32_t* __restrict__ hs) {
+                              int32_t* __restrict__ hq, int32_t* __restrict__ hs, const int32_t* __restrict__ qlen,
+                              int l, int band, unsigned long long* __restrict__ cells) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nstrands) return;
   const int n = hcnt[s];
+  // every hit of the strand fills band * (qlen - l) cells: backward rows + forward rows
+  if (n) atomicAdd(cells, (unsigned long long)n * (unsigned long long)band * (unsigned long long)(qlen[s] - l));
   const int64_t a = off[s], b = hoff[s];
   for (int i = 0; i < n; ++i) {
     hk[b + i] = skey[a + i];
@@ -955,6 +989,13 @@ void build_strands(const char* reads, const int64_t* offsets, int64_t n_reads, i
   }
 }
 
+void build_window(const char* src, const int64_t* src_off, const int32_t* gateway, const int32_t* lengths,
+                  int nseqs, int64_t n, char* out, cudaStream_t st) {
+  if (n <= 0 || nseqs <= 0) return;
+  k_build_window<<<blocks_for(n, 256), 256, 0, st>>>(src, src_off, gateway, lengths, nseqs, n, out);
+  CLAST_LAUNCHED();
+}
+
 void sample_keys(const uint64_t* packed, const uint64_t* nmask, int64_t n_samples, int stride, int l,
                  uint64_t* keys, int32_t* vals, cudaStream_t st) {
   if (n_samples <= 0) return;
@@ -1031,9 +1072,10 @@ void index_directory(const uint64_t* ukeys, int64_t n_unique, int shift, int dir
   CLAST_LAUNCHED();
 }
 
-void seed_count(const QueryView& q, const IndexView& ix, int64_t* cnt, cudaStream_t st) {
+void seed_count(const QueryView& q, const IndexView& ix, int64_t* cnt, unsigned long long* n_kmers,
+                cudaStream_t st) {
   if (q.nstrands <= 0) return;
-  k_seed_count<<<blocks_for((int64_t)q.nstrands * 32, 256), 256, 0, st>>>(q, ix, cnt);
+  k_seed_count<<<blocks_for((int64_t)q.nstrands * 32, 256), 256, 0, st>>>(q, ix, cnt, n_kmers);
   CLAST_LAUNCHED();
 }
 void seed_write(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
@@ -1072,9 +1114,11 @@ void seed_filter(uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t
   CLAST_LAUNCHED();
 }
 void gather_hits(const uint64_t* skey, const uint32_t* sq, const int64_t* off, const int32_t* hcnt,
-                 const int64_t* hoff, int64_t nstrands, uint64_t* hk, int32_t* hq, int32_t* hs, cudaStream_t st) {
+                 const int64_t* hoff, int64_t nstrands, uint64_t* hk, int32_t* hq, int32_t* hs,
+                 const int32_t* qlen, int l, int band, unsigned long long* cells, cudaStream_t st) {
   if (nstrands <= 0) return;
-  k_gather_hits<<<blocks_for(nstrands, 256), 256, 0, st>>>(skey, sq, off, hcnt, hoff, nstrands, hk, hq, hs);
+  k_gather_hits<<<blocks_for(nstrands, 256), 256, 0, st>>>(skey, sq, off, hcnt, hoff, nstrands, hk, hq, hs, qlen, l,
+                                                           band, cells);
   CLAST_LAUNCHED();
 }
 

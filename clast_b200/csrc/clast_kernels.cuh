@@ -25,6 +25,10 @@ void build_strands(const char* reads, const int64_t* offsets, int64_t n_reads, i
                    char* strands, int64_t* strand_start, int32_t* strand_len, cudaStream_t st);
 
 // ---- index of one target window (CDeviceHashTable.cu:20-174) ----
+// Window base array (sequences with their joints) from a one-strand source set:
+// sequence k of the window is src[src_off[k] .. src_off[k]+lengths[k]).
+void build_window(const char* src, const int64_t* src_off, const int32_t* gateway, const int32_t* lengths,
+                  int nseqs, int64_t n, char* out, cudaStream_t st);
 // Sampled keys at window positions j*stride; invalid k-mers get key 1<<(2l).
 void sample_keys(const uint64_t* packed, const uint64_t* nmask, int64_t n_samples, int stride, int l,
                  uint64_t* keys, int32_t* vals, cudaStream_t st);
@@ -48,7 +52,9 @@ void index_directory(const uint64_t* ukeys, int64_t n_unique, int shift, int dir
                      cudaStream_t st);
 
 // ---- seeds (CDeviceHitList_createRawSeedList.cu, _deleteSeeds*.cu, _sortSeeds.cu) ----
-void seed_count(const QueryView& q, const IndexView& ix, int64_t* cnt, cudaStream_t st);
+// cnt[s] = seeds of strand s before the corner filter; *n_kmers += valid l-mers
+void seed_count(const QueryView& q, const IndexView& ix, int64_t* cnt, unsigned long long* n_kmers,
+                cudaStream_t st);
 void seed_write(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
                 const int64_t* off, uint64_t* skey, uint32_t* sq, int32_t* nvalid, cudaStream_t st);
 void window_first(const int32_t* nvalid, const int32_t* win_start, int n_windows, int32_t* win_first,
@@ -67,9 +73,10 @@ void to_i32(const int64_t* in, int64_t n, int32_t* out, cudaStream_t st);
 void seed_filter(uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t* nvalid,
                  const int32_t* win_start, int n_windows, const int32_t* win_first, int width, int gap,
                  int64_t nstrands, int32_t* hcnt, cudaStream_t st);
+// also adds band * (qlen - l) DP cells per hit to *cells
 void gather_hits(const uint64_t* skey, const uint32_t* sq, const int64_t* off, const int32_t* hcnt,
                  const int64_t* hoff, int64_t nstrands, uint64_t* hk, int32_t* hq, int32_t* hs,
-                 cudaStream_t st);
+                 const int32_t* qlen, int l, int band, unsigned long long* cells, cudaStream_t st);
 
 // ---- banded DP + E-value (krnlAlignment.cu, krnlCalculateEvalue.cu) ----
 struct DpOut {

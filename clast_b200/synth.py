@@ -187,6 +187,67 @@ def make_reads(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, indel=0.
     return SeqSet(["r%d" % i for i in range(n_reads)], bases, offsets)
 
 
+def make_reads_fixed(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, indel=0.005, indel_mean=2.0,
+                     rev_frac=0.5, decoy_frac=0.05, batch=65536) -> SeqSet:
+    """Vectorised fixed-length version of :func:`make_reads` (same error model:
+    substitutions, indel events of geometric length, reverse strand, decoys)."""
+    tl = target.lengths
+    cum = np.concatenate([[0], np.cumsum(tl)])
+    pad = 16 + 8 * int(np.ceil(length * indel * indel_mean))
+    M = length + pad
+    ok = np.flatnonzero(tl >= M)
+    if ok.size == 0:
+        raise ValueError("target contigs shorter than a read")
+    w = tl[ok].astype(np.float64)
+    w /= w.sum()
+    out = np.empty((n_reads, length), dtype=np.uint8)
+    for b0 in range(0, n_reads, batch):
+        B = min(batch, n_reads - b0)
+        c = ok[rng.choice(len(ok), size=B, p=w)]
+        start = target.offsets[c] + (rng.random(B) * (tl[c] - M + 1)).astype(np.int64)
+        src = target.bases[start[:, None] + np.arange(M)[None, :]]
+        ev = rng.random((B, M)) < indel
+        ins = ev & (rng.random((B, M)) < 0.5)
+        dele = ev & ~ins
+        ln = rng.geometric(1.0 / indel_mean, size=(B, M))
+        diff = np.zeros((B, M + 1), dtype=np.int32)
+        rb, rc = np.nonzero(dele)
+        np.add.at(diff, (rb, rc), 1)
+        np.add.at(diff, (rb, np.minimum(rc + ln[rb, rc], M)), -1)
+        covered = np.cumsum(diff[:, :M], axis=1) > 0
+        n_ins = np.where(ins & ~covered, ln, 0)
+        emit = n_ins + (~covered).astype(np.int64)
+        cs = np.cumsum(emit, axis=1)
+        total = cs[:, -1]
+        if (total < length).any():  # pathological deletions: fall back to the source
+            short = total < length
+            emit[short] = 1
+            n_ins[short] = 0
+            cs = np.cumsum(emit, axis=1)
+        big = int(cs[:, -1].max()) + 1
+        flat = (cs + (np.arange(B) * big)[:, None]).ravel()
+        o = (np.arange(length)[None, :] + (np.arange(B) * big)[:, None]).ravel()
+        j = np.searchsorted(flat, o, side="right").reshape(B, length) - np.arange(B)[:, None] * M
+        j = np.minimum(j, M - 1)
+        before = np.take_along_axis(cs, j, axis=1) - np.take_along_axis(emit, j, axis=1)
+        k = np.arange(length)[None, :] - before   # rank within position j's emission
+        is_ins = k < np.take_along_axis(n_ins, j, axis=1)
+        r = np.take_along_axis(src, j, axis=1)
+        r = np.where(is_ins, ACGT[rng.integers(0, 4, size=(B, length))], r)
+        m = rng.random((B, length)) < sub
+        idx = np.searchsorted(ACGT, r)
+        valid = (idx < 4) & (ACGT[np.minimum(idx, 3)] == r)
+        newb = ACGT[(np.where(valid, idx, 0) + rng.integers(1, 4, size=(B, length))) % 4]
+        r = np.where(m & valid, newb, r)
+        rev = rng.random(B) < rev_frac
+        r[rev] = _COMP[r[rev, ::-1]]
+        dec = rng.random(B) < decoy_frac
+        r[dec] = ACGT[rng.integers(0, 4, size=(int(dec.sum()), length))]
+        out[b0:b0 + B] = r
+    offsets = np.arange(n_reads + 1, dtype=np.int64) * length
+    return SeqSet(["r%d" % i for i in range(n_reads)], out.ravel(), offsets)
+
+
 def workload(name: str, seed: int = 0xC1A57, scale: float = 1.0):
     """(target, reads) for a named shape; ``scale`` shrinks sizes for tests."""
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -196,7 +257,7 @@ def workload(name: str, seed: int = 0xC1A57, scale: float = 1.0):
     elif name == "medium":
         t = make_target(rng, int(100_000_000 * scale), n_contigs=max(1, int(200 * min(1.0, scale * 10))),
                         median=300_000 * scale, repeat_frac=0.10, n_families=max(1, int(500 * scale)))
-        q = make_reads(rng, t, max(1, int(1_000_000 * scale)))
+        q = make_reads_fixed(rng, t, max(1, int(1_000_000 * scale)))
     elif name == "uneven":
         t = make_target(rng, int(100_000_000 * scale), n_contigs=max(1, int(200 * min(1.0, scale * 10))),
                         median=300_000 * scale, repeat_frac=0.10, n_families=max(1, int(500 * scale)))

@@ -100,11 +100,14 @@ void clast_hits_free(clast_hits* h);
 /* ---- whole job: resident target indexes, every query RAM load at once ---- */
 
 /* One set of sequences, one strand, no joints: record i is
- * bases[offsets[i] .. offsets[i+1]). */
+ * bases[offsets[i] .. offsets[i+1]).  offsets is always a host array; bases
+ * is a host pointer, or a device pointer on the context's GPU when
+ * bases_on_device is 1 (inputs already resident in HBM). */
 typedef struct clast_seqs {
   int64_t n_seqs;
   const char* bases;
   const int64_t* offsets; /* n_seqs + 1 values */
+  int32_t bases_on_device;
 } clast_seqs;
 
 /* Builds and keeps in HBM the index of every target window.  The target
@@ -148,6 +151,30 @@ void clast_map_result_free(clast_map_result* r);
 /* Device-side timing of the last clast_map call in milliseconds (kernels and
  * copies on the context's stream), and how many kernels it launched. */
 int clast_last_map_stats(const clast_ctx* ctx, double* device_ms, int64_t* kernel_launches);
+
+/* Measurements of the last clast_targets_create and clast_map calls, taken
+ * with CUDA events on the context's stream.  Units: milliseconds and counts. */
+typedef struct clast_stats {
+  double index_ms;           /* index builds, target upload excluded          */
+  double index_upload_ms;    /* target host-to-device copies                  */
+  double map_ms;             /* clast_map after the reads are resident (result download included) */
+  double map_upload_ms;      /* read host-to-device copies                    */
+  int64_t index_launches;    /* kernels launched by clast_targets_create      */
+  int64_t map_launches;      /* kernels launched by clast_map                 */
+  int64_t query_bases;       /* bases of every query strand                   */
+  int64_t query_kmers;       /* valid (all-ACGT) query l-mers looked up, summed over target windows */
+  int64_t seeds;             /* seeds written (boundary filters applied)      */
+  int64_t hits;              /* hits extended by the banded DP               */
+  int64_t results;           /* hits returned                                 */
+  int64_t dp_cells;          /* sum over hits of (2*gap+1) * (backward + forward rows) */
+  double seed_ms;            /* seed_count + seed_write kernels               */
+  int64_t seed_launches;
+  double dp_ms;              /* banded-DP kernels                             */
+  int64_t dp_launches;
+  double sort_ms;            /* segmented sorts + seed filter                 */
+  double final_ms;           /* result order, duplicate removal, compaction  */
+} clast_stats;
+int clast_get_stats(const clast_ctx* ctx, clast_stats* out);
 
 #ifdef __cplusplus
 }
