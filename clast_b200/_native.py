@@ -67,6 +67,7 @@ SIGNATURES = {
     "clast_map_result_free": (None, [C.POINTER(clast_map_result)]),
     "clast_last_map_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "clast_get_stats": (C.c_int, [C.c_void_p, C.POINTER(clast_stats)]),
+    "clast_int32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "clast_cli_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), C.c_char_p, C.c_int]),
 }
 

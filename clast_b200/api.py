@@ -291,6 +291,12 @@ class Engine:
         self._check(self._lib.clast_get_stats(self.ctx, C.byref(st)))
         return {f: getattr(st, f) for f, _ in N.clast_stats._fields_}
 
+    def int32_peak(self) -> float:
+        """Measured INT32 tera-ops/s of this GPU (clast_int32_peak)."""
+        v = C.c_double()
+        self._check(self._lib.clast_int32_peak(self.ctx, C.byref(v)))
+        return v.value
+
     def last_map_stats(self):
         ms = C.c_double()
         k = C.c_int64()

@@ -19,6 +19,8 @@ constexpr uint64_t kDroppedSeed = ~0ull;
 // CDeviceHashTable.cuh:13-16, reorganised for direct lookup).
 struct IndexView {
   int l;
+  int fshift;              // key >> fshift = bit of the presence filter
+  const uint32_t* filter;  // one bit per (key >> fshift) of every indexed key
   int shift;               // key >> shift = directory slot
   const uint32_t* dir;     // (1 << dir_bits) + 1 entries: first unique key with slot >= p
   const uint64_t* ukeys;   // unique valid keys, ascending
@@ -70,8 +72,12 @@ __device__ __forceinline__ bool kmer_at(const uint64_t* packed, const uint64_t* 
   return true;
 }
 
-// Index of key among the unique keys, or -1 (krnlBinarySearch.cu:3-33).
+// Index of key among the unique keys, or -1 (krnlBinarySearch.cu:3-33).  The
+// presence filter (<= 128 MB, mostly L2-resident) answers the common miss
+// without touching the directory or the key array.
 __device__ __forceinline__ int64_t index_lookup(const IndexView& ix, uint64_t key) {
+  const uint64_t fb = key >> ix.fshift;
+  if (!((ix.filter[fb >> 5] >> (fb & 31)) & 1u)) return -1;
   const uint32_t p = (uint32_t)(key >> ix.shift);
   int64_t lo = ix.dir[p];
   const int64_t end = ix.dir[p + 1];

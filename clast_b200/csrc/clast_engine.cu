@@ -90,19 +90,27 @@ struct clast_ctx {
 
 namespace {
 
+// Stream used for the stream-ordered allocations of the current API call.
+thread_local cudaStream_t g_alloc_stream = nullptr;
+
+// Owning device allocation from the device's stream-ordered memory pool
+// (cudaMallocAsync / cudaFreeAsync on the owning context's stream), so
+// steady-state calls reuse pool memory instead of calling cudaMalloc.
 template <class T>
-struct DevArray {  // owning device allocation
+struct DevArray {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t st = nullptr;
   DevArray() = default;
   DevArray(const DevArray&) = delete;
   DevArray& operator=(const DevArray&) = delete;
-  DevArray(DevArray&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevArray(DevArray&& o) noexcept : p(o.p), n(o.n), st(o.st) { o.p = nullptr; o.n = 0; }
   DevArray& operator=(DevArray&& o) noexcept {
     if (this != &o) {
       release();
       p = o.p;
       n = o.n;
+      st = o.st;
       o.p = nullptr;
       o.n = 0;
     }
@@ -111,14 +119,16 @@ struct DevArray {  // owning device allocation
   void alloc(size_t count) {
     release();
     n = count;
-    if (cudaMalloc(&p, (count ? count : 1) * sizeof(T)) != cudaSuccess) {
+    st = g_alloc_stream;
+    if (cudaMallocAsync(reinterpret_cast<void**>(&p), (count ? count : 1) * sizeof(T), st) != cudaSuccess) {
       (void)cudaGetLastError();
       p = nullptr;
+      n = 0;
       throw std::bad_alloc();
     }
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     n = 0;
   }
@@ -156,16 +166,18 @@ struct clast_index {
   int32_t nseqs = 0;
   DevArray<char> bases;  // padded
   DevArray<int32_t> gateway, lengths;
-  DevArray<uint32_t> dir;
+  DevArray<uint32_t> dir, filter;
   DevArray<uint64_t> ukeys;
   DevArray<int32_t> ustart, ucnt;
   DevArray<int2> entries;
   int64_t n_unique = 0, n_entries = 0;
-  int dir_bits = 1, shift = 0;
+  int dir_bits = 1, shift = 0, filter_bits = 1, fshift = 0;
 
   IndexView view() const {
     IndexView v;
     v.l = l;
+    v.fshift = fshift;
+    v.filter = filter.p;
     v.shift = shift;
     v.dir = dir.p;
     v.ukeys = ukeys.p;
@@ -242,6 +254,11 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix) {
   ix->shift = 2 * l - bits;
   ix->dir.alloc(((size_t)1 << bits) + 1);
   index_directory(ix->ukeys.p, nu, ix->shift, bits, ix->dir.p, st);
+  // presence filter over the top min(2l, 30) key bits (at most 128 MB)
+  ix->filter_bits = std::min(2 * l, 30);
+  ix->fshift = 2 * l - ix->filter_bits;
+  ix->filter.alloc((((size_t)1 << ix->filter_bits) + 31) / 32);
+  index_filter(ix->ukeys.p, nu, ix->fshift, ix->filter_bits, ix->filter.p, st);
   CLAST_CK(cudaStreamSynchronize(st));
 }
 
@@ -322,22 +339,25 @@ struct QueryBatch {
 };
 
 // Host copy of one batch's result (reference order within each query window).
-struct HostHits {
-  std::vector<int32_t> t_id, t_idx, q_id, q_idx, t_len, q_len, match, score;
-  std::vector<double> evalue;
-  size_t size() const { return t_id.size(); }
+// One batch's hits on the device, reads ascending (reference order within
+// every query window), with per-read offsets.
+struct DevHits {
+  int64_t n = 0;
+  DevArray<int32_t> t_id, t_idx, q_id, q_idx, t_len, q_len, match, score;
+  DevArray<double> evalue;
+  DevArray<int64_t> foff;
 };
 
 // CDeviceHitList for every query window of `qb` against one index.
 void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, const QueryBatch& qb,
-                  int32_t q_first, HostHits& out) {
+                  int32_t q_first, DevHits& out) {
   cudaStream_t st = c->st;
   Workspace& ws = c->ws;
   const QueryView q = qb.view();
   const IndexView iv = ix->view();
   const TargetView tv = ix->tview();
   const int64_t ns = qb.nstrands, nr = ns / 2;
-  out = HostHits();
+  out = DevHits();
   if (ns == 0 || ix->n_unique == 0) return;
   // createRawSeedList + deleteSeedsOnSequenceBoundary
   int64_t* cnt = ws.get<int64_t>("s_cnt", ns);
@@ -345,8 +365,9 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   unsigned long long* counters = ws.get<unsigned long long>("s_counters", 2);  // k-mers, DP cells
   CLAST_CK(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st));
   StageTimer& tm = c->timer;
+  int32_t* kidx = ws.get<int32_t>("s_kidx", (size_t)qb.n + 1);
   tm.begin(st);
-  seed_count(q, iv, cnt, counters, st);
+  seed_count(q, iv, cnt, counters, kidx, st);
   tm.end(StageTimer::SEED, st);
   scan_i64(ws, cnt, ns, off, st);
   const int64_t S = read_scalar(off + ns, st);
@@ -367,7 +388,7 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   uint32_t* sq = ws.get<uint32_t>("s_q", S);
   int32_t* nvalid = ws.get<int32_t>("s_nvalid", ns);
   tm.begin(st);
-  seed_write(q, iv, tv, p->gap, p->local, off, skey, sq, nvalid, st);
+  seed_write(q, iv, tv, p->gap, p->local, off, kidx, skey, sq, nvalid, st);
   tm.end(StageTimer::SEED, st);
   int32_t* wfirst = ws.get<int32_t>("s_wfirst", qb.nwin);
   window_first(nvalid, qb.wstart.p, qb.nwin, wfirst, st);
@@ -425,32 +446,14 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   c->stats.results += F;
   add_counters();
   if (F == 0) return;
-  FinalOut fo;
-  fo.t_id = ws.get<int32_t>("o_tid", F);
-  fo.t_idx = ws.get<int32_t>("o_tidx", F);
-  fo.q_id = ws.get<int32_t>("o_qid", F);
-  fo.q_idx = ws.get<int32_t>("o_qidx", F);
-  fo.t_len = ws.get<int32_t>("o_tlen", F);
-  fo.q_len = ws.get<int32_t>("o_qlen", F);
-  fo.match = ws.get<int32_t>("o_match", F);
-  fo.score = ws.get<int32_t>("o_score", F);
-  fo.evalue = ws.get<double>("o_e", F);
+  out.n = F;
+  out.t_id.alloc(F); out.t_idx.alloc(F); out.q_id.alloc(F); out.q_idx.alloc(F); out.t_len.alloc(F);
+  out.q_len.alloc(F); out.match.alloc(F); out.score.alloc(F); out.evalue.alloc(F);
+  out.foff.alloc(nr + 1);
+  CLAST_CK(cudaMemcpyAsync(out.foff.p, foff, (nr + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
+  FinalOut fo{out.t_id.p, out.t_idx.p, out.q_id.p, out.q_idx.p, out.t_len.p, out.q_len.p, out.match.p,
+              out.score.p, out.evalue.p};
   final_compact(fsel, roff, fcnt, foff, nr, hk, hs, o, ix->t_begin, q_first, fo, st);
-  auto d2h = [&](std::vector<int32_t>& v, const int32_t* d) {
-    v.resize(F);
-    CLAST_CK(cudaMemcpyAsync(v.data(), d, F * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-  };
-  d2h(out.t_id, fo.t_id);
-  d2h(out.t_idx, fo.t_idx);
-  d2h(out.q_id, fo.q_id);
-  d2h(out.q_idx, fo.q_idx);
-  d2h(out.t_len, fo.t_len);
-  d2h(out.q_len, fo.q_len);
-  d2h(out.match, fo.match);
-  d2h(out.score, fo.score);
-  out.evalue.resize(F);
-  CLAST_CK(cudaMemcpyAsync(out.evalue.data(), fo.evalue, F * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CLAST_CK(cudaStreamSynchronize(st));
 }
 
 template <class T>
@@ -535,6 +538,14 @@ int clast_ctx_create(int device, clast_ctx** out) {
   if (device < 0 || device >= ndev) return CLAST_ERR_ARG;
   if (cudaSetDevice(device) != cudaSuccess) return CLAST_ERR_CUDA;
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
+  {  // keep freed pool memory for reuse by later calls of this process
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    (void)cudaGetLastError();
+  }
   if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaEventCreate(&c->ev2) != cudaSuccess)
     return CLAST_ERR_CUDA;
@@ -567,6 +578,7 @@ int clast_index_build(clast_ctx* ctx, const clast_params* p, const char* bases, 
       throw std::invalid_argument("bad window arrays");
     if (n_bases >= INT32_MAX) throw std::invalid_argument("window larger than 2^31 bases");
     CLAST_CK(cudaSetDevice(ctx->device));
+    g_alloc_stream = ctx->st;
     g_kernel_launches = 0;
     ctx->stats.index_ms = ctx->stats.index_upload_ms = 0;
     ctx->stats.index_launches = 0;
@@ -592,6 +604,7 @@ int clast_search(clast_ctx* ctx, const clast_index* ix, const clast_params* p, c
     if (n_qbases < 0 || (n_qbases > 0 && !q_bases) || (n_qseqs > 0 && (!q_gateway || !q_lengths)))
       throw std::invalid_argument("bad query arrays");
     CLAST_CK(cudaSetDevice(ctx->device));
+    g_alloc_stream = ctx->st;
     g_kernel_launches = 0;
     cudaStream_t st = ctx->st;
     QueryBatch qb;
@@ -615,18 +628,21 @@ int clast_search(clast_ctx* ctx, const clast_index* ix, const clast_params* p, c
     qb.wstart.alloc(2);
     CLAST_CK(cudaMemcpyAsync(qb.wstart.p, ws2, sizeof(ws2), cudaMemcpyHostToDevice, st));
     qb.pack(st);
-    HostHits h;
+    DevHits h;
     search_batch(ctx, ix, p, qb, q_begin, h);
-    out->n = (int64_t)h.size();
-    out->t_id = host_copy(h.t_id);
-    out->t_idx = host_copy(h.t_idx);
-    out->q_id = host_copy(h.q_id);
-    out->q_idx = host_copy(h.q_idx);
-    out->t_len = host_copy(h.t_len);
-    out->q_len = host_copy(h.q_len);
-    out->match = host_copy(h.match);
-    out->score = host_copy(h.score);
-    out->evalue = host_copy(h.evalue);
+    const int64_t F = h.n;
+    out->n = F;
+    auto d2h32 = [&](int32_t*& dst, const DevArray<int32_t>& src) {
+      dst = static_cast<int32_t*>(std::malloc((F ? F : 1) * sizeof(int32_t)));
+      if (!dst) throw std::bad_alloc();
+      if (F) CLAST_CK(cudaMemcpyAsync(dst, src.p, F * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    };
+    d2h32(out->t_id, h.t_id); d2h32(out->t_idx, h.t_idx); d2h32(out->q_id, h.q_id); d2h32(out->q_idx, h.q_idx);
+    d2h32(out->t_len, h.t_len); d2h32(out->q_len, h.q_len); d2h32(out->match, h.match); d2h32(out->score, h.score);
+    out->evalue = static_cast<double*>(std::malloc((F ? F : 1) * sizeof(double)));
+    if (!out->evalue) throw std::bad_alloc();
+    if (F) CLAST_CK(cudaMemcpyAsync(out->evalue, h.evalue.p, F * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CLAST_CK(cudaStreamSynchronize(st));
     ctx->last_launches = g_kernel_launches;
     return CLAST_OK;
   });
@@ -651,6 +667,7 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
     for (int32_t k = 0; k < n_loads; ++k) total += load_sizes[k];
     if (total != targets->n_seqs) throw std::invalid_argument("load sizes do not add up to n_seqs");
     CLAST_CK(cudaSetDevice(ctx->device));
+    g_alloc_stream = ctx->st;
     g_kernel_launches = 0;
     ctx->stats.index_ms = ctx->stats.index_upload_ms = 0;
     ctx->stats.index_launches = 0;
@@ -749,6 +766,7 @@ int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int
       if (p->lmer != w.ix->l || p->stride != w.ix->stride || p->cut_repeat != w.ix->cut)
         throw std::invalid_argument("params differ from the ones the targets were built with");
     CLAST_CK(cudaSetDevice(ctx->device));
+    g_alloc_stream = ctx->st;
     g_kernel_launches = 0;
     cudaStream_t st = ctx->st;
     clast_stats& S = ctx->stats;
@@ -796,8 +814,59 @@ int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int
     qb.pack(st);
     S.query_bases = qb.n;
     // every target window, in holder order (target load, window)
-    std::vector<HostHits> per_win(T->wins.size());
+    std::vector<DevHits> per_win(T->wins.size());
     for (size_t w = 0; w < T->wins.size(); ++w) search_batch(ctx, T->wins[w].ix.get(), p, qb, 0, per_win[w]);
+    // fixResult: stable merge by (read, score desc) over the windows, on the device
+    std::vector<WinHits> wh;
+    int64_t n_items = 0;
+    for (size_t w = 0; w < T->wins.size(); ++w) {
+      const DevHits& h = per_win[w];
+      if (h.n == 0) continue;
+      wh.push_back(WinHits{h.t_id.p, h.t_idx.p, h.q_id.p, h.q_idx.p, h.t_len.p, h.q_len.p, h.match.p, h.score.p,
+                           h.evalue.p, h.foff.p, n_items, T->wins[w].load});
+      n_items += h.n;
+    }
+    DevArray<WinHits> dwh;
+    dwh.alloc(wh.size());
+    if (!wh.empty())
+      CLAST_CK(cudaMemcpyAsync(dwh.p, wh.data(), wh.size() * sizeof(WinHits), cudaMemcpyHostToDevice, st));
+    const int64_t F = n_items;
+    DevArray<int32_t> m_read, m_strand, m_load, m_seq, m_tidx, m_qidx, m_tlen, m_qlen, m_match, m_score;
+    DevArray<double> m_e;
+    for (auto* a : {&m_read, &m_strand, &m_load, &m_seq, &m_tidx, &m_qidx, &m_tlen, &m_qlen, &m_match, &m_score})
+      a->alloc(F);
+    m_e.alloc(F);
+    int32_t* mcnt = ctx->ws.get<int32_t>("m_cnt", nreads + 1);
+    int64_t* moff = ctx->ws.get<int64_t>("m_off", nreads + 1);
+    MapOut mo{m_read.p, m_strand.p, m_load.p, m_seq.p, m_tidx.p, m_qidx.p, m_tlen.p, m_qlen.p, m_match.p,
+              m_score.p, m_e.p};
+    merge_windows(dwh.p, (int)wh.size(), n_items, nreads, mcnt, moff, mo, ctx->ws, st);
+    // per query load offsets
+    std::vector<int64_t> lf(load_first.begin(), load_first.end());
+    DevArray<int64_t> dlf, dlo;
+    dlf.alloc(lf.size());
+    dlo.alloc(lf.size());
+    CLAST_CK(cudaMemcpyAsync(dlf.p, lf.data(), lf.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    if (nreads > 0) gather_i64(moff, dlf.p, (int)lf.size(), dlo.p, st);
+    clast_map_result res;
+    std::memset(&res, 0, sizeof(res));
+    res.n = F;
+    res.load_offsets = static_cast<int64_t*>(std::calloc(n_loads + 1, sizeof(int64_t)));
+    if (!res.load_offsets) throw std::bad_alloc();
+    if (nreads > 0)
+      CLAST_CK(cudaMemcpyAsync(res.load_offsets, dlo.p, (n_loads + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                               st));
+    auto d2h32 = [&](int32_t*& dst, const DevArray<int32_t>& src) {
+      dst = static_cast<int32_t*>(std::malloc((F ? F : 1) * sizeof(int32_t)));
+      if (!dst) throw std::bad_alloc();
+      if (F) CLAST_CK(cudaMemcpyAsync(dst, src.p, F * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    };
+    d2h32(res.read, m_read); d2h32(res.strand, m_strand); d2h32(res.t_load, m_load); d2h32(res.t_seq, m_seq);
+    d2h32(res.t_idx, m_tidx); d2h32(res.q_idx, m_qidx); d2h32(res.t_len, m_tlen); d2h32(res.q_len, m_qlen);
+    d2h32(res.match, m_match); d2h32(res.score, m_score);
+    res.evalue = static_cast<double*>(std::malloc((F ? F : 1) * sizeof(double)));
+    if (!res.evalue) throw std::bad_alloc();
+    if (F) CLAST_CK(cudaMemcpyAsync(res.evalue, m_e.p, F * sizeof(double), cudaMemcpyDeviceToHost, st));
     CLAST_CK(cudaEventRecord(ctx->ev2, st));
     CLAST_CK(cudaEventSynchronize(ctx->ev2));
     float up = 0, ms = 0;
@@ -815,59 +884,6 @@ int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int
     S.final_ms = ctx->timer.ms[StageTimer::FINAL];
     ctx->last_ms = up + ms;
     ctx->last_launches = g_kernel_launches;
-    // fixResult: per read, stable merge by score desc over the windows in holder order
-    std::vector<std::vector<std::pair<int64_t, int64_t>>> ranges(T->wins.size());
-    std::vector<int64_t> per_read(nreads + 1, 0);
-    for (size_t w = 0; w < T->wins.size(); ++w) {
-      const HostHits& h = per_win[w];
-      for (size_t i = 0; i < h.size(); ++i) per_read[h.q_id[i] / 2 + 1]++;
-    }
-    for (int64_t r = 0; r < nreads; ++r) per_read[r + 1] += per_read[r];
-    const int64_t F = per_read[nreads];
-    clast_map_result res;
-    std::memset(&res, 0, sizeof(res));
-    res.n = F;
-    auto alloc32 = [&](int32_t*& q) {
-      q = static_cast<int32_t*>(std::malloc((F ? F : 1) * sizeof(int32_t)));
-      if (!q) throw std::bad_alloc();
-    };
-    alloc32(res.read); alloc32(res.strand); alloc32(res.t_load); alloc32(res.t_seq); alloc32(res.t_idx);
-    alloc32(res.q_idx); alloc32(res.t_len); alloc32(res.q_len); alloc32(res.match); alloc32(res.score);
-    res.evalue = static_cast<double*>(std::malloc((F ? F : 1) * sizeof(double)));
-    res.load_offsets = static_cast<int64_t*>(std::malloc((n_loads + 1) * sizeof(int64_t)));
-    if (!res.evalue || !res.load_offsets) throw std::bad_alloc();
-    for (int32_t k = 0; k <= n_loads; ++k) res.load_offsets[k] = per_read[load_first[k]];
-    std::vector<int64_t> fill(per_read.begin(), per_read.end() - 1);
-    struct Ref { int32_t w; int64_t i; };
-    std::vector<Ref> refs(F);
-    for (size_t w = 0; w < T->wins.size(); ++w) {
-      const HostHits& h = per_win[w];
-      for (size_t i = 0; i < h.size(); ++i) refs[fill[h.q_id[i] / 2]++] = Ref{(int32_t)w, (int64_t)i};
-    }
-#pragma omp parallel for schedule(dynamic, 4096)
-    for (int64_t r = 0; r < nreads; ++r) {
-      const int64_t a = per_read[r], b = per_read[r + 1];
-      if (b - a > 1)
-        std::stable_sort(refs.begin() + a, refs.begin() + b, [&](const Ref& x, const Ref& y) {
-          return per_win[x.w].score[x.i] > per_win[y.w].score[y.i];
-        });
-      for (int64_t j = a; j < b; ++j) {
-        const HostHits& h = per_win[refs[j].w];
-        const int64_t i = refs[j].i;
-        const auto& win = T->wins[refs[j].w];
-        res.read[j] = h.q_id[i] / 2;
-        res.strand[j] = h.q_id[i] & 1;
-        res.t_load[j] = win.load;
-        res.t_seq[j] = h.t_id[i];
-        res.t_idx[j] = h.t_idx[i];
-        res.q_idx[j] = h.q_idx[i];
-        res.t_len[j] = h.t_len[i];
-        res.q_len[j] = h.q_len[i];
-        res.match[j] = h.match[i];
-        res.score[j] = h.score[i];
-        res.evalue[j] = h.evalue[i];
-      }
-    }
     *out = res;
     return CLAST_OK;
   });
@@ -879,6 +895,16 @@ void clast_map_result_free(clast_map_result* r) {
   std::free(r->t_seq); std::free(r->t_idx); std::free(r->q_idx); std::free(r->t_len); std::free(r->q_len);
   std::free(r->match); std::free(r->score); std::free(r->evalue);
   std::memset(r, 0, sizeof(*r));
+}
+
+int clast_int32_peak(clast_ctx* ctx, double* tera_ops) {
+  if (!ctx || !tera_ops) return CLAST_ERR_ARG;
+  return guarded(ctx, [&]() -> int {
+    CLAST_CK(cudaSetDevice(ctx->device));
+    int* sink = ctx->ws.get<int>("probe_sink", 1);
+    *tera_ops = int32_probe(ctx->st, sink);
+    return CLAST_OK;
+  });
 }
 
 int clast_get_stats(const clast_ctx* ctx, clast_stats* out) {

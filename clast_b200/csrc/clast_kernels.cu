@@ -155,20 +155,19 @@ __global__ void k_strand_meta(const int64_t* __restrict__ off, int64_t n_reads, 
   slen[2 * r + 1] = (int32_t)len;
 }
 
+// One warp per read: the '+' strand copy and the reverse complement are both
+// coalesced (the reversed writes of a warp still cover one contiguous run).
 __global__ void k_strands(const char* __restrict__ reads, const int64_t* __restrict__ off, int64_t n_reads,
-                          int64_t n_bases, char* __restrict__ out) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_bases) return;
-  int64_t lo = 0, hi = n_reads;  // last read with off[r] <= i
-  while (hi - lo > 1) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (off[mid] <= i) lo = mid;
-    else hi = mid;
+                          char* __restrict__ out) {
+  const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n_reads) return;
+  const int64_t a = off[r], len = off[r + 1] - a;
+  for (int64_t j = lane; j < len; j += 32) {
+    const char c = reads[a + j];
+    out[2 * a + j] = c;
+    out[2 * a + len + (len - 1 - j)] = complement(c);
   }
-  const int64_t a = off[lo], len = off[lo + 1] - a, j = i - a;
-  const char c = reads[i];
-  out[2 * a + j] = c;
-  out[2 * a + len + (len - 1 - j)] = complement(c);
 }
 
 // Base array of one target window: every sequence followed by its first l-1
@@ -177,14 +176,22 @@ __global__ void k_strands(const char* __restrict__ reads, const int64_t* __restr
 __global__ void k_build_window(const char* __restrict__ src, const int64_t* __restrict__ src_off,
                                const int32_t* __restrict__ gw, const int32_t* __restrict__ len, int nseqs,
                                int64_t n, char* __restrict__ out) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int lo = 0, hi = nseqs;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if ((int64_t)gw[mid] <= i) lo = mid;
-    else hi = mid;
+  __shared__ int first_seq;
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x;
+  if (threadIdx.x == 0) {  // sequence of the block's first base; others walk forward from it
+    int lo = 0, hi = nseqs;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if ((int64_t)gw[mid] <= i0) lo = mid;
+      else hi = mid;
+    }
+    first_seq = lo;
   }
+  __syncthreads();
+  const int64_t i = i0 + threadIdx.x;
+  if (i >= n) return;
+  int lo = first_seq;
+  while (lo + 1 < nseqs && (int64_t)gw[lo + 1] <= i) ++lo;
   const int64_t j = i - gw[lo];
   const int64_t L = len[lo];
   char c;
@@ -338,6 +345,14 @@ __global__ void k_index_buckets(const int64_t* __restrict__ ufirst, const int64_
   ucnt[k] = (int32_t)(b - a);
 }
 
+__global__ void k_index_filter(const uint64_t* __restrict__ ukeys, int64_t nu, int fshift,
+                               uint32_t* __restrict__ filter) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nu) return;
+  const uint64_t fb = ukeys[k] >> fshift;
+  atomicOr(&filter[fb >> 5], 1u << (fb & 31));
+}
+
 __global__ void k_index_dir(const uint64_t* __restrict__ ukeys, int64_t nu, int shift, int64_t nslots,
                             uint32_t* __restrict__ dir) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -356,7 +371,7 @@ __global__ void k_index_dir(const uint64_t* __restrict__ ukeys, int64_t nu, int 
 // seeds
 // ------------------------------------------------------------------------
 __global__ void k_seed_count(QueryView q, IndexView ix, int64_t* __restrict__ cnt,
-                             unsigned long long* __restrict__ n_kmers) {
+                             unsigned long long* __restrict__ n_kmers, int32_t* __restrict__ kidx) {
   const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (s >= q.nstrands) return;
@@ -366,11 +381,17 @@ __global__ void k_seed_count(QueryView q, IndexView ix, int64_t* __restrict__ cn
   int valid = 0;
   for (int qi = lane; qi < nk; qi += 32) {
     uint64_t key;
+    int32_t hit = -1;
     if (kmer_at(q.packed, q.nmask, st + qi, ix.l, key)) {
       ++valid;
       const int64_t u = index_lookup(ix, key);
-      if (u >= 0) sum += ix.ucnt[u];
+      if (u >= 0) {
+        const int c = ix.ucnt[u];
+        sum += c;
+        if (c > 0) hit = (int32_t)u;
+      }
     }
+    kidx[st + qi] = hit;  // the write pass reuses the lookup
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) {
@@ -384,8 +405,9 @@ __global__ void k_seed_count(QueryView q, IndexView ix, int64_t* __restrict__ cn
 }
 
 __global__ void k_seed_write(QueryView q, IndexView ix, TargetView t, int gap, int local,
-                             const int64_t* __restrict__ off, uint64_t* __restrict__ skey,
-                             uint32_t* __restrict__ sq, int32_t* __restrict__ nvalid) {
+                             const int64_t* __restrict__ off, const int32_t* __restrict__ kidx,
+                             uint64_t* __restrict__ skey, uint32_t* __restrict__ sq,
+                             int32_t* __restrict__ nvalid) {
   const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (s >= q.nstrands) return;
@@ -398,13 +420,10 @@ __global__ void k_seed_write(QueryView q, IndexView ix, TargetView t, int gap, i
     const int qi = c0 + lane;
     int c = 0, us = 0;
     if (qi < nk) {
-      uint64_t key;
-      if (kmer_at(q.packed, q.nmask, st + qi, ix.l, key)) {
-        const int64_t u = index_lookup(ix, key);
-        if (u >= 0) {
-          c = ix.ucnt[u];
-          us = ix.ustart[u];
-        }
+      const int32_t u = kidx[st + qi];
+      if (u >= 0) {
+        c = ix.ucnt[u];
+        us = ix.ustart[u];
       }
     }
     int incl = c;
@@ -455,12 +474,19 @@ template <class K2, bool PAY>
 __global__ void k_classify(const int32_t* __restrict__ len, int64_t nseg, int32_t* __restrict__ lists,
                            int32_t* __restrict__ counts) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nseg) return;
-  const int n = len[i];
-  if (n <= 1) return;
-  const int tier = (n <= 32) ? 0 : (n <= 2048 ? 1 : 2);
-  const int slot = atomicAdd(&counts[tier], 1);
-  lists[(int64_t)tier * nseg + slot] = (int32_t)i;
+  const int n = (i < nseg) ? len[i] : 0;
+  const int tier = (n <= 1) ? -1 : ((n <= 32) ? 0 : (n <= 2048 ? 1 : 2));
+  const int lane = threadIdx.x & 31;
+  // one atomic per warp and tier
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    const unsigned m = __ballot_sync(kFull, tier == t);
+    if (!m) continue;
+    int base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd(&counts[t], __popc(m));
+    base = __shfl_sync(kFull, base, __ffs(m) - 1);
+    if (tier == t) lists[(int64_t)t * nseg + base + __popc(m & lanemask_lt())] = (int32_t)i;
+  }
 }
 
 template <class K2, bool PAY>
@@ -698,10 +724,13 @@ __global__ void k_gather_hits(const uint64_t* __restrict__ skey, const uint32_t*
                               int32_t* __restrict__ hq, int32_t* __restrict__ hs, const int32_t* __restrict__ qlen,
                               int l, int band, unsigned long long* __restrict__ cells) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nstrands) return;
-  const int n = hcnt[s];
+  const int n = (s < nstrands) ? hcnt[s] : 0;
   // every hit of the strand fills band * (qlen - l) cells: backward rows + forward rows
-  if (n) atomicAdd(cells, (unsigned long long)n * (unsigned long long)band * (unsigned long long)(qlen[s] - l));
+  unsigned long long c = n ? (unsigned long long)n * (unsigned long long)band * (unsigned long long)(qlen[s] - l) : 0;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(cells, c);
+  if (s >= nstrands) return;
   const int64_t a = off[s], b = hoff[s];
   for (int i = 0; i < n; ++i) {
     hk[b + i] = skey[a + i];
@@ -960,6 +989,88 @@ __global__ void k_final_compact(const int32_t* __restrict__ fsel, const int64_t*
   }
 }
 
+// ------------------------------------------------------------------------
+// merge of the per-window results in holder order (CHostResultHolder::fixResult)
+// ------------------------------------------------------------------------
+__global__ void k_merge_count(const WinHits* __restrict__ w, int nw, int64_t nreads, int32_t* __restrict__ cnt) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nreads) return;
+  int64_t c = 0;
+  for (int i = 0; i < nw; ++i) c += w[i].foff[r + 1] - w[i].foff[r];
+  cnt[r] = (int32_t)c;
+}
+
+// Item j of window wi goes after every item of the same read from an earlier
+// window with score >= its score, and every item of a later window with a
+// strictly higher score: the stable sort by (read, score desc) of the
+// concatenation in window order.
+__global__ void k_merge_place(const WinHits* __restrict__ w, int nw, int64_t total, const int64_t* __restrict__ moff,
+                              MapOut out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  int wi = 0;
+  while (wi + 1 < nw && w[wi + 1].base <= i) ++wi;
+  const WinHits& a = w[wi];
+  const int64_t j = i - a.base;
+  const int qid = a.q_id[j];
+  const int64_t r = qid >> 1;
+  const int sc = a.score[j];
+  int64_t pos = moff[r] + (j - a.foff[r]);
+  for (int k = 0; k < nw; ++k) {
+    if (k == wi) continue;
+    const WinHits& b = w[k];
+    int64_t lo = b.foff[r], hi = b.foff[r + 1];
+    const int64_t first = lo;
+    // scores are non-increasing within a read: count the prefix that precedes sc
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      const int v = b.score[mid];
+      if (k < wi ? v >= sc : v > sc) lo = mid + 1;
+      else hi = mid;
+    }
+    pos += lo - first;
+  }
+  out.read[pos] = qid >> 1;
+  out.strand[pos] = qid & 1;
+  out.t_load[pos] = a.load;
+  out.t_seq[pos] = a.t_id[j];
+  out.t_idx[pos] = a.t_idx[j];
+  out.q_idx[pos] = a.q_idx[j];
+  out.t_len[pos] = a.t_len[j];
+  out.q_len[pos] = a.q_len[j];
+  out.match[pos] = a.match[j];
+  out.score[pos] = sc;
+  out.evalue[pos] = a.evalue[j];
+}
+
+// INT32 throughput probe: 8 independent chains per thread of the DP's
+// integer operation mix (add, max, logic): 4 ops per chain and iteration.
+__global__ void __launch_bounds__(256) k_int32_probe(int iters, int k1, int k2, int* __restrict__ sink) {
+  int a[8], b[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    a[c] = threadIdx.x + c * k1;
+    b[c] = blockIdx.x - c * k2;
+  }
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      a[c] = max(a[c] + k1, b[c]);
+      b[c] = (b[c] ^ a[c]) + k2;
+    }
+  }
+  int x = 0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) x += a[c] ^ b[c];
+  if (x == 0x7fffffff) sink[0] = x;  // keeps the chains live
+}
+
+__global__ void k_gather_i64(const int64_t* __restrict__ src, const int64_t* __restrict__ idx, int n,
+                             int64_t* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = src[idx[i]];
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------
@@ -984,7 +1095,7 @@ void build_strands(const char* reads, const int64_t* offsets, int64_t n_reads, i
   k_strand_meta<<<blocks_for(n_reads, 256), 256, 0, st>>>(offsets, n_reads, strand_start, strand_len);
   CLAST_LAUNCHED();
   if (n_bases > 0) {
-    k_strands<<<blocks_for(n_bases, 256), 256, 0, st>>>(reads, offsets, n_reads, n_bases, strands);
+    k_strands<<<blocks_for(n_reads * 32, 256), 256, 0, st>>>(reads, offsets, n_reads, strands);
     CLAST_LAUNCHED();
   }
 }
@@ -1065,6 +1176,15 @@ void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n_unique,
   k_index_buckets<<<blocks_for(n_unique, 256), 256, 0, st>>>(ufirst, kpos, n_unique, ustart, ucnt);
   CLAST_LAUNCHED();
 }
+void index_filter(const uint64_t* ukeys, int64_t n_unique, int fshift, int filter_bits, uint32_t* filter,
+                  cudaStream_t st) {
+  const int64_t words = ((1ll << filter_bits) + 31) / 32;
+  CLAST_CK(cudaMemsetAsync(filter, 0, words * sizeof(uint32_t), st));
+  if (n_unique <= 0) return;
+  k_index_filter<<<blocks_for(n_unique, 256), 256, 0, st>>>(ukeys, n_unique, fshift, filter);
+  CLAST_LAUNCHED();
+}
+
 void index_directory(const uint64_t* ukeys, int64_t n_unique, int shift, int dir_bits, uint32_t* dir,
                      cudaStream_t st) {
   const int64_t nslots = 1ll << dir_bits;
@@ -1073,16 +1193,17 @@ void index_directory(const uint64_t* ukeys, int64_t n_unique, int shift, int dir
 }
 
 void seed_count(const QueryView& q, const IndexView& ix, int64_t* cnt, unsigned long long* n_kmers,
-                cudaStream_t st) {
+                int32_t* kidx, cudaStream_t st) {
   if (q.nstrands <= 0) return;
-  k_seed_count<<<blocks_for((int64_t)q.nstrands * 32, 256), 256, 0, st>>>(q, ix, cnt, n_kmers);
+  k_seed_count<<<blocks_for((int64_t)q.nstrands * 32, 256), 256, 0, st>>>(q, ix, cnt, n_kmers, kidx);
   CLAST_LAUNCHED();
 }
 void seed_write(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
-                const int64_t* off, uint64_t* skey, uint32_t* sq, int32_t* nvalid, cudaStream_t st) {
+                const int64_t* off, const int32_t* kidx, uint64_t* skey, uint32_t* sq, int32_t* nvalid,
+                cudaStream_t st) {
   if (q.nstrands <= 0) return;
-  k_seed_write<<<blocks_for((int64_t)q.nstrands * 32, 256), 256, 0, st>>>(q, ix, t, gap, local, off, skey, sq,
-                                                                           nvalid);
+  k_seed_write<<<blocks_for((int64_t)q.nstrands * 32, 256), 256, 0, st>>>(q, ix, t, gap, local, off, kidx, skey,
+                                                                           sq, nvalid);
   CLAST_LAUNCHED();
 }
 void window_first(const int32_t* nvalid, const int32_t* win_start, int n_windows, int32_t* win_first,
@@ -1145,6 +1266,47 @@ void banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, cons
     case 16: launch_dp_gap<16>(a, local, st); break;
     default: throw std::invalid_argument("gap out of range 2..16");
   }
+}
+
+void merge_windows(const WinHits* wins, int nw, int64_t total, int64_t nreads, int32_t* cnt, int64_t* moff,
+                   const MapOut& out, Workspace& ws, cudaStream_t st) {
+  if (nreads <= 0) return;
+  k_merge_count<<<blocks_for(nreads, 256), 256, 0, st>>>(wins, nw, nreads, cnt);
+  CLAST_LAUNCHED();
+  scan_i32(ws, cnt, nreads, moff, st);
+  if (total > 0) {
+    k_merge_place<<<blocks_for(total, 256), 256, 0, st>>>(wins, nw, total, moff, out);
+    CLAST_LAUNCHED();
+  }
+}
+
+double int32_probe(cudaStream_t st, int* sink) {
+  int dev = 0, sms = 0;
+  CLAST_CK(cudaGetDevice(&dev));
+  CLAST_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int blocks = sms * 8, threads = 256, iters = 4096;
+  cudaEvent_t a, b;
+  CLAST_CK(cudaEventCreate(&a));
+  CLAST_CK(cudaEventCreate(&b));
+  k_int32_probe<<<blocks, threads, 0, st>>>(64, 3, 5, sink);  // warm-up
+  CLAST_LAUNCHED();
+  CLAST_CK(cudaEventRecord(a, st));
+  k_int32_probe<<<blocks, threads, 0, st>>>(iters, 3, 5, sink);
+  CLAST_LAUNCHED();
+  CLAST_CK(cudaEventRecord(b, st));
+  CLAST_CK(cudaEventSynchronize(b));
+  float ms = 0;
+  CLAST_CK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  const double ops = (double)blocks * threads * iters * 8 * 4;
+  return ops / (ms * 1e-3) / 1e12;
+}
+
+void gather_i64(const int64_t* src, const int64_t* idx, int n, int64_t* out, cudaStream_t st) {
+  if (n <= 0) return;
+  k_gather_i64<<<blocks_for(n, 256), 256, 0, st>>>(src, idx, n, out);
+  CLAST_LAUNCHED();
 }
 
 void final_keys(const uint64_t* hk, const int32_t* hq, const int32_t* hs, const DpOut& o, int64_t n_hits,

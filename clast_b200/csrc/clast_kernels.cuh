@@ -50,13 +50,18 @@ void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n_unique,
                    int32_t* ucnt, cudaStream_t st);
 void index_directory(const uint64_t* ukeys, int64_t n_unique, int shift, int dir_bits, uint32_t* dir,
                      cudaStream_t st);
+// Presence filter: bit (key >> fshift) set for every unique key; 2^filter_bits bits.
+void index_filter(const uint64_t* ukeys, int64_t n_unique, int fshift, int filter_bits, uint32_t* filter,
+                  cudaStream_t st);
 
 // ---- seeds (CDeviceHitList_createRawSeedList.cu, _deleteSeeds*.cu, _sortSeeds.cu) ----
-// cnt[s] = seeds of strand s before the corner filter; *n_kmers += valid l-mers
+// cnt[s] = seeds of strand s before the corner filter; *n_kmers += valid l-mers;
+// kidx[f] = unique-key index of the l-mer at strand position f, -1 when it seeds nothing
 void seed_count(const QueryView& q, const IndexView& ix, int64_t* cnt, unsigned long long* n_kmers,
-                cudaStream_t st);
+                int32_t* kidx, cudaStream_t st);
 void seed_write(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
-                const int64_t* off, uint64_t* skey, uint32_t* sq, int32_t* nvalid, cudaStream_t st);
+                const int64_t* off, const int32_t* kidx, uint64_t* skey, uint32_t* sq, int32_t* nvalid,
+                cudaStream_t st);
 void window_first(const int32_t* nvalid, const int32_t* win_start, int n_windows, int32_t* win_first,
                   cudaStream_t st);
 
@@ -104,5 +109,26 @@ struct FinalOut {
 void final_compact(const int32_t* fsel, const int64_t* roff, const int32_t* fcnt, const int64_t* foff,
                    int64_t n_reads, const uint64_t* hk, const int32_t* hs, const DpOut& o, int32_t t_first,
                    int32_t q_first, const FinalOut& out, cudaStream_t st);
+
+// ---- merge of target windows in holder order (CHostResultHolder::fixResult) ----
+struct WinHits {  // one target window's final hits (reads ascending)
+  const int32_t* t_id; const int32_t* t_idx; const int32_t* q_id; const int32_t* q_idx;
+  const int32_t* t_len; const int32_t* q_len; const int32_t* match; const int32_t* score;
+  const double* evalue;
+  const int64_t* foff;  // per read offsets, n_reads + 1
+  int64_t base;         // position of its first item in the concatenation of all windows
+  int32_t load;         // target RAM load of the window
+};
+struct MapOut {
+  int32_t* read; int32_t* strand; int32_t* t_load; int32_t* t_seq; int32_t* t_idx; int32_t* q_idx;
+  int32_t* t_len; int32_t* q_len; int32_t* match; int32_t* score; double* evalue;
+};
+// wins: device array of nw windows; total = items of all windows; moff (nreads+1)
+// receives per-read offsets of the merged result.
+void merge_windows(const WinHits* wins, int nw, int64_t total, int64_t nreads, int32_t* cnt, int64_t* moff,
+                   const MapOut& out, Workspace& ws, cudaStream_t st);
+void gather_i64(const int64_t* src, const int64_t* idx, int n, int64_t* out, cudaStream_t st);
+// Measured INT32 throughput of this GPU in tera-ops/s (add, max, logic mix).
+double int32_probe(cudaStream_t st, int* sink);
 
 }  // namespace clast

@@ -176,6 +176,12 @@ typedef struct clast_stats {
 } clast_stats;
 int clast_get_stats(const clast_ctx* ctx, clast_stats* out);
 
+/* Measurement helper, not part of the reference's seam: INT32 throughput of
+ * the context's GPU (tera-ops/s) on the banded DP's operation mix (integer
+ * add, max and logic; a fused add+max counts as two ops).  The roofline
+ * denominator of the DP stage. */
+int clast_int32_peak(clast_ctx* ctx, double* tera_ops);
+
 #ifdef __cplusplus
 }
 #endif
