@@ -201,15 +201,30 @@ def run_ours(args):
     q_dev = q_pin.to("cuda", non_blocking=False)
     torch.cuda.synchronize()
 
+    host = {"targets_ms": 0.0, "map_ms": 0.0, "close_ms": 0.0, "n": 0, "py": [0.0, 0.0, 0.0]}
+
     def step(tb, qb):
+        c0 = time.perf_counter()
         T = eng.targets(s, tb, t.offsets, t_loads, int(T_VRAM))
+        c1 = time.perf_counter()
         res = eng.map(s, T, qb, q.offsets, q_loads, int(Q_VRAM))
+        c2 = time.perf_counter()
         T.close()
+        c3 = time.perf_counter()
+        host["targets_ms"] += (c1 - c0) * 1e3
+        host["map_ms"] += (c2 - c1) * 1e3
+        host["close_ms"] += (c3 - c2) * 1e3
+        host["n"] += 1
+        for i in range(3):
+            host["py"][i] += eng.last_map_py_ms[i]
         return res
 
     def timed(tb, qb, sampler=None):
         for _ in range(args.warmup):
             step(tb, qb)
+        for k in ("targets_ms", "map_ms", "close_ms", "n"):
+            host[k] = 0
+        host["py"] = [0.0, 0.0, 0.0]
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -229,11 +244,17 @@ def run_ours(args):
             x = torch.tensor([ms], device="cuda")
             dist.all_reduce(x, op=dist.ReduceOp.MAX)
             ms = float(x.item())
-        return ms, launches, res, st
+        n = max(1, host["n"])
+        hw = {"targets_call": round(host["targets_ms"] / n, 3), "map_call": round(host["map_ms"] / n, 3),
+              "targets_free": round(host["close_ms"] / n, 3),
+              "inside_targets": round(st["index_wall_ms"], 3), "inside_map": round(st["map_wall_ms"], 3),
+              "map_host_prep": round(st["map_prep_ms"], 3), "map_whole_call": round(st["map_call_ms"], 3),
+              "map_py_before_call_ctypes_call_after": [round(x / n, 3) for x in host["py"]]}
+        return ms, launches, res, st, hw
 
     with ClockSampler(local) as clk:
-        ms_dev, launches, res, st = timed(t_dev, q_dev)
-    ms_e2e, _, res2, st2 = timed(t_pin, q_pin)
+        ms_dev, launches, res, st, hw_dev = timed(t_dev, q_dev)
+    ms_e2e, _, res2, st2, hw_e2e = timed(t_pin, q_pin)
     assert np.array_equal(res["score"], res2["score"])
     mbp_rank = q.offsets[-1] / 1e6
     value = mbp_rank * world * args.steps / (ms_dev / 1e3)
@@ -257,6 +278,7 @@ def run_ours(args):
         "traffic": None,
         "stage_ms_per_step": {k: round(v, 3) for k, v in stages.items()},
         "step_device_ms": round(st["index_ms"] + st["map_ms"], 3),
+        "index_ms": round(st["index_ms"], 3), "map_ms": round(st["map_ms"], 3),
         "dp": {"cells": st["dp_cells"], "ms": round(st["dp_ms"], 3), "launches": st["dp_launches"],
                "gcups": round(st["dp_cells"] / (st["dp_ms"] / 1e3) / 1e9, 1) if st["dp_ms"] > 0 else None,
                "int32_ops_per_cell": 13,
@@ -281,6 +303,7 @@ def run_ours(args):
         "counts_per_step": {k: st[k] for k in ("query_bases", "query_kmers", "seeds", "hits", "results",
                                                "dp_cells", "index_launches", "map_launches")},
         "clocks": clk.summary(),
+        "host_wall_ms_per_step": {"value_loop": hw_dev, "e2e_loop": hw_e2e},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -35,7 +35,7 @@ class clast_map_result(C.Structure):
     _fields_ = [("n", C.c_int64), ("load_offsets", C.POINTER(C.c_int64))] + \
                [(f, C.POINTER(C.c_int32)) for f in ("read", "strand", "t_load", "t_seq", "t_idx", "q_idx",
                                                    "t_len", "q_len", "match", "score")] + \
-               [("evalue", C.POINTER(C.c_double))]
+               [("evalue", C.POINTER(C.c_double)), ("owner", C.c_void_p)]
 
 
 class clast_stats(C.Structure):
@@ -44,7 +44,8 @@ class clast_stats(C.Structure):
                 ("query_bases", C.c_int64), ("query_kmers", C.c_int64), ("seeds", C.c_int64), ("hits", C.c_int64),
                 ("results", C.c_int64), ("dp_cells", C.c_int64), ("seed_ms", C.c_double),
                 ("seed_launches", C.c_int64), ("dp_ms", C.c_double), ("dp_launches", C.c_int64),
-                ("sort_ms", C.c_double), ("final_ms", C.c_double)]
+                ("sort_ms", C.c_double), ("final_ms", C.c_double), ("index_wall_ms", C.c_double),
+                ("map_wall_ms", C.c_double), ("map_prep_ms", C.c_double), ("map_call_ms", C.c_double)]
 
 
 # symbol name -> (restype, argtypes); the full export list of include/clast_gpu.h

@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import time
 
 import numpy as np
 
@@ -151,6 +152,36 @@ def _hits_to_numpy(h: N.clast_hits) -> dict:
     return out
 
 
+class _MapResultOwner:
+    """Keeps one clast_map result (pinned buffers of the context) alive while
+    any of its numpy views exists; releases it afterwards."""
+
+    def __init__(self, engine, r):
+        self.engine = engine
+        self.r = r
+
+    def __del__(self):
+        if self.r is not None and getattr(self.engine, "ctx", None):
+            N.load().clast_map_result_free(C.byref(self.r))
+        self.r = None
+
+
+def _map_result_arrays(engine, r, n_loads) -> dict:
+    """Zero-copy numpy views of a clast_map result."""
+    owner = _MapResultOwner(engine, r)
+    n = int(r.n)
+    out = {}
+    for f in MAP_FIELDS:
+        ct = C.c_double if f == "evalue" else C.c_int32
+        buf = (ct * max(n, 1)).from_address(C.cast(getattr(r, f), C.c_void_p).value)
+        buf._owner = owner
+        out[f] = np.frombuffer(buf, dtype=np.float64 if f == "evalue" else np.int32, count=n)
+    lo = (C.c_int64 * (n_loads + 1)).from_address(C.cast(r.load_offsets, C.c_void_p).value)
+    lo._owner = owner
+    out["load_offsets"] = np.frombuffer(lo, dtype=np.int64, count=n_loads + 1)
+    return out
+
+
 class HashTable:
     """Resident index of one target window (CDeviceHashTable)."""
 
@@ -170,8 +201,9 @@ class HashTable:
 class Targets:
     """Every target window of every RAM load, resident in HBM."""
 
-    def __init__(self, handle):
+    def __init__(self, handle, engine=None):
         self.handle = handle
+        self.engine = engine  # the context must outlive its indexes
 
     def close(self):
         if self.handle:
@@ -262,27 +294,23 @@ class Engine:
         p = s.c()
         self._check(self._lib.clast_targets_create(self.ctx, C.byref(p), int(t_vram), C.byref(seqs), len(ls),
                                                    ls.ctypes.data, C.byref(out)))
-        return Targets(out.value)
+        return Targets(out.value, self)
 
     def map(self, s: Setting, targets: Targets, bases, offsets: np.ndarray, load_sizes, q_vram: int) -> dict:
         """Every read against every target window; hits per query load in
         the order CHostResultHolder::fixResult leaves them."""
+        t0 = time.perf_counter()
         ls = np.ascontiguousarray(load_sizes, dtype=np.int64)
         seqs, _keep = self._seqs(bases, offsets)
         r = N.clast_map_result()
         p = s.c()
+        t1 = time.perf_counter()
         self._check(self._lib.clast_map(self.ctx, targets.handle, C.byref(p), int(q_vram), C.byref(seqs), len(ls),
                                         ls.ctypes.data, C.byref(r)))
-        try:
-            n = int(r.n)
-            out = {}
-            for f in MAP_FIELDS:
-                dt = np.float64 if f == "evalue" else np.int32
-                out[f] = np.ctypeslib.as_array(getattr(r, f), shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
-            out["load_offsets"] = np.ctypeslib.as_array(r.load_offsets, shape=(len(ls) + 1,)).copy()
-            return out
-        finally:
-            self._lib.clast_map_result_free(C.byref(r))
+        t2 = time.perf_counter()
+        out = _map_result_arrays(self, r, len(ls))
+        self.last_map_py_ms = ((t1 - t0) * 1e3, (t2 - t1) * 1e3, (time.perf_counter() - t2) * 1e3)
+        return out
 
     def stats(self) -> dict:
         """clast_get_stats: CUDA-event timings and counts of the last

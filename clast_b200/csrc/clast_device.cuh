@@ -57,17 +57,23 @@ __device__ __forceinline__ int base_class(char b) {
 
 // l-mer key at flat position f (SRead2bit.cuh:6-21 with SRepelHasOddBase.cuh:6-14):
 // false when any of the l bases is not A/C/G/T.
+// Streamed loads (evict-first in L2) so that the words of the query, read once,
+// do not push the presence filter out of L2.
+__device__ __forceinline__ uint64_t ld_stream(const uint64_t* p) {
+  return (uint64_t)__ldcs(reinterpret_cast<const unsigned long long*>(p));
+}
+
 __device__ __forceinline__ bool kmer_at(const uint64_t* packed, const uint64_t* nmask, int64_t f,
                                         int l, uint64_t& key) {
   const int64_t w = f >> 6;
   const int o = (int)(f & 63);
-  uint64_t m = nmask[w] << o;
-  if (o) m |= nmask[w + 1] >> (64 - o);
+  uint64_t m = ld_stream(nmask + w) << o;
+  if (o) m |= ld_stream(nmask + w + 1) >> (64 - o);
   if (m >> (64 - l)) return false;
   const int64_t w2 = f >> 5;
   const int o2 = (int)(f & 31) * 2;
-  uint64_t b = packed[w2] << o2;
-  if (o2) b |= packed[w2 + 1] >> (64 - o2);
+  uint64_t b = ld_stream(packed + w2) << o2;
+  if (o2) b |= ld_stream(packed + w2 + 1) >> (64 - o2);
   key = b >> (64 - 2 * l);
   return true;
 }
@@ -79,15 +85,15 @@ __device__ __forceinline__ int64_t index_lookup(const IndexView& ix, uint64_t ke
   const uint64_t fb = key >> ix.fshift;
   if (!((ix.filter[fb >> 5] >> (fb & 31)) & 1u)) return -1;
   const uint32_t p = (uint32_t)(key >> ix.shift);
-  int64_t lo = ix.dir[p];
-  const int64_t end = ix.dir[p + 1];
+  int64_t lo = __ldcs(ix.dir + p);
+  const int64_t end = __ldcs(ix.dir + p + 1);
   int64_t hi = end;
   while (lo < hi) {
     const int64_t mid = (lo + hi) >> 1;
-    if (ix.ukeys[mid] < key) lo = mid + 1;
+    if (ld_stream(ix.ukeys + mid) < key) lo = mid + 1;
     else hi = mid;
   }
-  return (lo < end && ix.ukeys[lo] == key) ? lo : -1;
+  return (lo < end && ld_stream(ix.ukeys + lo) == key) ? lo : -1;
 }
 
 }  // namespace clast

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -76,7 +77,15 @@ struct StageTimer {
   }
 };
 
+// Pinned host buffer that holds one clast_map result; reused once released.
+struct PinnedArena {
+  void* p = nullptr;
+  size_t bytes = 0;
+  bool in_use = false;
+};
+
 struct clast_ctx {
+  std::vector<std::unique_ptr<PinnedArena>> arenas;
   int device = 0;
   cudaStream_t st = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
@@ -86,9 +95,14 @@ struct clast_ctx {
   int64_t last_launches = 0;
   clast_stats stats{};
   StageTimer timer;
+  int64_t seed_hint = 0;  // seed buffer capacity that sufficed before
 };
 
 namespace {
+
+double wall_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 // Stream used for the stream-ordered allocations of the current API call.
 thread_local cudaStream_t g_alloc_stream = nullptr;
@@ -254,8 +268,12 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix) {
   ix->shift = 2 * l - bits;
   ix->dir.alloc(((size_t)1 << bits) + 1);
   index_directory(ix->ukeys.p, nu, ix->shift, bits, ix->dir.p, st);
-  // presence filter over the top min(2l, 30) key bits (at most 128 MB)
-  ix->filter_bits = std::min(2 * l, 30);
+  // presence filter over the top min(2l, F) key bits; F = 28 (32 MB, L2-resident
+  // next to the streams that pass through L2 while seeding) unless
+  // CLAST_FILTER_BITS says otherwise (16..32)
+  int fbits = 28;
+  if (const char* e = std::getenv("CLAST_FILTER_BITS")) fbits = std::max(16, std::min(32, std::atoi(e)));
+  ix->filter_bits = std::min(2 * l, fbits);
   ix->fshift = 2 * l - ix->filter_bits;
   ix->filter.alloc((((size_t)1 << ix->filter_bits) + 31) / 32);
   index_filter(ix->ukeys.p, nu, ix->fshift, ix->filter_bits, ix->filter.p, st);
@@ -359,18 +377,38 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   const int64_t ns = qb.nstrands, nr = ns / 2;
   out = DevHits();
   if (ns == 0 || ix->n_unique == 0) return;
-  // createRawSeedList + deleteSeedsOnSequenceBoundary
-  int64_t* cnt = ws.get<int64_t>("s_cnt", ns);
+  // createRawSeedList + deleteSeedsOnSequenceBoundary, one pass
   int64_t* off = ws.get<int64_t>("s_off", ns + 1);
-  unsigned long long* counters = ws.get<unsigned long long>("s_counters", 2);  // k-mers, DP cells
-  CLAST_CK(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st));
+  int32_t* len32 = ws.get<int32_t>("s_len32", ns);
+  int32_t* nvalid = ws.get<int32_t>("s_nvalid", ns);
+  const int parts = seed_parts();
+  // k-mers, DP cells, then one seed cursor per partition
+  unsigned long long* counters = ws.get<unsigned long long>("s_counters", 2 + parts);
   StageTimer& tm = c->timer;
-  int32_t* kidx = ws.get<int32_t>("s_kidx", (size_t)qb.n + 1);
-  tm.begin(st);
-  seed_count(q, iv, cnt, counters, kidx, st);
-  tm.end(StageTimer::SEED, st);
-  scan_i64(ws, cnt, ns, off, st);
-  const int64_t S = read_scalar(off + ns, st);
+  int64_t part_cap = std::max<int64_t>(c->seed_hint, qb.n / 16 + (1 << 20)) / parts + 1;
+  int64_t S = 0;
+  uint64_t* skey = nullptr;
+  uint32_t* sq = nullptr;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    skey = ws.get<uint64_t>("s_key", (size_t)part_cap * parts);
+    sq = ws.get<uint32_t>("s_q", (size_t)part_cap * parts);
+    CLAST_CK(cudaMemsetAsync(counters, 0, (2 + parts) * sizeof(unsigned long long), st));
+    tm.begin(st);
+    seed_fused(q, iv, tv, p->gap, p->local, counters + 2, counters, off, len32, nvalid, skey, sq, part_cap, st);
+    tm.end(StageTimer::SEED, st);
+    unsigned long long cur[64];
+    CLAST_CK(cudaMemcpyAsync(cur, counters + 2, parts * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CLAST_CK(cudaStreamSynchronize(st));
+    S = 0;
+    int64_t most = 0;
+    for (int i = 0; i < parts; ++i) {
+      S += (int64_t)cur[i];
+      most = std::max<int64_t>(most, (int64_t)cur[i]);
+    }
+    if (most <= part_cap) break;
+    part_cap = most;  // strands past a full partition wrote nothing: run again
+  }
+  c->seed_hint = std::max<int64_t>(c->seed_hint, S + S / 4);
   auto add_counters = [&]() {
     unsigned long long h[2];
     CLAST_CK(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st));
@@ -384,22 +422,13 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
     add_counters();
     return;
   }
-  uint64_t* skey = ws.get<uint64_t>("s_key", S);
-  uint32_t* sq = ws.get<uint32_t>("s_q", S);
-  int32_t* nvalid = ws.get<int32_t>("s_nvalid", ns);
-  tm.begin(st);
-  seed_write(q, iv, tv, p->gap, p->local, off, kidx, skey, sq, nvalid, st);
-  tm.end(StageTimer::SEED, st);
   int32_t* wfirst = ws.get<int32_t>("s_wfirst", qb.nwin);
   window_first(nvalid, qb.wstart.p, qb.nwin, wfirst, st);
   // sortSeeds, deletingIsolateSeeds, deleteDuplicateSeeds
-  int32_t* len32 = ws.get<int32_t>("s_len32", ns);
   tm.begin(st);
-  to_i32(cnt, ns, len32, st);
-  segmented_sort_u32(ws, skey, sq, off, len32, ns, st, 0);
   int32_t* hcnt = ws.get<int32_t>("s_hcnt", ns);
-  seed_filter(skey, sq, off, nvalid, qb.wstart.p, qb.nwin, wfirst, p->width, p->gap, ns, hcnt, st);
-  tm.end(StageTimer::SORT, st, 7);
+  seed_sort_filter(ws, skey, sq, off, len32, nvalid, qb.wstart.p, qb.nwin, wfirst, p->width, p->gap, ns, hcnt, st);
+  tm.end(StageTimer::SORT, st, 4);
   int64_t* hoff = ws.get<int64_t>("s_hoff", ns + 1);
   scan_i32(ws, hcnt, ns, hoff, st);
   const int64_t H = read_scalar(hoff + ns, st);
@@ -502,21 +531,24 @@ struct clast_targets {
 
 namespace {
 
-// One read window list per query load (moveQueryWindow, CHostSchedular.cu:12-23).
+// One read window list per query load (moveQueryWindow, CHostSchedular.cu:12-23):
+// the window [qb, qe) grows while gateway(2*qe+2) - gateway(2*qb) < q_vram,
+// where every read adds two strands of len + l - 1 bases.  With the prefix
+// sums cum[], qe = clamp(first j with cum[j] >= cum[qb] + q_vram, minus one,
+// to [qb + 1, n]).
 void query_windows(const int64_t* offsets, int64_t r0, int64_t r1, int l, int32_t q_vram,
                    std::vector<int64_t>& win_first_read) {
-  // gateway over strands: every read adds two strands of len + l - 1
-  const int64_t nreads = r1 - r0;
-  auto gw = [&](int64_t strand) -> int64_t {  // gateway(strand) relative to the load
-    const int64_t r = strand / 2;
-    int64_t v = 2 * (offsets[r0 + r] - offsets[r0]) + 2 * r * (int64_t)(l - 1);
-    if (strand & 1) v += (offsets[r0 + r + 1] - offsets[r0 + r]) + (l - 1);
-    return v;
-  };
-  for (int64_t qb = 0, qe = 1; qb < nreads; qb = qe++) {
-    const int64_t base = gw(2 * qb);
-    while (qe < nreads && gw(2 * qe + 2) - base < (int64_t)q_vram) ++qe;
+  const int64_t n = r1 - r0;
+  std::vector<int64_t> cum(n + 1);
+  cum[0] = 0;
+  for (int64_t r = 0; r < n; ++r)
+    cum[r + 1] = cum[r] + 2 * ((offsets[r0 + r + 1] - offsets[r0 + r]) + (l - 1));
+  for (int64_t qb = 0; qb < n;) {
+    const int64_t lim = cum[qb] + (int64_t)q_vram;
+    const int64_t j = std::lower_bound(cum.begin() + qb, cum.end(), lim) - cum.begin();
+    const int64_t qe = std::max(qb + 1, std::min(n, j - 1));
     win_first_read.push_back(r0 + qb);
+    qb = qe;
   }
 }
 
@@ -558,6 +590,8 @@ void clast_ctx_destroy(clast_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->st) cudaStreamSynchronize(ctx->st);
   ctx->ws.release_all();
+  for (auto& a : ctx->arenas)
+    if (a->p) cudaFreeHost(a->p);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->ev2) cudaEventDestroy(ctx->ev2);
@@ -671,6 +705,7 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
     g_kernel_launches = 0;
     ctx->stats.index_ms = ctx->stats.index_upload_ms = 0;
     ctx->stats.index_launches = 0;
+    const double w0 = wall_ms();
     const int l = p->lmer;
     std::unique_ptr<clast_targets> T(new clast_targets());
     T->ctx = ctx;
@@ -745,6 +780,7 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
         T->wins.push_back(std::move(w));
       }
     }
+    ctx->stats.index_wall_ms = wall_ms() - w0;
     *out = T.release();
     return CLAST_OK;
   });
@@ -752,9 +788,20 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
 
 void clast_targets_free(clast_targets* t) { delete t; }
 
+static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int32_t q_vram,
+                    const clast_seqs* reads, int32_t n_loads, const int64_t* load_sizes, clast_map_result* out);
+
 int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int32_t q_vram,
               const clast_seqs* reads, int32_t n_loads, const int64_t* load_sizes, clast_map_result* out) {
   if (!ctx || !out) return CLAST_ERR_ARG;
+  const double w0 = wall_ms();
+  const int rc = map_impl(ctx, T, p, q_vram, reads, n_loads, load_sizes, out);
+  ctx->stats.map_call_ms = wall_ms() - w0;
+  return rc;
+}
+
+static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int32_t q_vram,
+                    const clast_seqs* reads, int32_t n_loads, const int64_t* load_sizes, clast_map_result* out) {
   std::memset(out, 0, sizeof(*out));
   return guarded(ctx, [&]() -> int {
     check_params(p);
@@ -770,6 +817,7 @@ int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int
     g_kernel_launches = 0;
     cudaStream_t st = ctx->st;
     clast_stats& S = ctx->stats;
+    const double w0 = wall_ms();
     S.map_ms = S.map_upload_ms = 0;
     S.map_launches = S.query_bases = S.query_kmers = S.seeds = S.hits = S.results = S.dp_cells = 0;
     ctx->timer.reset();
@@ -785,8 +833,13 @@ int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int
     for (size_t i = 0; i < wfirst.size(); ++i) wstart[i] = (int32_t)(2 * wfirst[i]);
     // every read uploaded once; strands are built on the device
     const int64_t nb = reads->offsets[nreads] - reads->offsets[0];
-    std::vector<int64_t> off0(nreads + 1);
-    for (int64_t i = 0; i <= nreads; ++i) off0[i] = reads->offsets[i] - reads->offsets[0];
+    std::vector<int64_t> off0;
+    const int64_t* offs_rel = reads->offsets;  // offsets relative to the first read
+    if (reads->offsets[0] != 0) {
+      off0.resize(nreads + 1);
+      for (int64_t i = 0; i <= nreads; ++i) off0[i] = reads->offsets[i] - reads->offsets[0];
+      offs_rel = off0.data();
+    }
     DevArray<char> draw;
     DevArray<int64_t> doff;
     if (!reads->bases_on_device) draw.alloc((size_t)nb + 64);
@@ -799,13 +852,14 @@ int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int
     qb.len.alloc(2 * nreads);
     qb.nwin = (int32_t)wfirst.size() - 1;
     qb.wstart.alloc(wstart.size());
+    S.map_prep_ms = wall_ms() - w0;
     CLAST_CK(cudaEventRecord(ctx->ev0, st));
     const char* rsrc = reads->bases + reads->offsets[0];
     if (!reads->bases_on_device) {
       if (nb) CLAST_CK(cudaMemcpyAsync(draw.p, rsrc, nb, cudaMemcpyHostToDevice, st));
       rsrc = draw.p;
     }
-    CLAST_CK(cudaMemcpyAsync(doff.p, off0.data(), (nreads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    CLAST_CK(cudaMemcpyAsync(doff.p, offs_rel, (nreads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
     CLAST_CK(cudaMemcpyAsync(qb.wstart.p, wstart.data(), wstart.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
                              st));
     CLAST_CK(cudaEventRecord(ctx->ev1, st));
@@ -851,21 +905,45 @@ int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int
     clast_map_result res;
     std::memset(&res, 0, sizeof(res));
     res.n = F;
-    res.load_offsets = static_cast<int64_t*>(std::calloc(n_loads + 1, sizeof(int64_t)));
-    if (!res.load_offsets) throw std::bad_alloc();
+    // one pinned arena: load offsets, ten int32 arrays, evalue
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t need = al((n_loads + 1) * sizeof(int64_t)) + 10 * al((F ? F : 1) * sizeof(int32_t)) +
+                        al((F ? F : 1) * sizeof(double));
+    PinnedArena* arena = nullptr;
+    for (auto& a : ctx->arenas)
+      if (!a->in_use && (arena == nullptr || a->bytes > arena->bytes)) arena = a.get();
+    if (!arena) {
+      ctx->arenas.emplace_back(new PinnedArena());
+      arena = ctx->arenas.back().get();
+    }
+    if (arena->bytes < need) {
+      if (arena->p) CLAST_CK(cudaFreeHost(arena->p));
+      arena->p = nullptr;
+      arena->bytes = 0;
+      const size_t nb = need + need / 4;
+      if (cudaMallocHost(&arena->p, nb) != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw std::bad_alloc();
+      }
+      arena->bytes = nb;
+    }
+    arena->in_use = true;
+    res.owner = arena;
+    char* cur = static_cast<char*>(arena->p);
+    auto take = [&](size_t b) { char* q = cur; cur += al(b); return q; };
+    res.load_offsets = reinterpret_cast<int64_t*>(take((n_loads + 1) * sizeof(int64_t)));
+    std::memset(res.load_offsets, 0, (n_loads + 1) * sizeof(int64_t));
     if (nreads > 0)
       CLAST_CK(cudaMemcpyAsync(res.load_offsets, dlo.p, (n_loads + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
                                st));
     auto d2h32 = [&](int32_t*& dst, const DevArray<int32_t>& src) {
-      dst = static_cast<int32_t*>(std::malloc((F ? F : 1) * sizeof(int32_t)));
-      if (!dst) throw std::bad_alloc();
+      dst = reinterpret_cast<int32_t*>(take((F ? F : 1) * sizeof(int32_t)));
       if (F) CLAST_CK(cudaMemcpyAsync(dst, src.p, F * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     };
     d2h32(res.read, m_read); d2h32(res.strand, m_strand); d2h32(res.t_load, m_load); d2h32(res.t_seq, m_seq);
     d2h32(res.t_idx, m_tidx); d2h32(res.q_idx, m_qidx); d2h32(res.t_len, m_tlen); d2h32(res.q_len, m_qlen);
     d2h32(res.match, m_match); d2h32(res.score, m_score);
-    res.evalue = static_cast<double*>(std::malloc((F ? F : 1) * sizeof(double)));
-    if (!res.evalue) throw std::bad_alloc();
+    res.evalue = reinterpret_cast<double*>(take((F ? F : 1) * sizeof(double)));
     if (F) CLAST_CK(cudaMemcpyAsync(res.evalue, m_e.p, F * sizeof(double), cudaMemcpyDeviceToHost, st));
     CLAST_CK(cudaEventRecord(ctx->ev2, st));
     CLAST_CK(cudaEventSynchronize(ctx->ev2));
@@ -884,6 +962,7 @@ int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int
     S.final_ms = ctx->timer.ms[StageTimer::FINAL];
     ctx->last_ms = up + ms;
     ctx->last_launches = g_kernel_launches;
+    S.map_wall_ms = wall_ms() - w0;
     *out = res;
     return CLAST_OK;
   });
@@ -891,9 +970,7 @@ int clast_map(clast_ctx* ctx, const clast_targets* T, const clast_params* p, int
 
 void clast_map_result_free(clast_map_result* r) {
   if (!r) return;
-  std::free(r->load_offsets); std::free(r->read); std::free(r->strand); std::free(r->t_load);
-  std::free(r->t_seq); std::free(r->t_idx); std::free(r->q_idx); std::free(r->t_len); std::free(r->q_len);
-  std::free(r->match); std::free(r->score); std::free(r->evalue);
+  if (r->owner) static_cast<PinnedArena*>(r->owner)->in_use = false;
   std::memset(r, 0, sizeof(*r));
 }
 

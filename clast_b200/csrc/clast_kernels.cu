@@ -449,6 +449,131 @@ __global__ void k_seed_write(QueryView q, IndexView ix, TargetView t, int gap, i
   if (lane == 0) nvalid[s] = valid;
 }
 
+// Seeding in one pass, one warp per strand: every l-mer is looked up once; the
+// first kSeedRegChunks*32 results stay in registers (longer strands look the
+// rest up again in the second phase).  The strand's seeds get one contiguous
+// range from an atomic cursor; if the range would pass `cap`, nothing is
+// written and the host reruns with a larger buffer (the cursor then holds the
+// exact total).  Seeds are written in the reference's order: l-mer position
+// ascending, then bucket order (window position ascending).
+constexpr int kSeedRegChunks = 8;
+constexpr int kSeedParts = 32;
+
+__device__ __forceinline__ void seed_lookup(const QueryView& q, const IndexView& ix, int64_t st, int qi, int nk,
+                                            int& u, int& c, int& valid) {
+  u = -1;
+  c = 0;
+  if (qi < nk) {
+    uint64_t key;
+    if (kmer_at(q.packed, q.nmask, st + qi, ix.l, key)) {
+      ++valid;
+      const int64_t x = index_lookup(ix, key);
+      if (x >= 0) {
+        const int k = __ldcs(ix.ucnt + x);
+        if (k > 0) {
+          u = (int)x;
+          c = k;
+        }
+      }
+    }
+  }
+}
+
+constexpr int kSeedFusedThreads = 256;
+
+// The seed buffer is split into kSeedParts partitions of part_cap seeds, each
+// with its own cursor; strand s takes its range in partition s % kSeedParts, so
+// the range reservations of neighbouring warps hit different counters.
+__global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, IndexView ix, TargetView t, int gap,
+                                                                   int local, unsigned long long* __restrict__ cursor,
+                                                                   unsigned long long* __restrict__ n_kmers,
+                                                                   int64_t* __restrict__ off, int32_t* __restrict__ cnt,
+                                                                   int32_t* __restrict__ nvalid,
+                                                                   uint64_t* __restrict__ skey,
+                                                                   uint32_t* __restrict__ sq, int64_t part_cap) {
+  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (s >= q.nstrands) return;
+  const int64_t st = q.start[s];
+  const int qlen = q.len[s];
+  const int nk = qlen - ix.l + 1;
+  int ureg[kSeedRegChunks];
+  int total = 0, valid_kmers = 0;
+#pragma unroll
+  for (int ci = 0; ci < kSeedRegChunks; ++ci) {
+    int u = -1, c = 0;
+    if (ci * 32 < nk) seed_lookup(q, ix, st, ci * 32 + lane, nk, u, c, valid_kmers);
+    ureg[ci] = u;
+    total += c;
+  }
+  for (int c0 = kSeedRegChunks * 32; c0 < nk; c0 += 32) {
+    int u, c;
+    seed_lookup(q, ix, st, c0 + lane, nk, u, c, valid_kmers);
+    total += c;
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    total += __shfl_xor_sync(kFull, total, o);
+    valid_kmers += __shfl_xor_sync(kFull, valid_kmers, o);
+  }
+  const int part = (int)(s % kSeedParts);
+  unsigned long long rel = 0;
+  if (lane == 0) {
+    if (valid_kmers) atomicAdd(n_kmers, (unsigned long long)valid_kmers);
+    rel = total ? atomicAdd(&cursor[part], (unsigned long long)total) : 0ull;
+  }
+  rel = __shfl_sync(kFull, rel, 0);
+  const unsigned long long base = (unsigned long long)part * (unsigned long long)part_cap + rel;
+  if (lane == 0) {
+    off[s] = (int64_t)base;
+    cnt[s] = total;
+  }
+  const int64_t cap = (int64_t)(part + 1) * part_cap;
+  if (total == 0 || (int64_t)(base + total) > cap) {
+    if (lane == 0) nvalid[s] = 0;
+    return;
+  }
+  int64_t w = (int64_t)base;
+  int valid = 0;
+  for (int c0 = 0, ci = 0; c0 < nk; c0 += 32, ++ci) {
+    const int qi = c0 + lane;
+    int u = -1, c = 0, dummy = 0;
+    if (ci < kSeedRegChunks) {
+#pragma unroll
+      for (int k = 0; k < kSeedRegChunks; ++k)
+        if (k == ci) u = ureg[k];
+      if (u >= 0) c = ix.ucnt[u];
+    } else {
+      seed_lookup(q, ix, st, qi, nk, u, c, dummy);
+    }
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int chunk_total = __shfl_sync(kFull, incl, 31);
+    if (c) {
+      const int us = ix.ustart[u];
+      const int64_t w0 = w + incl - c;
+      for (int i = 0; i < c; ++i) {
+        const int2 e = ix.entries[us + i];
+        const int s0 = e.y - qi;  // tHitStartIdx, is_onCorner
+        const bool drop = !local && ((s0 + gap < 0) || (s0 + qlen - gap > t.lengths[e.x]));
+        // streaming stores: the seeds must not evict the presence filter from L2
+        __stcs(reinterpret_cast<unsigned long long*>(skey + w0 + i),
+               drop ? kDroppedSeed : (((uint64_t)(uint32_t)e.x << 32) | ((uint32_t)s0 ^ 0x80000000u)));
+        __stcs(sq + w0 + i, (uint32_t)qi);
+        valid += drop ? 0 : 1;
+      }
+    }
+    w += chunk_total;
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) valid += __shfl_xor_sync(kFull, valid, o);
+  if (lane == 0) nvalid[s] = valid;
+}
+
 __global__ void k_window_first(const int32_t* __restrict__ nvalid, const int32_t* __restrict__ wstart, int nwin,
                                int32_t* __restrict__ wfirst) {
   const int w = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -718,6 +843,204 @@ __global__ void k_seed_filter(uint64_t* __restrict__ skey, uint32_t* __restrict_
   if (lane == 0) hcnt[s] = (int32_t)(out - o);
 }
 
+// ---- seed sort fused with the isolate / duplicate filters ----
+struct SeedFilterCtx {
+  const int64_t* off;
+  const int32_t* cnt;
+  const int32_t* nvalid;
+  const int32_t* wstart;
+  int nwin;
+  const int32_t* wfirst;
+  int width, gap;
+  int32_t* hcnt;
+};
+
+__device__ __forceinline__ bool window_first_strand(int64_t s, const SeedFilterCtx& c) {
+  int lo = 0, hi = c.nwin;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (c.wstart[mid] <= s) lo = mid;
+    else hi = mid;
+  }
+  return c.wfirst[lo] == (int32_t)s;
+}
+
+// State carried from one 32-seed chunk of a strand to the next.
+struct FilterState {
+  int ptid = 0, ptidx = 0, pdiag = 0;  // last seed of the previous chunk
+  bool have_surv = false;
+  int stid = 0, stidx = 0, sdiag = 0;  // last isolate-filter survivor so far
+  int64_t out = 0;                     // next hit slot
+};
+
+// deletingIsolateSeeds then deleteDuplicateSeeds on the chunk of sorted seeds
+// j = c0 + lane (valid when j < n); survivors are written at f.out onwards.
+__device__ __forceinline__ void filter_chunk(int c0, int n, uint64_t k, uint32_t qi, bool wf, int width, int gap,
+                                             FilterState& f, uint64_t* __restrict__ skey,
+                                             uint32_t* __restrict__ sq) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = lanemask_lt();
+  const int j = c0 + lane;
+  const bool in = j < n;
+  const int tid = (int)(k >> 32);
+  const int diag = (int)((uint32_t)k ^ 0x80000000u);
+  const int tidx = diag + (int)qi;
+  int ptid_l = __shfl_up_sync(kFull, tid, 1);
+  int ptidx_l = __shfl_up_sync(kFull, tidx, 1);
+  int pdiag_l = __shfl_up_sync(kFull, diag, 1);
+  if (lane == 0) { ptid_l = f.ptid; ptidx_l = f.ptidx; pdiag_l = f.pdiag; }
+  bool keep8 = false;
+  if (in) keep8 = (j == 0) ? wf : near_pred(tid, tidx, diag, ptid_l, ptidx_l, pdiag_l, width, gap);
+  const unsigned b8 = __ballot_sync(kFull, keep8);
+  const unsigned below = b8 & lt;
+  const int src = below ? 31 - __clz(below) : 0;
+  const int qtid = __shfl_sync(kFull, tid, src);
+  const int qtidx = __shfl_sync(kFull, tidx, src);
+  const int qdiag = __shfl_sync(kFull, diag, src);
+  bool keep9 = keep8;
+  if (keep8) {
+    if (below) keep9 = !near_pred(tid, tidx, diag, qtid, qtidx, qdiag, width, gap);
+    else if (f.have_surv) keep9 = !near_pred(tid, tidx, diag, f.stid, f.stidx, f.sdiag, width, gap);
+  }
+  const unsigned b9 = __ballot_sync(kFull, keep9);
+  if (keep9) {
+    const int64_t w = f.out + __popc(b9 & lt);
+    skey[w] = k;
+    sq[w] = qi;
+  }
+  f.out += __popc(b9);
+  f.ptid = __shfl_sync(kFull, tid, 31);
+  f.ptidx = __shfl_sync(kFull, tidx, 31);
+  f.pdiag = __shfl_sync(kFull, diag, 31);
+  if (b8) {
+    const int last = 31 - __clz(b8);
+    f.stid = __shfl_sync(kFull, tid, last);
+    f.stidx = __shfl_sync(kFull, tidx, last);
+    f.sdiag = __shfl_sync(kFull, diag, last);
+    f.have_surv = true;
+  }
+}
+
+__global__ void k_seed_classify(SeedFilterCtx c, int64_t ns, int32_t* __restrict__ lists,
+                                int32_t* __restrict__ counts) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = (i < ns && c.nvalid[i] > 0) ? c.cnt[i] : 0;
+  const int tier = (n <= 0) ? -1 : ((n <= 32) ? 0 : (n <= kCtaSortCap ? 1 : 2));
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    const unsigned m = __ballot_sync(kFull, tier == t);
+    if (!m) continue;
+    int base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd(&counts[t], __popc(m));
+    base = __shfl_sync(kFull, base, __ffs(m) - 1);
+    if (tier == t) lists[(int64_t)t * ns + base + __popc(m & lanemask_lt())] = (int32_t)i;
+  }
+}
+
+// <= 32 seeds: one warp, sorted in registers and filtered from registers.
+__global__ void k_seed_sort_filter_warp(uint64_t* __restrict__ skey, uint32_t* __restrict__ sq, SeedFilterCtx c,
+                                        const int32_t* __restrict__ list, const int32_t* __restrict__ count) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int total = *count;
+  for (int64_t li = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; li < total; li += nwarps) {
+    const int s = list[li];
+    const int64_t o = c.off[s];
+    const int n = c.cnt[s];
+    uint64_t a1 = ~0ull;
+    uint32_t a2 = ~0u;
+    if (lane < n) {
+      a1 = skey[o + lane];
+      a2 = sq[o + lane];
+    }
+    for (int size = 2; size <= 32; size <<= 1) {
+      {
+        const int partner = lane ^ (size - 1);
+        const uint64_t b1 = __shfl_sync(kFull, a1, partner);
+        const uint32_t b2 = __shfl_sync(kFull, a2, partner);
+        const bool b_less = less2(b1, b2, a1, a2);
+        if (lane < partner ? b_less : !b_less && (b1 != a1 || b2 != a2)) { a1 = b1; a2 = b2; }
+      }
+      for (int stride = size >> 2; stride > 0; stride >>= 1) {
+        const int partner = lane ^ stride;
+        const uint64_t b1 = __shfl_sync(kFull, a1, partner);
+        const uint32_t b2 = __shfl_sync(kFull, a2, partner);
+        const bool b_less = less2(b1, b2, a1, a2);
+        if (lane < partner ? b_less : !b_less && (b1 != a1 || b2 != a2)) { a1 = b1; a2 = b2; }
+      }
+    }
+    FilterState f;
+    f.out = o;
+    filter_chunk(0, c.nvalid[s], a1, a2, window_first_strand(s, c), c.width, c.gap, f, skey, sq);
+    if (lane == 0) c.hcnt[s] = (int32_t)(f.out - o);
+  }
+}
+
+// <= 2048 seeds: one CTA sorts in shared memory, warp 0 filters from there.
+__global__ void __launch_bounds__(256) k_seed_sort_filter_cta(uint64_t* __restrict__ skey, uint32_t* __restrict__ sq,
+                                                              SeedFilterCtx c, const int32_t* __restrict__ list,
+                                                              const int32_t* __restrict__ count) {
+  __shared__ uint64_t s1[kCtaSortCap];
+  __shared__ uint32_t s2[kCtaSortCap];
+  const int total = *count;
+  for (int li = blockIdx.x; li < total; li += gridDim.x) {
+    const int s = list[li];
+    const int64_t o = c.off[s];
+    const int n = c.cnt[s];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      s1[i] = skey[o + i];
+      s2[i] = sq[o + i];
+    }
+    __syncthreads();
+    cta_network<uint32_t, false>(s1, s2, nullptr, n);
+    if (threadIdx.x < 32) {
+      const int nv = c.nvalid[s];
+      const bool wf = window_first_strand(s, c);
+      FilterState f;
+      f.out = o;
+      for (int c0 = 0; c0 < nv; c0 += 32) {
+        const int j = c0 + (int)threadIdx.x;
+        filter_chunk(c0, nv, j < nv ? s1[j] : 0ull, j < nv ? s2[j] : 0u, wf, c.width, c.gap, f, skey, sq);
+      }
+      if (threadIdx.x == 0) c.hcnt[s] = (int32_t)(f.out - o);
+    }
+    __syncthreads();
+  }
+}
+
+// Longer: one CTA sorts in global memory, warp 0 filters in place.
+__global__ void __launch_bounds__(1024) k_seed_sort_filter_global(uint64_t* __restrict__ skey,
+                                                                  uint32_t* __restrict__ sq, SeedFilterCtx c,
+                                                                  const int32_t* __restrict__ list,
+                                                                  const int32_t* __restrict__ count) {
+  const int total = *count;
+  for (int li = blockIdx.x; li < total; li += gridDim.x) {
+    const int s = list[li];
+    const int64_t o = c.off[s];
+    cta_network<uint32_t, false>(skey + o, sq + o, nullptr, c.cnt[s]);
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int nv = c.nvalid[s];
+      const bool wf = window_first_strand(s, c);
+      FilterState f;
+      f.out = o;
+      for (int c0 = 0; c0 < nv; c0 += 32) {
+        const int j = c0 + (int)threadIdx.x;
+        uint64_t k = 0;
+        uint32_t qv = 0;
+        if (j < nv) {
+          k = skey[o + j];
+          qv = sq[o + j];
+        }
+        filter_chunk(c0, nv, k, qv, wf, c.width, c.gap, f, skey, sq);
+      }
+      if (threadIdx.x == 0) c.hcnt[s] = (int32_t)(f.out - o);
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void k_gather_hits(const uint64_t* __restrict__ skey, const uint32_t* __restrict__ sq,
                               const int64_t* __restrict__ off, const int32_t* __restrict__ hcnt,
                               const int64_t* __restrict__ hoff, int64_t nstrands, uint64_t* __restrict__ hk,
@@ -742,95 +1065,174 @@ __global__ void k_gather_hits(const uint64_t* __restrict__ skey, const uint32_t*
 // ------------------------------------------------------------------------
 // banded DP
 // ------------------------------------------------------------------------
-// POINT_MATRIX / MATCH_COUNTER (krnlMatrix.cuh:11-67) as a rule over letter
-// classes, packed as (point << 16) | (match & 0xffff) at [target*32 + query].
-__device__ __forceinline__ int letter_group(int c) {  // 0..3 ACGT, 4 scored letter, 5 "-1" letter, 6 X
-  switch (c) {
-    case 0: return 0;   // A
-    case 2: return 1;   // C
-    case 6: return 2;   // G
-    case 19: return 3;  // T
-    case 23: return 6;  // X
-    case 4: case 5: case 8: case 9: case 11: case 14: case 15: case 16: case 25: return 5;  // E F I J L O P Q Z
-    default: return 4;
-  }
-}
+// POINT_MATRIX / MATCH_COUNTER (krnlMatrix.cuh:11-67) depend only on seven
+// letter classes: A, C, G, T, any other scored letter (B D H K M N R S U V W Y),
+// a '-1' letter (E F I J L O P Q Z) and the bad-area letter X.  Bytes outside
+// 'A'..'Z' score as 'N'.
+constexpr int kClassX = 6;
 
+__host__ __device__ constexpr int class_of_letter(int i) {  // i = letter - 'A'
+  return i == 0 ? 0 : i == 2 ? 1 : i == 6 ? 2 : i == 19 ? 3 : i == 23 ? kClassX
+       : (i == 4 || i == 5 || i == 8 || i == 9 || i == 11 || i == 14 || i == 15 || i == 16 || i == 25) ? 5 : 4;
+}
+// (point << 16) | (match & 0xffff) for target class t, query class q.
 __device__ __forceinline__ int packed_score(int t, int q) {
-  const int a = letter_group(t < 26 ? t : kNClass), b = letter_group(q < 26 ? q : kNClass);
   int point, match;
-  if (a == 6 || b == 6) { point = -1000; match = -1000; }
-  else if (a == 5 || b == 5) { point = -1; match = -1; }
-  else if (a == b && a < 4) { point = 1; match = 1; }
+  if (t == kClassX || q == kClassX) { point = -1000; match = -1000; }
+  else if (t == 5 || q == 5) { point = -1; match = -1; }
+  else if (t == q && t < 4) { point = 1; match = 1; }
   else { point = -3; match = 0; }
   return (int)((unsigned)point << 16) | (match & 0xffff);
 }
 
-template <int GAP, bool LOCAL, bool BACKWARD>
-__device__ __forceinline__ void dp_pass(const int* __restrict__ tab, const char* __restrict__ tb, int64_t tstart,
-                                        int tlen, const char* __restrict__ qb, int64_t qfirst, int rows, int tidx,
-                                        int l, int& move, int& endp, int& best, int& best_m) {
-  constexpr int W = 2 * GAP + 1;
-  constexpr int kBotS = (GAP + 1) * kGapExtend + kGapOpen;
-  constexpr int kBotV = kBotS + kGapOpen;
-  int S[W], V[W], M[W], tc[W];
+// Banded DP of one hit, backward pass then forward pass, in ONE row loop of
+// rows_b + rows_f iterations: every hit of a read has qLen - l rows in total,
+// so the threads of a warp stay converged although each switches from the
+// backward to the forward pass at its own row.
+//
+// Per band column the registers hold A = S - 7 (score minus gap open +
+// extend), B = V - 2 (vertical state minus gap extend) and M (matches); along
+// a row the chain carries hA = S - 7 and hB = H - 2 of the previous column.
+// Then, exactly as calcutlateCell (krnlAlignment.cu:42-77):
+//   V = max(Sv - 7, Vv - 2) = max(A_v, B_v)        H = max(Sh - 7, Hh - 2) = max(hA, hB)
+//   pt = S_diag + POINT = A_diag + (POINT + 7)      (the table stores POINT + 7)
+//   H wins over V iff H >= V; the diagonal wins iff pt > max(V, H)
+// __vibmax_s32 returns the max and that comparison in one instruction.
+template <int GAP>
+struct Band {
+  static constexpr int W = 2 * GAP + 1;
+  int A[W], B[W], M[W], tc[W];
+
+  // initTempNodeArray, krnlAlignment.cu:6-38 (band rows 1..W), and the first W
+  // target bases of a pass: index ib0 + step * c, 'X' outside [lo, hi).
+  __device__ __forceinline__ void init(const char* __restrict__ tb, int64_t tstart, int64_t ib0, int step,
+                                       int64_t lo, int64_t hi) {
 #pragma unroll
-  for (int c = 0; c < W; ++c) {  // initTempNodeArray, krnlAlignment.cu:6-38 (band rows 1..W)
-    const int r = c + 1;
-    if (r < GAP + 1) { S[c] = kMarginScore; V[c] = kMarginScore; M[c] = kMarginScore; }
-    else if (r == GAP + 1) { S[c] = 0; V[c] = kGapOpen; M[c] = 0; }
-    else { S[c] = (r - GAP - 1) * kGapExtend + kGapOpen; V[c] = S[c] + kGapOpen; M[c] = 0; }
-    const int64_t ib = BACKWARD ? (int64_t)tidx + l - GAP + c : (int64_t)tidx + GAP - c - 1;
-    const bool bad = BACKWARD ? (ib >= tlen) : (ib < 0);
-    tc[c] = (bad ? kBadClass : base_class(tb[tstart + ib])) << 5;
+    for (int c = 0; c < W; ++c) {
+      const int r = c + 1;
+      int sc, v, m;
+      if (r < GAP + 1) { sc = kMarginScore; v = kMarginScore; m = kMarginScore; }
+      else if (r == GAP + 1) { sc = 0; v = kGapOpen; m = 0; }
+      else { sc = (r - GAP - 1) * kGapExtend + kGapOpen; v = sc + kGapOpen; m = 0; }
+      A[c] = sc + kGapOpen + kGapExtend;
+      B[c] = v + kGapExtend;
+      M[c] = m;
+      const int64_t ib = ib0 + (int64_t)step * c;
+      tc[c] = ((ib < lo || ib >= hi) ? kBadClass : base_class(tb[tstart + ib])) << 5;
+    }
   }
-  int bs = 0, bm = 0, calc = -1, ep = GAP;
-  for (int q = 0; q < rows; ++q) {
-    const int qc = base_class(BACKWARD ? qb[qfirst + q] : qb[qfirst - q]);
-    int hS = kMarginScore, hH = kMarginScore, hM = kMarginScore;
+  // select end node (global mode), krnlAlignment.cu:170-185
+  __device__ __forceinline__ void end_node(int& best, int& best_m, int& ep) const {
+    best = kMarginScore;
+    best_m = kMarginScore;
+    ep = -1;
 #pragma unroll
-    for (int c = 0; c < W; ++c) {  // calcutlateCell, krnlAlignment.cu:42-77
-      const int vS = (c + 1 < W) ? S[(c + 1) % W] : kBotS;
-      const int vV = (c + 1 < W) ? V[(c + 1) % W] : kBotV;
-      const int vM = (c + 1 < W) ? M[(c + 1) % W] : 0;
-      const int nV = max(vS + (kGapOpen + kGapExtend), vV + kGapExtend);
-      const int nH = max(hS + (kGapOpen + kGapExtend), hH + kGapExtend);
-      const int w = tab[tc[c] | qc];
-      const int pt = S[c] + (w >> 16);
-      const int mx = max(nV, nH);
-      const int side_m = (nV > nH) ? vM : hM;
-      const int nM = (pt > mx) ? (M[c] + ((w << 16) >> 16)) : side_m;
-      const int nS = max(pt, mx);
-      S[c] = nS;
-      V[c] = nV;
-      M[c] = nM;
-      hS = nS;
-      hH = nH;
+    for (int c = 0; c < W; ++c) {
+      const int sc = A[c] - (kGapOpen + kGapExtend);
+      if (best < sc) { best = sc; best_m = M[c]; ep = c; }
+    }
+  }
+};
+
+template <int GAP, bool LOCAL>
+__device__ __forceinline__ void banded_hit(const int* __restrict__ tab, const char* __restrict__ tb, int64_t tstart,
+                                           int tlen, const char* __restrict__ qb, int64_t qstart, int qlen, int tidx,
+                                           int qidx, int l, int& t_hl, int& q_hl, int& match, int& score,
+                                           int& o_tidx, int& o_qidx) {
+  constexpr int W = Band<GAP>::W;
+  constexpr int kGapSO = kGapOpen + kGapExtend;  // -7
+  constexpr int kBotA = (GAP + 1) * kGapExtend + kGapOpen + kGapSO;  // fixed band row 2*GAP+2
+  constexpr int kBotB = (GAP + 1) * kGapExtend + kGapOpen + kGapOpen + kGapExtend;
+  constexpr int kMarginA = kMarginScore + kGapSO, kMarginB = kMarginScore + kGapExtend;
+  constexpr int64_t kNoLow = INT64_MIN / 2, kNoHigh = INT64_MAX / 2;
+  const int rows_b = qlen - (qidx + l);  // alignmentSize of the backward pass
+  const int rows_f = qidx;              // rows of the forward pass
+  const int rows = rows_b + rows_f;
+  Band<GAP> bd;
+  // backward pass (globalAlignBackward / localAlignBackward): target bases
+  // tIdx + l - gap + q + c ('X' at or past tLen), query bases qIdx + l + q
+  int64_t q_at = qstart + qidx + l;
+  int q_step = 1;
+  int64_t t_at = (int64_t)tidx + l + GAP + 1;  // next target base to shift in after row 0
+  int t_step = 1;
+  int64_t t_lo = kNoLow, t_hi = tlen;
+  bd.init(tb, tstart, (int64_t)tidx + l - GAP, 1, t_lo, t_hi);
+  int bs = 0, bm = 0, calc = -1, ep = GAP, qrow = 0;
+  int pass = 0;
+  auto finish = [&](int pass_rows) {  // result of the pass that just ended
+    int move, best, best_m, e;
+    if (LOCAL) { best = bs; best_m = bm; e = ep; move = calc + 1; }
+    else { bd.end_node(best, best_m, e); move = pass_rows; }
+    e -= GAP;
+    if (pass_rows != 0) {
+      if (pass == 1) {  // forward: the hit's start moves
+        o_tidx -= move + e;
+        o_qidx -= move;
+      }
+      t_hl += move + e;
+      q_hl += move;
+      match += best_m;
+      score += best;
+    }
+  };
+  char q_cur = (rows_b > 0) ? qb[q_at] : 'N';
+  for (int r = 0; r < rows; ++r) {
+    if (r == rows_b) {  // switch to the forward pass (globalAlignForward / localAlignForward)
+      finish(rows_b);
+      pass = 1;
+      q_at = qstart + qidx - 1;  // query bases qIdx - q - 1
+      q_step = -1;
+      t_at = (int64_t)tidx - GAP - 2;  // target bases tIdx + gap - 1 - q - c ('X' below 0)
+      t_step = -1;
+      t_lo = 0;
+      t_hi = kNoHigh;
+      bd.init(tb, tstart, (int64_t)tidx + GAP - 1, -1, t_lo, t_hi);
+      bs = 0; bm = 0; calc = -1; ep = GAP; qrow = 0;
+      q_cur = qb[q_at];
+    }
+    // loads for the next row go out first; their latency hides behind this row
+    const int64_t ib = t_at + (int64_t)t_step * qrow;
+    const char t_next = (ib < t_lo || ib >= t_hi) ? 'X' : tb[tstart + ib];
+    const bool more = (pass == 0) ? (r + 1 < rows_b) : (r + 1 < rows);
+    const char q_next = more ? qb[q_at + (int64_t)q_step * (qrow + 1)] : 'N';
+    const int qc = base_class(q_cur);
+    int hA = kMarginA, hB = kMarginB, hM = kMarginScore;  // row 0 of the band (left margin)
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      const int vA = (c + 1 < W) ? bd.A[(c + 1) % W] : kBotA;
+      const int vB = (c + 1 < W) ? bd.B[(c + 1) % W] : kBotB;
+      const int vM = (c + 1 < W) ? bd.M[(c + 1) % W] : 0;
+      const int nV = max(vA, vB);
+      const int nH = max(hA, hB);
+      const int w = tab[bd.tc[c] | qc];
+      const int pt = bd.A[c] + (w >> 16);
+      bool h_wins, not_diag;
+      const int mx = __vibmax_s32(nH, nV, &h_wins);   // h_wins = nH >= nV
+      const int nS = __vibmax_s32(mx, pt, &not_diag);  // not_diag = mx >= pt
+      const int side_m = h_wins ? hM : vM;
+      const int nM = not_diag ? side_m : (bd.M[c] + ((w << 16) >> 16));
+      const int nA = nS + kGapSO;
+      bd.A[c] = nA;
+      bd.B[c] = nV + kGapExtend;
+      bd.M[c] = nM;
+      hA = nA;
+      hB = nH + kGapExtend;
       hM = nM;
       if (LOCAL) {
-        if (bs < nS) { bs = nS; bm = nM; calc = q; ep = c; }
+        if (bs < nS) { bs = nS; bm = nM; calc = qrow; ep = c; }
       }
     }
 #pragma unroll
-    for (int c = 0; c < W - 1; ++c) tc[c] = tc[c + 1];
-    const int64_t ib = BACKWARD ? (int64_t)tidx + l + GAP + q + 1 : (int64_t)tidx - GAP - q - 2;
-    const bool bad = BACKWARD ? (ib >= tlen) : (ib < 0);
-    tc[W - 1] = (bad ? kBadClass : base_class(tb[tstart + ib])) << 5;
+    for (int c = 0; c < W - 1; ++c) bd.tc[c] = bd.tc[c + 1];
+    bd.tc[W - 1] = base_class(t_next) << 5;  // 'X' above is the bad-area letter itself
+    q_cur = q_next;
+    ++qrow;
   }
-  if (!LOCAL) {  // select end node, krnlAlignment.cu:170-185
-    bs = kMarginScore;
-    bm = kMarginScore;
-    ep = -1;
-#pragma unroll
-    for (int c = 0; c < W; ++c)
-      if (bs < S[c]) { bs = S[c]; bm = M[c]; ep = c; }
-    move = rows;
+  if (rows_b == rows) {  // the loop never switched: close the backward pass (rows_f == 0)
+    finish(rows_b);
   } else {
-    move = calc + 1;
+    finish(rows_f);
   }
-  endp = ep - GAP;
-  best = bs;
-  best_m = bm;
 }
 
 struct DpKernelArgs {
@@ -846,8 +1248,11 @@ struct DpKernelArgs {
 
 template <int GAP, bool LOCAL>
 __global__ void __launch_bounds__(128) k_banded_dp(DpKernelArgs a) {
-  __shared__ int tab[32 * 32];
-  for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) tab[i] = packed_score(i >> 5, i & 31);
+  __shared__ int tab[32 * 32];  // [target letter][query letter], letters 'A'..'Z'
+  for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x)
+    tab[i] = packed_score(class_of_letter((i >> 5) < 26 ? (i >> 5) : kNClass),
+                          class_of_letter((i & 31) < 26 ? (i & 31) : kNClass)) +
+             ((kGapOpen + kGapExtend) * -65536);  // POINT + 7 in the high half
   __syncthreads();
   const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= a.n) return;
@@ -863,27 +1268,8 @@ __global__ void __launch_bounds__(128) k_banded_dp(DpKernelArgs a) {
   const int l = a.p.l;
   int t_hl = l, q_hl = l, match = l, score = l;  // CDeviceHitList.cu:283-286
   int o_tidx = tidx, o_qidx = qidx;
-  int move, endp, best, best_m;
-  const int rows_b = qlen - (qidx + l);  // globalAlignBackward / localAlignBackward
-  dp_pass<GAP, LOCAL, true>(tab, a.t.bases, tstart, tlen, a.q.bases, qstart + qidx + l, rows_b, tidx, l, move,
-                            endp, best, best_m);
-  if (rows_b != 0) {
-    t_hl += move + endp;
-    q_hl += move;
-    match += best_m;
-    score += best;
-  }
-  const int rows_f = qidx;  // globalAlignForward / localAlignForward
-  dp_pass<GAP, LOCAL, false>(tab, a.t.bases, tstart, tlen, a.q.bases, qstart + qidx - 1, rows_f, tidx, l, move,
-                             endp, best, best_m);
-  if (rows_f != 0) {
-    o_tidx -= move + endp;
-    o_qidx -= move;
-    t_hl += move + endp;
-    q_hl += move;
-    match += best_m;
-    score += best;
-  }
+  banded_hit<GAP, LOCAL>(tab, a.t.bases, tstart, tlen, a.q.bases, qstart, qlen, tidx, qidx, l, t_hl, q_hl, match,
+                         score, o_tidx, o_qidx);
   // calculateEvalue, krnlCalculateEvalue.cu:21 (same operation order)
   const double e = a.p.K * a.p.total_db * (double)qlen * exp(-a.p.lambda * (double)score);
   const bool keep = !(a.p.cutoff != -1.0 && a.p.cutoff < e) && !(l + a.p.stride > q_hl);
@@ -1206,6 +1592,17 @@ void seed_write(const QueryView& q, const IndexView& ix, const TargetView& t, in
                                                                            sq, nvalid);
   CLAST_LAUNCHED();
 }
+int seed_parts() { return kSeedParts; }
+
+void seed_fused(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
+                unsigned long long* cursors, unsigned long long* n_kmers, int64_t* off, int32_t* cnt, int32_t* nvalid,
+                uint64_t* skey, uint32_t* sq, int64_t part_cap, cudaStream_t st) {
+  if (q.nstrands <= 0) return;
+  k_seed_fused<<<blocks_for((int64_t)q.nstrands * 32, kSeedFusedThreads), kSeedFusedThreads, 0, st>>>(
+      q, ix, t, gap, local, cursors, n_kmers, off, cnt, nvalid, skey, sq, part_cap);
+  CLAST_LAUNCHED();
+}
+
 void window_first(const int32_t* nvalid, const int32_t* win_start, int n_windows, int32_t* win_first,
                   cudaStream_t st) {
   if (n_windows <= 0) return;
@@ -1234,6 +1631,27 @@ void seed_filter(uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t
                                                                  win_first, width, gap, nstrands, hcnt);
   CLAST_LAUNCHED();
 }
+void seed_sort_filter(Workspace& ws, uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t* cnt,
+                      const int32_t* nvalid, const int32_t* win_start, int n_windows, const int32_t* win_first,
+                      int width, int gap, int64_t nstrands, int32_t* hcnt, cudaStream_t st) {
+  if (nstrands <= 0) return;
+  SeedFilterCtx c{off, cnt, nvalid, win_start, n_windows, win_first, width, gap, hcnt};
+  int32_t* lists = ws.get<int32_t>("ssf_lists", 3 * nstrands);
+  int32_t* counts = ws.get<int32_t>("ssf_counts", 3);
+  CLAST_CK(cudaMemsetAsync(counts, 0, 3 * sizeof(int32_t), st));
+  CLAST_CK(cudaMemsetAsync(hcnt, 0, nstrands * sizeof(int32_t), st));
+  k_seed_classify<<<blocks_for(nstrands, 256), 256, 0, st>>>(c, nstrands, lists, counts);
+  CLAST_LAUNCHED();
+  k_seed_sort_filter_warp<<<grid_cap((nstrands * 32 + 255) / 256), 256, 0, st>>>(skey, sq, c, lists, counts);
+  CLAST_LAUNCHED();
+  k_seed_sort_filter_cta<<<grid_cap(nstrands < 4096 ? nstrands : 4096), 256, 0, st>>>(skey, sq, c,
+                                                                                     lists + nstrands, counts + 1);
+  CLAST_LAUNCHED();
+  k_seed_sort_filter_global<<<grid_cap(nstrands < 1024 ? nstrands : 1024), 1024, 0, st>>>(
+      skey, sq, c, lists + 2 * nstrands, counts + 2);
+  CLAST_LAUNCHED();
+}
+
 void gather_hits(const uint64_t* skey, const uint32_t* sq, const int64_t* off, const int32_t* hcnt,
                  const int64_t* hoff, int64_t nstrands, uint64_t* hk, int32_t* hq, int32_t* hs,
                  const int32_t* qlen, int l, int band, unsigned long long* cells, cudaStream_t st) {

@@ -62,6 +62,15 @@ void seed_count(const QueryView& q, const IndexView& ix, int64_t* cnt, unsigned 
 void seed_write(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
                 const int64_t* off, const int32_t* kidx, uint64_t* skey, uint32_t* sq, int32_t* nvalid,
                 cudaStream_t st);
+// One-pass seeding (lookups once): off/cnt/nvalid per strand, seeds in skey/sq,
+// which hold seed_parts() partitions of part_cap seeds.  Strand s reserves its
+// range in partition s % seed_parts() through cursors[partition]; a partition
+// whose cursor ends above part_cap was not fully written and the call must be
+// repeated with part_cap >= the largest cursor.
+int seed_parts();
+void seed_fused(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
+                unsigned long long* cursors, unsigned long long* n_kmers, int64_t* off, int32_t* cnt, int32_t* nvalid,
+                uint64_t* skey, uint32_t* sq, int64_t part_cap, cudaStream_t st);
 void window_first(const int32_t* nvalid, const int32_t* win_start, int n_windows, int32_t* win_first,
                   cudaStream_t st);
 
@@ -75,6 +84,12 @@ void segmented_sort_u64(Workspace& ws, uint64_t* k1, uint64_t* k2, int32_t* payl
 // seed counts per strand (int32) from the int64 count array
 void to_i32(const int64_t* in, int64_t n, int32_t* out, cudaStream_t st);
 
+// sortSeeds + deletingIsolateSeeds + deleteDuplicateSeeds per strand: sorts the
+// cnt[s] seeds of strand s by (sequence, diagonal, qIdx) and writes the surviving
+// hits at off[s] onwards, hcnt[s] of them.
+void seed_sort_filter(Workspace& ws, uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t* cnt,
+                      const int32_t* nvalid, const int32_t* win_start, int n_windows, const int32_t* win_first,
+                      int width, int gap, int64_t nstrands, int32_t* hcnt, cudaStream_t st);
 void seed_filter(uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t* nvalid,
                  const int32_t* win_start, int n_windows, const int32_t* win_first, int width, int gap,
                  int64_t nstrands, int32_t* hcnt, cudaStream_t st);

@@ -122,7 +122,9 @@ void clast_targets_free(clast_targets* t);
 /* Result of clast_map: hits of every query load in the order
  * CHostResultHolder::fixResult leaves them (load by load).  read = record
  * index in the query set; strand 0 '+', 1 '-'; t_load / t_seq locate the
- * target record (t_seq counts within its load). */
+ * target record (t_seq counts within its load).  The arrays live in pinned
+ * host memory owned by the context and reused once released: call
+ * clast_map_result_free before clast_ctx_destroy. */
 typedef struct clast_map_result {
   int64_t n;
   int64_t* load_offsets; /* n_qloads + 1 values: hits of query load k */
@@ -137,6 +139,7 @@ typedef struct clast_map_result {
   int32_t* match;
   int32_t* score;
   double* evalue;
+  void* owner; /* library-internal: the pinned buffer holding the arrays */
 } clast_map_result;
 
 /* Maps every read against every target window.  The reads are split into RAM
@@ -173,6 +176,10 @@ typedef struct clast_stats {
   int64_t dp_launches;
   double sort_ms;            /* segmented sorts + seed filter                 */
   double final_ms;           /* result order, duplicate removal, compaction  */
+  double index_wall_ms;      /* host wall time of the last clast_targets_create */
+  double map_wall_ms;        /* host wall time of the last clast_map          */
+  double map_prep_ms;        /* ... of which host preparation before the first copy */
+  double map_call_ms;        /* host wall time of the whole clast_map call, buffers released */
 } clast_stats;
 int clast_get_stats(const clast_ctx* ctx, clast_stats* out);
 
