@@ -60,6 +60,9 @@ SIGNATURES = {
     "clast_search": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(clast_params), C.c_void_p, C.c_int64,
                                C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(clast_hits)]),
     "clast_hits_free": (None, [C.POINTER(clast_hits)]),
+    "clast_search_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(clast_params), C.c_void_p, C.c_int64,
+                                       C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int64,
+                                       C.POINTER(clast_hits)]),
     "clast_targets_create": (C.c_int, [C.c_void_p, C.POINTER(clast_params), C.c_int32, C.POINTER(clast_seqs),
                                        C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
     "clast_targets_free": (None, [C.c_void_p]),

@@ -264,6 +264,35 @@ class Engine:
         finally:
             self._lib.clast_hits_free(C.byref(h))
 
+    def hit_list_window_noalloc(self, s: Setting, ix: HashTable, q_bases: bytes, q_gateway, q_lengths,
+                                q_begin: int, capacity: int) -> dict:
+        """clast_search_noalloc: hit_list_window on the library's fixed
+        scratch, writing into host arrays of ``capacity`` hits owned here.
+        Raises ClastError (with ``needed`` set when the capacity was short)."""
+        gw = np.ascontiguousarray(q_gateway, dtype=np.int32)
+        ln = np.ascontiguousarray(q_lengths, dtype=np.int32)
+        cap = int(capacity)
+        bufs = {f: np.empty(max(cap, 1), np.float64 if f == "evalue" else np.int32) for f in HIT_FIELDS}
+        h = N.clast_hits()
+        for f in HIT_FIELDS:
+            ct = C.c_double if f == "evalue" else C.c_int32
+            setattr(h, f, bufs[f].ctypes.data_as(C.POINTER(ct)))
+        p = s.c()
+        rc = self._lib.clast_search_noalloc(self.ctx, ix.handle, C.byref(p), q_bases, len(q_bases), gw.ctypes.data,
+                                            ln.ctypes.data, len(gw), q_begin, cap, C.byref(h))
+        if rc != 0:
+            err = ClastError(rc, self._lib.clast_last_error(self.ctx).decode(errors="replace"))
+            err.needed = int(h.n)
+            raise err
+        n = int(h.n)
+        return {f: bufs[f][:n] for f in HIT_FIELDS}
+
+    def hit_list_noalloc(self, s: Setting, ix: HashTable, queries: SeqList, q_begin: int, q_end: int,
+                         capacity: int) -> dict:
+        """hit_list through clast_search_noalloc."""
+        bases, gw, ln = queries.window(2 * q_begin, 2 * q_end)
+        return self.hit_list_window_noalloc(s, ix, bases, gw, ln, 2 * q_begin, capacity)
+
     def hit_list(self, s: Setting, ix: HashTable, queries: SeqList, q_begin: int, q_end: int) -> dict:
         """CDeviceSeqList_query(s, q, q_begin, q_end) + CDeviceHitList(s, h, q,
         t_begin, 2*q_begin) + getResult: the window's hits as numpy arrays

@@ -10,11 +10,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -998,3 +1000,229 @@ int clast_last_map_stats(const clast_ctx* ctx, double* device_ms, int64_t* kerne
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------------------------
+// clast_search_noalloc: clast_search on a fixed scratch buffer, allocating
+// nothing.  The stage sequence is search_batch's for one query window; every
+// device buffer is a slot of the static scratch (Workspace arena mode) and
+// the hits go straight into the caller's host arrays.
+// ----------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kSearchScratchBytes = (size_t)CLAST_NOALLOC_SCRATCH_BYTES;
+static __device__ __align__(256) unsigned char g_search_scratch[kSearchScratchBytes];
+
+constexpr int kMaxScratchDevices = 64;
+std::mutex g_scratch_mu;
+void* g_scratch_addr[kMaxScratchDevices];           // device address of g_search_scratch, per device
+std::atomic<int> g_scratch_busy[kMaxScratchDevices];  // 1 while a call uses that device's scratch
+
+// Address of this device's scratch; the device must be current.  Looked up
+// once per device.
+char* search_scratch(int device) {
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_addr[device]) {
+    void* ptr = nullptr;
+    CLAST_CK(cudaGetSymbolAddress((void**)&ptr, g_search_scratch));
+    g_scratch_addr[device] = ptr;
+  }
+  return static_cast<char*>(g_scratch_addr[device]);
+}
+
+__global__ void k_widen_i32(const int32_t* __restrict__ in, int64_t n, int64_t* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i];
+}
+
+// Bytes of the query-sized buffers, as Workspace::get rounds them.
+size_t fixed_scratch_bytes(int64_t n, int64_t ns, int parts) {
+  auto r = [](size_t b) { return ((b ? b : 1) + 255) & ~size_t(255); };
+  const size_t nb = (size_t)n, s = (size_t)ns;
+  return r(nb + 2 * kPad) + r(8 * s) + r(4 * s) + r(4 * s) + r(8) + r(8 * (nb / 32 + 4)) + r(8 * (nb / 64 + 4)) +
+         r(8 * (s + 1)) + r(4 * s) + r(4 * s) + r(8 * (2 + (size_t)parts)) + r(4 * s) + r(8 * (s + 1)) +
+         r(12 * s) + (64 << 10);
+}
+
+// Clears the busy flag of a device's scratch once the call's stream work has
+// ended (also when the call failed after launching work).
+struct ScratchClaim {
+  int device;
+  cudaStream_t st;
+  ~ScratchClaim() {
+    cudaStreamSynchronize(st);
+    (void)cudaGetLastError();
+    g_scratch_busy[device].store(0);
+  }
+};
+
+}  // namespace
+
+extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const clast_params* p,
+                                    const char* q_bases, int64_t n_qbases, const int32_t* q_gateway,
+                                    const int32_t* q_lengths, int32_t n_qseqs, int32_t q_begin, int64_t capacity,
+                                    clast_hits* out) {
+  if (!ctx || !out) return CLAST_ERR_ARG;
+  out->n = 0;
+  return guarded(ctx, [&]() -> int {
+    check_params(p);
+    if (!ix) throw std::invalid_argument("index is null");
+    if (p->lmer != ix->l || p->stride != ix->stride || p->cut_repeat != ix->cut)
+      throw std::invalid_argument("params differ from the ones the index was built with");
+    if (n_qseqs < 0 || (n_qseqs & 1) || (q_begin & 1))
+      throw std::invalid_argument("query windows hold whole reads: n_qseqs and q_begin must be even");
+    if (n_qbases < 0 || (n_qbases > 0 && !q_bases) || (n_qseqs > 0 && (!q_gateway || !q_lengths)))
+      throw std::invalid_argument("bad query arrays");
+    if (capacity < 0 || (capacity > 0 && (!out->t_id || !out->t_idx || !out->q_id || !out->q_idx ||
+                                          !out->t_len || !out->q_len || !out->match || !out->score ||
+                                          !out->evalue)))
+      throw std::invalid_argument("capacity < 0, or a null output array");
+    for (int32_t i = 0; i < n_qseqs; ++i)
+      if (q_gateway[i] < 0 || q_lengths[i] < 0 || (int64_t)q_gateway[i] + q_lengths[i] > n_qbases)
+        throw std::invalid_argument("query sequence outside the base array");
+    if (ctx->device < 0 || ctx->device >= kMaxScratchDevices)
+      throw std::invalid_argument("device ordinal beyond the scratch table");
+    const int parts = seed_parts();
+    const size_t fixed = fixed_scratch_bytes(n_qbases, n_qseqs, parts);
+    if (fixed > kSearchScratchBytes)
+      throw std::invalid_argument("query window of " + std::to_string(n_qbases) + " bases and " +
+                                  std::to_string(n_qseqs) + " sequences needs " + std::to_string(fixed) +
+                                  " bytes of scratch before seeding; clast_search_noalloc has " +
+                                  std::to_string(kSearchScratchBytes) + " (use clast_search)");
+    CLAST_CK(cudaSetDevice(ctx->device));
+    int idle = 0;
+    if (!g_scratch_busy[ctx->device].compare_exchange_strong(idle, 1))
+      throw std::invalid_argument("another clast_search_noalloc call is using this device's scratch");
+    cudaStream_t st = ctx->st;
+    ScratchClaim claim{ctx->device, st};
+    char* base = search_scratch(ctx->device);
+    g_kernel_launches = 0;
+    Workspace ws;
+    ws.arena_begin(base, kSearchScratchBytes);
+    const int64_t ns = n_qseqs, nr = ns / 2, n = n_qbases;
+    // the query window: padded bases, strand starts and lengths, 2-bit words
+    char* qbases = ws.get<char>("q_bases", (size_t)n + 2 * kPad);
+    CLAST_CK(cudaMemsetAsync(qbases, 'N', (size_t)n + 2 * kPad, st));
+    if (n > 0) CLAST_CK(cudaMemcpyAsync(qbases + kPad, q_bases, (size_t)n, cudaMemcpyHostToDevice, st));
+    int64_t* qstart = ws.get<int64_t>("q_start", ns);
+    int32_t* qlen = ws.get<int32_t>("q_len", ns);
+    int32_t* qgw = ws.get<int32_t>("q_gw32", ns);
+    int32_t* wstart = ws.get<int32_t>("q_wstart", 2);
+    if (ns > 0) {
+      CLAST_CK(cudaMemcpyAsync(qgw, q_gateway, ns * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+      CLAST_CK(cudaMemcpyAsync(qlen, q_lengths, ns * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+      k_widen_i32<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(qgw, ns, qstart);
+      CLAST_LAUNCHED();
+    }
+    const int32_t ws2[2] = {0, n_qseqs};
+    CLAST_CK(cudaMemcpyAsync(wstart, ws2, sizeof(ws2), cudaMemcpyHostToDevice, st));
+    uint64_t* packed = ws.get<uint64_t>("q_packed", (size_t)(n / 32 + 4));
+    uint64_t* nmask = ws.get<uint64_t>("q_nmask", (size_t)(n / 64 + 4));
+    pack_bases(qbases + kPad, n, packed, nmask, st);
+    QueryView q;
+    q.bases = qbases + kPad;
+    q.n = n;
+    q.packed = packed;
+    q.nmask = nmask;
+    q.start = qstart;
+    q.len = qlen;
+    q.nstrands = n_qseqs;
+    const IndexView iv = ix->view();
+    const TargetView tv = ix->tview();
+    auto finish = [&](int64_t F) {
+      CLAST_CK(cudaStreamSynchronize(st));
+      ctx->last_launches = g_kernel_launches;
+      out->n = F;
+      return CLAST_OK;
+    };
+    if (ns == 0 || ix->n_unique == 0) return finish(0);
+    // createRawSeedList + deleteSeedsOnSequenceBoundary, one pass
+    int64_t* off = ws.get<int64_t>("s_off", ns + 1);
+    int32_t* len32 = ws.get<int32_t>("s_len32", ns);
+    int32_t* nvalid = ws.get<int32_t>("s_nvalid", ns);
+    unsigned long long* counters = ws.get<unsigned long long>("s_counters", 2 + parts);
+    // the seed partitions take at most half of the scratch still free
+    const size_t mark = ws.arena_used;
+    const int64_t fit = (int64_t)((ws.arena_cap - mark) / 2 / (12 * (size_t)parts)) - 256;
+    int64_t part_cap = std::max<int64_t>(ctx->seed_hint, n / 16 + (1 << 20)) / parts + 1;
+    part_cap = std::max<int64_t>(1, std::min(part_cap, fit));
+    int64_t S = 0;
+    uint64_t* skey = nullptr;
+    uint32_t* sq = nullptr;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      skey = ws.get<uint64_t>("s_key", (size_t)part_cap * parts);
+      sq = ws.get<uint32_t>("s_q", (size_t)part_cap * parts);
+      CLAST_CK(cudaMemsetAsync(counters, 0, (2 + parts) * sizeof(unsigned long long), st));
+      seed_fused(q, iv, tv, p->gap, p->local, counters + 2, counters, off, len32, nvalid, skey, sq, part_cap, st);
+      unsigned long long cur[64];
+      CLAST_CK(cudaMemcpyAsync(cur, counters + 2, parts * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+      CLAST_CK(cudaStreamSynchronize(st));
+      S = 0;
+      int64_t most = 0;
+      for (int i = 0; i < parts; ++i) {
+        S += (int64_t)cur[i];
+        most = std::max<int64_t>(most, (int64_t)cur[i]);
+      }
+      if (most <= part_cap) break;
+      ws.arena_rewind(mark);  // strands past a full partition wrote nothing: run again, larger
+      part_cap = most;
+    }
+    if (S == 0) return finish(0);
+    int32_t* wfirst = ws.get<int32_t>("s_wfirst", 1);
+    window_first(nvalid, wstart, 1, wfirst, st);
+    // sortSeeds, deletingIsolateSeeds, deleteDuplicateSeeds
+    int32_t* hcnt = ws.get<int32_t>("s_hcnt", ns);
+    seed_sort_filter(ws, skey, sq, off, len32, nvalid, wstart, 1, wfirst, p->width, p->gap, ns, hcnt, st);
+    int64_t* hoff = ws.get<int64_t>("s_hoff", ns + 1);
+    scan_i32(ws, hcnt, ns, hoff, st);
+    const int64_t H = read_scalar(hoff + ns, st);
+    if (H == 0) return finish(0);
+    uint64_t* hk = ws.get<uint64_t>("h_key", H);
+    int32_t* hq = ws.get<int32_t>("h_q", H);
+    int32_t* hs = ws.get<int32_t>("h_s", H);
+    gather_hits(skey, sq, off, hcnt, hoff, ns, hk, hq, hs, qlen, p->lmer, 2 * p->gap + 1, counters + 1, st);
+    // alignmentHits + calculateEvalue + deleteHits_lowEValue / _tooShort
+    DpOut o;
+    o.t_idx = ws.get<int32_t>("d_tidx", H);
+    o.q_idx = ws.get<int32_t>("d_qidx", H);
+    o.t_len = ws.get<int32_t>("d_tlen", H);
+    o.q_len = ws.get<int32_t>("d_qlen", H);
+    o.match = ws.get<int32_t>("d_match", H);
+    o.score = ws.get<int32_t>("d_score", H);
+    o.evalue = ws.get<double>("d_e", H);
+    o.keep = ws.get<uint8_t>("d_keep", H);
+    DpParams dp{p->lmer, p->stride, p->gap, p->local, p->cutoff, p->total_db, p->K, p->lambda};
+    banded_dp(tv, q, hk, hq, hs, H, dp, o, st);
+    // resultSorting + deleteHits_duplicateResult, per read
+    uint64_t* k1 = ws.get<uint64_t>("f_k1", H);
+    uint64_t* k2 = ws.get<uint64_t>("f_k2", H);
+    int32_t* idx = ws.get<int32_t>("f_idx", H);
+    final_keys(hk, hq, hs, o, H, k1, k2, idx, st);
+    int64_t* roff = ws.get<int64_t>("f_roff", nr);
+    int32_t* rlen = ws.get<int32_t>("f_rlen", nr);
+    read_ranges(hoff, nr, roff, rlen, st);
+    segmented_sort_u64(ws, k1, k2, idx, roff, rlen, nr, st, 1);
+    int32_t* fcnt = ws.get<int32_t>("f_cnt", nr);
+    int32_t* fsel = ws.get<int32_t>("f_sel", H);
+    final_dedupe(k1, k2, idx, hk, hs, o, roff, rlen, nr, fcnt, fsel, st);
+    int64_t* foff = ws.get<int64_t>("f_off", nr + 1);
+    scan_i32(ws, fcnt, nr, foff, st);
+    const int64_t F = read_scalar(foff + nr, st);
+    if (F > capacity) {
+      out->n = F;
+      throw std::invalid_argument("window has " + std::to_string(F) + " hits, capacity is " +
+                                  std::to_string(capacity));
+    }
+    if (F == 0) return finish(0);
+    FinalOut fo{ws.get<int32_t>("o_tid", F), ws.get<int32_t>("o_tidx", F), ws.get<int32_t>("o_qid", F),
+                ws.get<int32_t>("o_qidx", F), ws.get<int32_t>("o_tlen", F), ws.get<int32_t>("o_qlen", F),
+                ws.get<int32_t>("o_match", F), ws.get<int32_t>("o_score", F), ws.get<double>("o_e", F)};
+    final_compact(fsel, roff, fcnt, foff, nr, hk, hs, o, ix->t_begin, q_begin, fo, st);
+    int32_t* const dst[8] = {out->t_id, out->t_idx, out->q_id, out->q_idx, out->t_len, out->q_len, out->match,
+                             out->score};
+    const int32_t* const src[8] = {fo.t_id, fo.t_idx, fo.q_id, fo.q_idx, fo.t_len, fo.q_len, fo.match, fo.score};
+    for (int k = 0; k < 8; ++k)
+      CLAST_CK(cudaMemcpyAsync(dst[k], src[k], F * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CLAST_CK(cudaMemcpyAsync(out->evalue, fo.evalue, F * sizeof(double), cudaMemcpyDeviceToHost, st));
+    return finish(F);
+  });
+}

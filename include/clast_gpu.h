@@ -97,6 +97,36 @@ int clast_search(clast_ctx* ctx, const clast_index* ix, const clast_params* p,
                  const int32_t* q_lengths, int32_t n_qseqs, int32_t q_begin, clast_hits* out);
 void clast_hits_free(clast_hits* h);
 
+/* Allocation-free variant of clast_search.  It has no counterpart in the
+ * reference (CDeviceHitList allocates its device_vectors on every call); it
+ * serves callers that must not allocate: a process whose device memory is
+ * already handed out (a caching allocator that reserved the free HBM, where
+ * a cudaMalloc would fail or fragment it), and a serving loop that cannot
+ * take the device-wide synchronisation cudaMalloc/cudaFree may cause.
+ *
+ * Same inputs, same hits in the same order as clast_search.  It calls no
+ * cudaMalloc, cudaFree, stream-ordered or pinned allocation and no
+ * allocating library routine: all device scratch is carved out of one
+ * statically sized buffer of CLAST_NOALLOC_SCRATCH_BYTES inside the library
+ * (one per device), and the hits are copied into caller-owned host arrays.
+ *   out: t_id .. evalue point at `capacity` elements each (owned by the
+ *        caller; never pass them to clast_hits_free); out->n = hit count.
+ *   A window whose scratch need exceeds the buffer (its query arrays, or the
+ *   seeds / hits it produces) fails with CLAST_ERR_ARG and a message naming
+ *   the buffer; more hits than `capacity` fail with CLAST_ERR_ARG and out->n
+ *   set to the count needed.  clast_search has neither limit.
+ * The scratch is shared by every context of the process on that device, so
+ * overlapping calls would race on it: an overlapping call on the same device
+ * is rejected with CLAST_ERR_ARG instead.  Each call synchronises its
+ * context's stream before returning.  The first call on a device looks up
+ * the buffer's address (cudaGetSymbolAddress); make that first call before
+ * any stream capture on the device begins. */
+#define CLAST_NOALLOC_SCRATCH_BYTES (64ll << 20)
+int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const clast_params* p,
+                         const char* q_bases, int64_t n_qbases, const int32_t* q_gateway,
+                         const int32_t* q_lengths, int32_t n_qseqs, int32_t q_begin,
+                         int64_t capacity, clast_hits* out);
+
 /* ---- whole job: resident target indexes, every query RAM load at once ---- */
 
 /* One set of sequences, one strand, no joints: record i is
