@@ -47,7 +47,7 @@ T_RAM, Q_RAM, T_VRAM, Q_VRAM = 64e6, 64e6, 64e6, 2e6  # common.hpp:12-15, x 1e6 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="medium")
@@ -201,7 +201,7 @@ def run_ours(args):
     q_dev = q_pin.to("cuda", non_blocking=False)
     torch.cuda.synchronize()
 
-    host = {"targets_ms": 0.0, "map_ms": 0.0, "close_ms": 0.0, "n": 0, "py": [0.0, 0.0, 0.0]}
+    host = {"targets": [], "map": [], "close": [], "ctypes": [], "inside": [], "map_device": []}
 
     def step(tb, qb):
         c0 = time.perf_counter()
@@ -211,20 +211,24 @@ def run_ours(args):
         c2 = time.perf_counter()
         T.close()
         c3 = time.perf_counter()
-        host["targets_ms"] += (c1 - c0) * 1e3
-        host["map_ms"] += (c2 - c1) * 1e3
-        host["close_ms"] += (c3 - c2) * 1e3
-        host["n"] += 1
-        for i in range(3):
-            host["py"][i] += eng.last_map_py_ms[i]
+        host["targets"].append((c1 - c0) * 1e3)
+        host["map"].append((c2 - c1) * 1e3)
+        host["close"].append((c3 - c2) * 1e3)
+        host["ctypes"].append(eng.last_map_py_ms[1])
+        sm = eng.stats()
+        host["inside"].append(sm["map_call_ms"])
+        host["map_device"].append(sm["map_ms"] + sm["map_upload_ms"])
         return res
 
     def timed(tb, qb, sampler=None):
+        # warm-up in the timed loop's own pattern: the previous step's result is
+        # still held while the next one is mapped (two result buffers in use)
+        res = None
         for _ in range(args.warmup):
-            step(tb, qb)
-        for k in ("targets_ms", "map_ms", "close_ms", "n"):
-            host[k] = 0
-        host["py"] = [0.0, 0.0, 0.0]
+            res = step(tb, qb)
+        del res
+        for v in host.values():
+            v.clear()
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -244,18 +248,19 @@ def run_ours(args):
             x = torch.tensor([ms], device="cuda")
             dist.all_reduce(x, op=dist.ReduceOp.MAX)
             ms = float(x.item())
-        n = max(1, host["n"])
-        hw = {"targets_call": round(host["targets_ms"] / n, 3), "map_call": round(host["map_ms"] / n, 3),
-              "targets_free": round(host["close_ms"] / n, 3),
-              "inside_targets": round(st["index_wall_ms"], 3), "inside_map": round(st["map_wall_ms"], 3),
-              "map_host_prep": round(st["map_prep_ms"], 3), "map_whole_call": round(st["map_call_ms"], 3),
-              "map_py_before_call_ctypes_call_after": [round(x / n, 3) for x in host["py"]]}
+        # host wall time of the API calls per step: median and max over the timed steps
+        hw = {k: [round(statistics.median(v), 3), round(max(v), 3)] for k, v in host.items() if v}
+        hw["fields"] = ("[median, max] ms per step; ctypes = the clast_map call, inside = measured in clast_map, "
+                        "map_device = CUDA-event time of the map's uploads and stages")
+        hw["map_per_step"] = [round(x, 1) for x in host["map"]]
         return ms, launches, res, st, hw
 
     with ClockSampler(local) as clk:
         ms_dev, launches, res, st, hw_dev = timed(t_dev, q_dev)
+    scores = res["score"].copy()
+    del res
     ms_e2e, _, res2, st2, hw_e2e = timed(t_pin, q_pin)
-    assert np.array_equal(res["score"], res2["score"])
+    assert np.array_equal(scores, res2["score"])
     mbp_rank = q.offsets[-1] / 1e6
     value = mbp_rank * world * args.steps / (ms_dev / 1e3)
     e2e = mbp_rank * world * args.steps / (ms_e2e / 1e3)
@@ -264,12 +269,15 @@ def run_ours(args):
     peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     n_tw = max(1, st["seed_launches"] // 2)
-    seed_bytes = n_tw * st["query_bases"] / 4 + 8 * st["query_kmers"] + 20 * st["seeds"]
+    # algorithmic bytes of k_seed_fused per target window: 3/8 B per query base
+    # (2-bit code + N mask), one 8 B filter word per valid l-mer, 12 B written
+    # + 8 B of entry read per seed
+    seed_bytes = n_tw * st["query_bases"] * 3 / 8 + 8 * st["query_kmers"] + 20 * st["seeds"]
     stages = {"seeding": st["seed_ms"], "banded_dp": st["dp_ms"], "seed_sort_filter": st["sort_ms"],
               "result_order": st["final_ms"]}
     seed_gbs = seed_bytes / (st["seed_ms"] / 1e3) / 1e9 if st["seed_ms"] > 0 else 0.0
     roofline = {
-        "kernel": "seeding (k_seed_count + k_seed_write: l-mer keys, index lookups, seed writes)",
+        "kernel": "seeding (k_seed_fused: l-mer keys, filter + table lookups, seed writes)",
         "bound": "hbm", "achieved": round(seed_gbs, 1), "peak": hbm_peak, "unit": "GB/s",
         "frac": round(seed_gbs / hbm_peak, 4),
         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",

@@ -15,21 +15,23 @@ constexpr int kBadClass = 23;       // 'X' - 'A': the bad-area letter (common.hp
 constexpr int kNClass = 13;         // 'N' - 'A'
 constexpr uint64_t kDroppedSeed = ~0ull;
 
-// Resident index of one target window (the tables of CDeviceHashTable,
-// CDeviceHashTable.cuh:13-16, reorganised for direct lookup).
+// Resident index of one target window: the tables of CDeviceHashTable
+// (CDeviceHashTable.cuh:13-16) reorganised for one-probe lookup.  Every key
+// that keeps at least one entry after the repeat cut is a record {hash of
+// the key, payload} of an open-addressing table of 32-byte buckets (two records,
+// linear probing); payload is the key's only entry (sequence within window
+// << 32 | index within sequence) or, for keys with several entries, kMulti |
+// start << 32 | count into `entries`.  A blocked Bloom filter (3 bits in one
+// 32-bit word per key) answers most absent keys from L2.
 struct IndexView {
   int l;
-  int fshift;              // key >> fshift = bit of the presence filter
-  const uint32_t* filter;  // one bit per (key >> fshift) of every indexed key
-  int shift;               // key >> shift = directory slot
-  const uint32_t* dir;     // (1 << dir_bits) + 1 entries: first unique key with slot >= p
-  const uint64_t* ukeys;   // unique valid keys, ascending
-  const int32_t* ustart;   // first entry of each key
-  const int32_t* ucnt;     // entries of each key (0 when the repeat cut removes the key)
-  const int2* entries;     // (sequence within window, index within sequence), non-joint only
-  int64_t n_unique;
+  int fshift;                // filter word = hash >> fshift (fshift >= 32)
+  const uint32_t* filter;
+  const ulonglong2* table;   // 2 * nbuckets records; payload ~0 = free
+  uint32_t nbuckets;
+  const int2* entries;       // (sequence within window, index within sequence), non-joint only
+  int64_t n_keys;            // records in the table
 };
-
 // Target window for the DP and the corner filter.
 struct TargetView {
   const char* bases;       // window base array incl. joints; bases[-kPad .. n+kPad) readable
@@ -63,37 +65,100 @@ __device__ __forceinline__ uint64_t ld_stream(const uint64_t* p) {
   return (uint64_t)__ldcs(reinterpret_cast<const unsigned long long*>(p));
 }
 
-__device__ __forceinline__ bool kmer_at(const uint64_t* packed, const uint64_t* nmask, int64_t f,
-                                        int l, uint64_t& key) {
+// Whether any of the l bases from flat position f is not A/C/G/T.
+__device__ __forceinline__ bool kmer_has_n(const uint64_t* nmask, int64_t f, int l) {
   const int64_t w = f >> 6;
   const int o = (int)(f & 63);
   uint64_t m = ld_stream(nmask + w) << o;
   if (o) m |= ld_stream(nmask + w + 1) >> (64 - o);
-  if (m >> (64 - l)) return false;
+  return (m >> (64 - l)) != 0;
+}
+
+// 2-bit key of the l bases from flat position f (any non-ACGT base reads as A).
+__device__ __forceinline__ uint64_t kmer_key(const uint64_t* packed, int64_t f, int l) {
   const int64_t w2 = f >> 5;
   const int o2 = (int)(f & 31) * 2;
   uint64_t b = ld_stream(packed + w2) << o2;
   if (o2) b |= ld_stream(packed + w2 + 1) >> (64 - o2);
-  key = b >> (64 - 2 * l);
+  return b >> (64 - 2 * l);
+}
+
+// The same for l <= 16 from the 32-bit halves of the words: a 64-bit word
+// keeps its first base in its top bits, so the 16-base unit j of the packed
+// array (and the 32-base unit j of the N mask) is 32-bit element j ^ 1.
+__device__ __forceinline__ uint32_t kmer_key16(const uint32_t* packed32, int64_t f, int l) {
+  const int64_t j = f >> 4;
+  const uint32_t hi = __ldcs(packed32 + (j ^ 1));
+  const uint32_t lo = __ldcs(packed32 + ((j + 1) ^ 1));
+  return __funnelshift_l(lo, hi, 2 * (int)(f & 15)) >> (32 - 2 * l);
+}
+__device__ __forceinline__ bool kmer_has_n16(const uint32_t* nmask32, int64_t f, int l) {
+  const int64_t j = f >> 5;
+  const uint32_t hi = __ldcs(nmask32 + (j ^ 1));
+  const uint32_t lo = __ldcs(nmask32 + ((j + 1) ^ 1));
+  return (__funnelshift_l(lo, hi, (int)(f & 31)) >> (32 - l)) != 0;
+}
+
+__device__ __forceinline__ bool kmer_at(const uint64_t* packed, const uint64_t* nmask, int64_t f,
+                                        int l, uint64_t& key) {
+  if (kmer_has_n(nmask, f, l)) return false;
+  key = kmer_key(packed, f, l);
   return true;
 }
 
-// Index of key among the unique keys, or -1 (krnlBinarySearch.cu:3-33).  The
-// presence filter (<= 128 MB, mostly L2-resident) answers the common miss
-// without touching the directory or the key array.
-__device__ __forceinline__ int64_t index_lookup(const IndexView& ix, uint64_t key) {
-  const uint64_t fb = key >> ix.fshift;
-  if (!((ix.filter[fb >> 5] >> (fb & 31)) & 1u)) return -1;
-  const uint32_t p = (uint32_t)(key >> ix.shift);
-  int64_t lo = __ldcs(ix.dir + p);
-  const int64_t end = __ldcs(ix.dir + p + 1);
-  int64_t hi = end;
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (ld_stream(ix.ukeys + mid) < key) lo = mid + 1;
-    else hi = mid;
+constexpr uint64_t kMulti = 1ull << 63;
+constexpr uint64_t kNoPayload = ~0ull;  // also the payload of an empty record
+
+// Hash of an l-mer key: an xorshift then a multiply by an odd constant
+// (Fibonacci hashing), both invertible, so distinct keys have distinct hashes
+// and the table stores and compares hashes instead of keys.  The top bits
+// select the 32-bit filter word and the bucket, bits 16..30 the three filter
+// bits.
+__host__ __device__ __forceinline__ uint64_t key_hash(uint64_t key) {
+  return (key ^ (key >> 31)) * 0x9E3779B97F4A7C15ull;
+}
+// fshift >= 32: filter word = (h >> 32) >> (fshift - 32)
+__host__ __device__ __forceinline__ uint32_t filter_word(uint64_t h, int fshift) {
+  return (uint32_t)(h >> 32) >> (fshift - 32);
+}
+__host__ __device__ __forceinline__ uint32_t filter_mask(uint64_t h) {
+  const uint32_t v = (uint32_t)(h >> 16);
+  return (1u << (v & 31)) | (1u << ((v >> 5) & 31)) | (1u << ((v >> 10) & 31));
+}
+__device__ __forceinline__ bool filter_pass(uint32_t word, uint64_t h) {
+  const uint32_t m = filter_mask(h);
+  return (word & m) == m;
+}
+__device__ __forceinline__ uint32_t bucket_of(uint64_t h, uint32_t nbuckets) {
+  return __umulhi((uint32_t)(h >> 32), nbuckets);
+}
+// Entries of a payload (0 for none).
+__host__ __device__ __forceinline__ int payload_count(uint64_t p) {
+  return p == kNoPayload ? 0 : ((p & kMulti) ? (int)(uint32_t)p : 1);
+}
+
+// Linear probing from record j of bucket b for the key of hash h.  Records
+// are {hash, payload}; a free record has payload kNoPayload (no real payload
+// has that value), so an absent key ends at the first free record.  Loads are
+// evict-first so that the filter stays in L2.
+__device__ __forceinline__ uint64_t table_probe(const IndexView& ix, uint64_t h, uint32_t b, int j) {
+  for (uint32_t probe = 0; probe <= ix.nbuckets; ++probe) {
+    for (; j < 2; ++j) {
+      const ulonglong2 r = __ldcs(ix.table + 2 * (size_t)b + j);
+      if (r.x == h || r.y == kNoPayload) return r.y;
+    }
+    j = 0;
+    b = (b + 1 == ix.nbuckets) ? 0 : b + 1;
   }
-  return (lo < end && ld_stream(ix.ukeys + lo) == key) ? lo : -1;
+  return kNoPayload;
+}
+
+// Payload of key, or kNoPayload (krnlBinarySearch.cu:3-33 followed by the
+// bucket lookup of writeSeedList).
+__device__ __forceinline__ uint64_t index_find(const IndexView& ix, uint64_t key) {
+  const uint64_t h = key_hash(key);
+  if (!filter_pass(__ldg(ix.filter + filter_word(h, ix.fshift)), h)) return kNoPayload;
+  return table_probe(ix, h, bucket_of(h, ix.nbuckets), 0);
 }
 
 }  // namespace clast

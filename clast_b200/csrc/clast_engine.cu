@@ -182,25 +182,22 @@ struct clast_index {
   int32_t nseqs = 0;
   DevArray<char> bases;  // padded
   DevArray<int32_t> gateway, lengths;
-  DevArray<uint32_t> dir, filter;
-  DevArray<uint64_t> ukeys;
-  DevArray<int32_t> ustart, ucnt;
+  DevArray<uint32_t> filter;     // blocked Bloom filter, 2^(64 - fshift) words
+  DevArray<ulonglong2> table;    // 2 * nbuckets records {key, payload}
   DevArray<int2> entries;
-  int64_t n_unique = 0, n_entries = 0;
-  int dir_bits = 1, shift = 0, filter_bits = 1, fshift = 0;
+  int64_t n_unique = 0, n_keys = 0, n_entries = 0;
+  uint32_t nbuckets = 1;
+  int fshift = 63;
 
   IndexView view() const {
     IndexView v;
     v.l = l;
     v.fshift = fshift;
     v.filter = filter.p;
-    v.shift = shift;
-    v.dir = dir.p;
-    v.ukeys = ukeys.p;
-    v.ustart = ustart.p;
-    v.ucnt = ucnt.p;
+    v.table = table.p;
+    v.nbuckets = nbuckets;
     v.entries = entries.p;
-    v.n_unique = n_unique;
+    v.n_keys = n_keys;
     return v;
   }
   TargetView tview() const {
@@ -246,9 +243,9 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix) {
   scan_i32(ws, head, nv, hpos, st);
   const int64_t nu = read_scalar(hpos + nv, st);
   ix->n_unique = nu;
-  ix->ukeys.alloc(nu);
+  uint64_t* ukeys = ws.get<uint64_t>("ix_ukeys", nu);
   int64_t* ufirst = ws.get<int64_t>("ix_ufirst", nu + 1);
-  index_unique(keys, head, hpos, nv, ix->ukeys.p, ufirst, st);
+  index_unique(keys, head, hpos, nv, ukeys, ufirst, st);
   int32_t* keep = ws.get<int32_t>("ix_keep", nv);
   int2* resolved = ws.get<int2>("ix_resolved", nv);
   int64_t* kpos = ws.get<int64_t>("ix_kpos", nv + 1);
@@ -259,27 +256,33 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix) {
   ix->n_entries = ne;
   ix->entries.alloc(ne);
   index_entries(keep, kpos, resolved, nv, ix->entries.p, st);
-  ix->ustart.alloc(nu);
-  ix->ucnt.alloc(nu);
-  index_buckets(ufirst, kpos, nu, ix->ustart.p, ix->ucnt.p, st);
-  int bits = 1;
-  while (bits < 26 && (1ll << bits) < nu) ++bits;
-  bits = std::min(bits, 2 * l);
-  bits = std::max(bits, 1);
-  ix->dir_bits = bits;
-  ix->shift = 2 * l - bits;
-  ix->dir.alloc(((size_t)1 << bits) + 1);
-  index_directory(ix->ukeys.p, nu, ix->shift, bits, ix->dir.p, st);
-  // presence filter over the top min(2l, F) key bits; F = 28 (32 MB, L2-resident
-  // next to the streams that pass through L2 while seeding) unless
-  // CLAST_FILTER_BITS says otherwise (16..32)
+  int32_t* ustart = ws.get<int32_t>("ix_ustart", nu);
+  int32_t* ucnt = ws.get<int32_t>("ix_ucnt", nu);
+  index_buckets(ufirst, kpos, nu, ustart, ucnt, st);
+  // One record per unique key is an upper bound on the keys that keep entries;
+  // buckets of two records at most 70% full.
+  const int64_t nb = std::max<int64_t>(1, (nu * 10 + 13) / 14);
+  if (nb >= (int64_t)UINT32_MAX) throw std::invalid_argument("window has too many distinct l-mers");
+  ix->nbuckets = (uint32_t)nb;
+  ix->table.alloc((size_t)2 * nb);
+  CLAST_CK(cudaMemsetAsync(ix->table.p, 0xff, (size_t)2 * nb * sizeof(ulonglong2), st));
+  // Bloom filter: about 24 bits per key, between 2^12 and 2^F bits; F = 28
+  // (32 MB, L2-resident next to the streams that pass through L2 while
+  // seeding) unless CLAST_FILTER_BITS says otherwise (16..32)
   int fbits = 28;
   if (const char* e = std::getenv("CLAST_FILTER_BITS")) fbits = std::max(16, std::min(32, std::atoi(e)));
-  ix->filter_bits = std::min(2 * l, fbits);
-  ix->fshift = 2 * l - ix->filter_bits;
-  ix->filter.alloc((((size_t)1 << ix->filter_bits) + 31) / 32);
-  index_filter(ix->ukeys.p, nu, ix->fshift, ix->filter_bits, ix->filter.p, st);
-  CLAST_CK(cudaStreamSynchronize(st));
+  int bits = 12;
+  while (bits < fbits && (1ll << bits) < nu * 24) ++bits;
+  ix->fshift = 64 - (bits - 5);
+  ix->filter.alloc((size_t)1 << (bits - 5));
+  CLAST_CK(cudaMemsetAsync(ix->filter.p, 0, ((size_t)1 << (bits - 5)) * sizeof(uint32_t), st));
+  unsigned long long* failed = reinterpret_cast<unsigned long long*>(ws.get<int64_t>("ix_failed", 1));
+  CLAST_CK(cudaMemsetAsync(failed, 0, sizeof(unsigned long long), st));
+  index_table(ukeys, ustart, ucnt, ix->entries.p, nu, ix->table.p, ix->nbuckets, ix->filter.p, ix->fshift, failed,
+              st);
+  const int64_t nfail = read_scalar(reinterpret_cast<int64_t*>(failed), st);
+  if (nfail != 0) throw std::runtime_error("index table overflow");
+  ix->n_keys = nu;
 }
 
 // Index of a window whose padded base array is already on the device.
@@ -378,7 +381,7 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   const TargetView tv = ix->tview();
   const int64_t ns = qb.nstrands, nr = ns / 2;
   out = DevHits();
-  if (ns == 0 || ix->n_unique == 0) return;
+  if (ns == 0 || ix->n_keys == 0) return;
   // createRawSeedList + deleteSeedsOnSequenceBoundary, one pass
   int64_t* off = ws.get<int64_t>("s_off", ns + 1);
   int32_t* len32 = ws.get<int32_t>("s_len32", ns);
@@ -1134,7 +1137,7 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
       out->n = F;
       return CLAST_OK;
     };
-    if (ns == 0 || ix->n_unique == 0) return finish(0);
+    if (ns == 0 || ix->n_keys == 0) return finish(0);
     // createRawSeedList + deleteSeedsOnSequenceBoundary, one pass
     int64_t* off = ws.get<int64_t>("s_off", ns + 1);
     int32_t* len32 = ws.get<int32_t>("s_len32", ns);

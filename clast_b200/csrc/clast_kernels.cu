@@ -3,10 +3,10 @@
 // Reference (masayano/CLAST) stages and the kernels that replace them:
 //   SRead2bit/SRepelHasOddBase + CDeviceSeqList_query::createHashIndex -> pack_bases, kmer_at
 //   CDeviceHashTable (sort_by_key, unique, reduce_by_key, scan, cut)   -> sample_keys,
-//       radix_sort_pairs, index_* (directory for O(1) lookups)
-//   createRawSeedList (binarySearch, writeSeedList)                     -> seed_count, seed_write
-//   deleteSeedsOnSequenceBoundary                                       -> folded into seed_write
-//   sortSeeds / deletingIsolateSeeds / deleteDuplicateSeeds             -> segmented_sort, seed_filter
+//       radix_sort_pairs, index_* (hash table + Bloom filter for one-probe lookups)
+//   createRawSeedList (binarySearch, writeSeedList)                     -> seed_fused
+//   deleteSeedsOnSequenceBoundary                                       -> folded into seed_fused
+//   sortSeeds / deletingIsolateSeeds / deleteDuplicateSeeds             -> seed_sort_filter
 //   globalAlign* / localAlign* + calculateEvalue + deleteBadHits        -> banded_dp
 //   resultSorting + deleteHits_duplicateResult                          -> final_* (per read)
 #include <cuda_runtime.h>
@@ -345,145 +345,116 @@ __global__ void k_index_buckets(const int64_t* __restrict__ ufirst, const int64_
   ucnt[k] = (int32_t)(b - a);
 }
 
-__global__ void k_index_filter(const uint64_t* __restrict__ ukeys, int64_t nu, int fshift,
-                               uint32_t* __restrict__ filter) {
+// Inserts every key that keeps entries into the open-addressing table and
+// its three bits into the blocked Bloom filter.  Placement within a probe
+// chain depends on thread timing; lookups match the exact key, so results do
+// not.
+__global__ void k_index_table(const uint64_t* __restrict__ ukeys, const int32_t* __restrict__ ustart,
+                              const int32_t* __restrict__ ucnt, const int2* __restrict__ entries, int64_t nu,
+                              ulonglong2* __restrict__ table, uint32_t nbuckets, uint32_t* __restrict__ filter,
+                              int fshift, unsigned long long* __restrict__ failed) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nu) return;
-  const uint64_t fb = ukeys[k] >> fshift;
-  atomicOr(&filter[fb >> 5], 1u << (fb & 31));
-}
-
-__global__ void k_index_dir(const uint64_t* __restrict__ ukeys, int64_t nu, int shift, int64_t nslots,
-                            uint32_t* __restrict__ dir) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p > nslots) return;
-  const uint64_t target = (uint64_t)p << shift;
-  int64_t lo = 0, hi = nu;
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (ukeys[mid] < target) lo = mid + 1;
-    else hi = mid;
+  const int c = ucnt[k];
+  if (c <= 0) return;  // removed by the repeat cut, or joints only
+  const uint64_t h = key_hash(ukeys[k]);
+  atomicOr(filter + filter_word(h, fshift), filter_mask(h));
+  uint64_t payload;
+  if (c == 1) {
+    const int2 e = entries[ustart[k]];
+    payload = ((uint64_t)(uint32_t)e.x << 32) | (uint32_t)e.y;
+  } else {
+    payload = kMulti | ((uint64_t)(uint32_t)ustart[k] << 32) | (uint32_t)c;
   }
-  dir[p] = (uint32_t)lo;
+  // a record is claimed through its payload (free = kNoPayload); the hash is
+  // written after the claim, before any lookup kernel runs
+  uint32_t b = bucket_of(h, nbuckets);
+  for (uint32_t probe = 0; probe < nbuckets; ++probe) {
+    for (int j = 0; j < 2; ++j) {
+      ulonglong2* r = table + 2 * (size_t)b + j;
+      if (atomicCAS(reinterpret_cast<unsigned long long*>(&r->y), (unsigned long long)kNoPayload,
+                    (unsigned long long)payload) == (unsigned long long)kNoPayload) {
+        r->x = h;
+        return;
+      }
+    }
+    b = (b + 1 == nbuckets) ? 0 : b + 1;
+  }
+  atomicAdd(failed, 1ull);  // unreachable: the table always has free records
 }
 
 // ------------------------------------------------------------------------
 // seeds
 // ------------------------------------------------------------------------
-__global__ void k_seed_count(QueryView q, IndexView ix, int64_t* __restrict__ cnt,
-                             unsigned long long* __restrict__ n_kmers, int32_t* __restrict__ kidx) {
-  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (s >= q.nstrands) return;
-  const int64_t st = q.start[s];
-  const int nk = q.len[s] - ix.l + 1;
-  int64_t sum = 0;
-  int valid = 0;
-  for (int qi = lane; qi < nk; qi += 32) {
-    uint64_t key;
-    int32_t hit = -1;
-    if (kmer_at(q.packed, q.nmask, st + qi, ix.l, key)) {
-      ++valid;
-      const int64_t u = index_lookup(ix, key);
-      if (u >= 0) {
-        const int c = ix.ucnt[u];
-        sum += c;
-        if (c > 0) hit = (int32_t)u;
-      }
-    }
-    kidx[st + qi] = hit;  // the write pass reuses the lookup
+// Seeding in one pass, one warp per strand: every l-mer is looked up once; the
+// first kSeedRegChunks*32 results stay in registers (longer strands look the
+// rest up again in the second phase).  The lookups of those chunks are issued
+// together, stage by stage (query words, filter words, first table records),
+// so one strand waits for about one latency of each level instead of one per
+// chunk.  The strand's seeds get one contiguous range from an atomic cursor; if
+// the range would pass `cap`, nothing is written and the host reruns with a
+// larger buffer (the cursor then holds the exact total).  Seeds are written in
+// the reference's order: l-mer position ascending, then bucket order (window
+// position ascending).
+constexpr int kSeedRegChunks = 5;
+constexpr int kSeedParts = 32;
+
+__device__ __forceinline__ uint64_t seed_lookup(const QueryView& q, const IndexView& ix, int64_t st, int qi,
+                                                int nk, int& valid) {
+  uint64_t key;
+  if (qi < nk && kmer_at(q.packed, q.nmask, st + qi, ix.l, key)) {
+    ++valid;
+    return index_find(ix, key);
   }
-#pragma unroll
-  for (int o = 16; o; o >>= 1) {
-    sum += __shfl_xor_sync(kFull, sum, o);
-    valid += __shfl_xor_sync(kFull, valid, o);
-  }
-  if (lane == 0) {
-    cnt[s] = sum;
-    if (valid) atomicAdd(n_kmers, (unsigned long long)valid);
-  }
+  return kNoPayload;
 }
 
-__global__ void k_seed_write(QueryView q, IndexView ix, TargetView t, int gap, int local,
-                             const int64_t* __restrict__ off, const int32_t* __restrict__ kidx,
-                             uint64_t* __restrict__ skey, uint32_t* __restrict__ sq,
-                             int32_t* __restrict__ nvalid) {
-  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (s >= q.nstrands) return;
-  const int64_t st = q.start[s];
-  const int qlen = q.len[s];
-  const int nk = qlen - ix.l + 1;
-  int64_t base = off[s];
-  int valid = 0;
-  for (int c0 = 0; c0 < nk; c0 += 32) {
-    const int qi = c0 + lane;
-    int c = 0, us = 0;
-    if (qi < nk) {
-      const int32_t u = kidx[st + qi];
-      if (u >= 0) {
-        c = ix.ucnt[u];
-        us = ix.ustart[u];
-      }
-    }
+// Writes the seeds of one chunk of 32 l-mers (lane = l-mer qi, payload pl) at
+// w onwards and advances w past the chunk's seeds.
+__device__ __forceinline__ void seed_emit(const IndexView& ix, const TargetView& t, int gap, int local, int qlen,
+                                          int qi, uint64_t pl, int lane, int64_t& w, int& valid,
+                                          uint64_t* __restrict__ skey, uint32_t* __restrict__ sq) {
+  const int c = payload_count(pl);
+  int excl, chunk_total;
+  if (!__any_sync(kFull, c > 1)) {  // common case: at most one entry per l-mer
+    const unsigned b = __ballot_sync(kFull, c > 0);
+    excl = __popc(b & lanemask_lt());
+    chunk_total = __popc(b);
+  } else {
     int incl = c;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int y = __shfl_up_sync(kFull, incl, o);
       if (lane >= o) incl += y;
     }
-    const int total = __shfl_sync(kFull, incl, 31);
-    const int64_t w0 = base + incl - c;
+    excl = incl - c;
+    chunk_total = __shfl_sync(kFull, incl, 31);
+  }
+  if (c) {
+    const int64_t w0 = w + excl;
+    const bool multi = (pl & kMulti) != 0;
+    const int us = (int)(pl >> 32) & 0x7fffffff;
     for (int i = 0; i < c; ++i) {
-      const int2 e = ix.entries[us + i];
+      const int2 e = multi ? __ldcs(ix.entries + us + i) : make_int2((int)(pl >> 32), (int)(uint32_t)pl);
       const int s0 = e.y - qi;  // tHitStartIdx, is_onCorner
       const bool drop = !local && ((s0 + gap < 0) || (s0 + qlen - gap > t.lengths[e.x]));
-      skey[w0 + i] = drop ? kDroppedSeed : (((uint64_t)(uint32_t)e.x << 32) | ((uint32_t)s0 ^ 0x80000000u));
-      sq[w0 + i] = (uint32_t)qi;
+      // streaming stores: the seeds must not evict the filter from L2
+      __stcs(reinterpret_cast<unsigned long long*>(skey + w0 + i),
+             drop ? kDroppedSeed : (((uint64_t)(uint32_t)e.x << 32) | ((uint32_t)s0 ^ 0x80000000u)));
+      __stcs(sq + w0 + i, (uint32_t)qi);
       valid += drop ? 0 : 1;
     }
-    base += total;
   }
-#pragma unroll
-  for (int o = 16; o; o >>= 1) valid += __shfl_xor_sync(kFull, valid, o);
-  if (lane == 0) nvalid[s] = valid;
+  w += chunk_total;
 }
 
-// Seeding in one pass, one warp per strand: every l-mer is looked up once; the
-// first kSeedRegChunks*32 results stay in registers (longer strands look the
-// rest up again in the second phase).  The strand's seeds get one contiguous
-// range from an atomic cursor; if the range would pass `cap`, nothing is
-// written and the host reruns with a larger buffer (the cursor then holds the
-// exact total).  Seeds are written in the reference's order: l-mer position
-// ascending, then bucket order (window position ascending).
-constexpr int kSeedRegChunks = 8;
-constexpr int kSeedParts = 32;
-
-__device__ __forceinline__ void seed_lookup(const QueryView& q, const IndexView& ix, int64_t st, int qi, int nk,
-                                            int& u, int& c, int& valid) {
-  u = -1;
-  c = 0;
-  if (qi < nk) {
-    uint64_t key;
-    if (kmer_at(q.packed, q.nmask, st + qi, ix.l, key)) {
-      ++valid;
-      const int64_t x = index_lookup(ix, key);
-      if (x >= 0) {
-        const int k = __ldcs(ix.ucnt + x);
-        if (k > 0) {
-          u = (int)x;
-          c = k;
-        }
-      }
-    }
-  }
-}
-
-constexpr int kSeedFusedThreads = 256;
+constexpr int kSeedFusedThreads = 128;
 
 // The seed buffer is split into kSeedParts partitions of part_cap seeds, each
 // with its own cursor; strand s takes its range in partition s % kSeedParts, so
 // the range reservations of neighbouring warps hit different counters.
+// SMALL: l <= 16, keys read with 32-bit funnel shifts.
+template <bool SMALL>
 __global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, IndexView ix, TargetView t, int gap,
                                                                    int local, unsigned long long* __restrict__ cursor,
                                                                    unsigned long long* __restrict__ n_kmers,
@@ -491,31 +462,74 @@ __global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, I
                                                                    int32_t* __restrict__ nvalid,
                                                                    uint64_t* __restrict__ skey,
                                                                    uint32_t* __restrict__ sq, int64_t part_cap) {
+  constexpr int R = kSeedRegChunks;
   const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (s >= q.nstrands) return;
   const int64_t st = q.start[s];
   const int qlen = q.len[s];
   const int nk = qlen - ix.l + 1;
-  int ureg[kSeedRegChunks];
-  int total = 0, valid_kmers = 0;
+  // does the strand hold any non-ACGT base?  (one vote over its mask words)
+  bool any_n = false;
+  if (qlen > 0) {
+    const int64_t w0 = st >> 6, w1 = (st + qlen - 1) >> 6;
+    for (int64_t w = w0 + lane; w <= w1; w += 32) {
+      uint64_t m = ld_stream(q.nmask + w);
+      if (w == w0) m &= ~0ull >> (st & 63);
+      if (w == w1) m &= ~0ull << (63 - ((st + qlen - 1) & 63));
+      any_n |= m != 0;
+    }
+    any_n = __any_sync(kFull, any_n);
+  }
+  uint64_t preg[R];
+  uint32_t vmask = 0;
+  {
+    uint64_t hh[R];
 #pragma unroll
-  for (int ci = 0; ci < kSeedRegChunks; ++ci) {
-    int u = -1, c = 0;
-    if (ci * 32 < nk) seed_lookup(q, ix, st, ci * 32 + lane, nk, u, c, valid_kmers);
-    ureg[ci] = u;
-    total += c;
-  }
-  for (int c0 = kSeedRegChunks * 32; c0 < nk; c0 += 32) {
-    int u, c;
-    seed_lookup(q, ix, st, c0 + lane, nk, u, c, valid_kmers);
-    total += c;
-  }
+    for (int ci = 0; ci < R; ++ci) {
+      const int qi = ci * 32 + lane;
+      const int64_t f = st + qi;
+      bool v = qi < nk;
+      uint64_t key = 0;
+      if (SMALL) {
+        v = v && !(any_n && kmer_has_n16(reinterpret_cast<const uint32_t*>(q.nmask), f, ix.l));
+        if (v) key = kmer_key16(reinterpret_cast<const uint32_t*>(q.packed), f, ix.l);
+      } else {
+        v = v && !(any_n && kmer_has_n(q.nmask, f, ix.l));
+        if (v) key = kmer_key(q.packed, f, ix.l);
+      }
+      hh[ci] = key_hash(key);
+      vmask |= (uint32_t)v << ci;
+    }
+    uint32_t fw[R];
 #pragma unroll
-  for (int o = 16; o; o >>= 1) {
-    total += __shfl_xor_sync(kFull, total, o);
-    valid_kmers += __shfl_xor_sync(kFull, valid_kmers, o);
+    for (int ci = 0; ci < R; ++ci) fw[ci] = ((vmask >> ci) & 1u) ? __ldg(ix.filter + filter_word(hh[ci], ix.fshift)) : 0u;
+    ulonglong2 rec[R];
+    uint32_t pmask = 0;
+#pragma unroll
+    for (int ci = 0; ci < R; ++ci) {
+      const bool pass = ((vmask >> ci) & 1u) && filter_pass(fw[ci], hh[ci]);
+      pmask |= (uint32_t)pass << ci;
+      rec[ci] = make_ulonglong2(0ull, kNoPayload);
+      if (pass) rec[ci] = __ldcs(ix.table + 2 * (size_t)bucket_of(hh[ci], ix.nbuckets));
+    }
+#pragma unroll
+    for (int ci = 0; ci < R; ++ci) {
+      uint64_t pl = kNoPayload;
+      if ((pmask >> ci) & 1u) {
+        if (rec[ci].x == hh[ci]) pl = rec[ci].y;
+        else if (rec[ci].y != kNoPayload) pl = table_probe(ix, hh[ci], bucket_of(hh[ci], ix.nbuckets), 1);
+      }
+      preg[ci] = pl;
+    }
   }
+  int total = 0, valid_kmers = __popc(vmask);
+#pragma unroll
+  for (int ci = 0; ci < R; ++ci) total += payload_count(preg[ci]);
+  for (int c0 = R * 32; c0 < nk; c0 += 32)
+    total += payload_count(seed_lookup(q, ix, st, c0 + lane, nk, valid_kmers));
+  total = (int)__reduce_add_sync(kFull, (unsigned)total);
+  valid_kmers = (int)__reduce_add_sync(kFull, (unsigned)valid_kmers);
   const int part = (int)(s % kSeedParts);
   unsigned long long rel = 0;
   if (lane == 0) {
@@ -535,42 +549,15 @@ __global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, I
   }
   int64_t w = (int64_t)base;
   int valid = 0;
-  for (int c0 = 0, ci = 0; c0 < nk; c0 += 32, ++ci) {
-    const int qi = c0 + lane;
-    int u = -1, c = 0, dummy = 0;
-    if (ci < kSeedRegChunks) {
 #pragma unroll
-      for (int k = 0; k < kSeedRegChunks; ++k)
-        if (k == ci) u = ureg[k];
-      if (u >= 0) c = ix.ucnt[u];
-    } else {
-      seed_lookup(q, ix, st, qi, nk, u, c, dummy);
-    }
-    int incl = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += y;
-    }
-    const int chunk_total = __shfl_sync(kFull, incl, 31);
-    if (c) {
-      const int us = ix.ustart[u];
-      const int64_t w0 = w + incl - c;
-      for (int i = 0; i < c; ++i) {
-        const int2 e = ix.entries[us + i];
-        const int s0 = e.y - qi;  // tHitStartIdx, is_onCorner
-        const bool drop = !local && ((s0 + gap < 0) || (s0 + qlen - gap > t.lengths[e.x]));
-        // streaming stores: the seeds must not evict the presence filter from L2
-        __stcs(reinterpret_cast<unsigned long long*>(skey + w0 + i),
-               drop ? kDroppedSeed : (((uint64_t)(uint32_t)e.x << 32) | ((uint32_t)s0 ^ 0x80000000u)));
-        __stcs(sq + w0 + i, (uint32_t)qi);
-        valid += drop ? 0 : 1;
-      }
-    }
-    w += chunk_total;
+  for (int ci = 0; ci < R; ++ci)
+    if (ci * 32 < nk) seed_emit(ix, t, gap, local, qlen, ci * 32 + lane, preg[ci], lane, w, valid, skey, sq);
+  for (int c0 = R * 32; c0 < nk; c0 += 32) {
+    int dummy = 0;
+    const uint64_t pl = seed_lookup(q, ix, st, c0 + lane, nk, dummy);
+    seed_emit(ix, t, gap, local, qlen, c0 + lane, pl, lane, w, valid, skey, sq);
   }
-#pragma unroll
-  for (int o = 16; o; o >>= 1) valid += __shfl_xor_sync(kFull, valid, o);
+  valid = (int)__reduce_add_sync(kFull, (unsigned)valid);
   if (lane == 0) nvalid[s] = valid;
 }
 
@@ -757,10 +744,6 @@ void seg_sort(Workspace& ws, uint64_t* k1, K2* k2, int32_t* pay, const int64_t* 
   CLAST_LAUNCHED();
 }
 
-__global__ void k_to_i32(const int64_t* __restrict__ in, int64_t n, int32_t* __restrict__ out) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = (int32_t)in[i];
-}
 
 // is "s" near its predecessor "p" (hasNotNearPair / hasNearPair, same strand)
 __device__ __forceinline__ bool near_pred(int tid, int tidx, int diag, int ptid, int ptidx, int pdiag,
@@ -768,80 +751,6 @@ __device__ __forceinline__ bool near_pred(int tid, int tidx, int diag, int ptid,
   return tid == ptid && width >= tidx - ptidx && width >= ptidx - tidx && gap >= pdiag - diag;
 }
 
-__global__ void k_seed_filter(uint64_t* __restrict__ skey, uint32_t* __restrict__ sq,
-                              const int64_t* __restrict__ off, const int32_t* __restrict__ nvalid,
-                              const int32_t* __restrict__ wstart, int nwin, const int32_t* __restrict__ wfirst,
-                              int width, int gap, int64_t nstrands, int32_t* __restrict__ hcnt) {
-  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (s >= nstrands) return;
-  const int n = nvalid[s];
-  if (n == 0) {
-    if (lane == 0) hcnt[s] = 0;
-    return;
-  }
-  int lo = 0, hi = nwin;  // window of strand s
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (wstart[mid] <= s) lo = mid;
-    else hi = mid;
-  }
-  const bool wf = (wfirst[lo] == (int32_t)s);
-  const int64_t o = off[s];
-  const unsigned lt = lanemask_lt();
-  int ptid = 0, ptidx = 0, pdiag = 0;          // element j-1 of the previous chunk
-  bool have_surv = false;
-  int stid = 0, stidx = 0, sdiag = 0;          // last A8 survivor so far
-  int64_t out = o;
-  for (int c0 = 0; c0 < n; c0 += 32) {
-    const int j = c0 + lane;
-    const bool in = j < n;
-    uint64_t k = 0;
-    uint32_t qi = 0;
-    if (in) {
-      k = skey[o + j];
-      qi = sq[o + j];
-    }
-    const int tid = (int)(k >> 32);
-    const int diag = (int)((uint32_t)k ^ 0x80000000u);
-    const int tidx = diag + (int)qi;
-    int ptid_l = __shfl_up_sync(kFull, tid, 1);
-    int ptidx_l = __shfl_up_sync(kFull, tidx, 1);
-    int pdiag_l = __shfl_up_sync(kFull, diag, 1);
-    if (lane == 0) { ptid_l = ptid; ptidx_l = ptidx; pdiag_l = pdiag; }
-    bool keep8 = false;
-    if (in) keep8 = (j == 0) ? wf : near_pred(tid, tidx, diag, ptid_l, ptidx_l, pdiag_l, width, gap);
-    const unsigned b8 = __ballot_sync(kFull, keep8);
-    const unsigned below = b8 & lt;
-    const int src = below ? 31 - __clz(below) : 0;
-    const int qtid = __shfl_sync(kFull, tid, src);
-    const int qtidx = __shfl_sync(kFull, tidx, src);
-    const int qdiag = __shfl_sync(kFull, diag, src);
-    bool keep9 = keep8;
-    if (keep8) {
-      if (below) keep9 = !near_pred(tid, tidx, diag, qtid, qtidx, qdiag, width, gap);
-      else if (have_surv) keep9 = !near_pred(tid, tidx, diag, stid, stidx, sdiag, width, gap);
-    }
-    const unsigned b9 = __ballot_sync(kFull, keep9);
-    if (keep9) {
-      const int64_t w = out + __popc(b9 & lt);
-      skey[w] = k;
-      sq[w] = qi;
-    }
-    out += __popc(b9);
-    ptid = __shfl_sync(kFull, tid, 31);
-    ptidx = __shfl_sync(kFull, tidx, 31);
-    pdiag = __shfl_sync(kFull, diag, 31);
-    if (b8) {
-      const int last = 31 - __clz(b8);
-      stid = __shfl_sync(kFull, tid, last);
-      stidx = __shfl_sync(kFull, tidx, last);
-      sdiag = __shfl_sync(kFull, diag, last);
-      have_surv = true;
-    }
-  }
-  if (lane == 0) hcnt[s] = (int32_t)(out - o);
-}
 
 // ---- seed sort fused with the isolate / duplicate filters ----
 struct SeedFilterCtx {
@@ -1562,44 +1471,30 @@ void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n_unique,
   k_index_buckets<<<blocks_for(n_unique, 256), 256, 0, st>>>(ufirst, kpos, n_unique, ustart, ucnt);
   CLAST_LAUNCHED();
 }
-void index_filter(const uint64_t* ukeys, int64_t n_unique, int fshift, int filter_bits, uint32_t* filter,
-                  cudaStream_t st) {
-  const int64_t words = ((1ll << filter_bits) + 31) / 32;
-  CLAST_CK(cudaMemsetAsync(filter, 0, words * sizeof(uint32_t), st));
-  if (n_unique <= 0) return;
-  k_index_filter<<<blocks_for(n_unique, 256), 256, 0, st>>>(ukeys, n_unique, fshift, filter);
-  CLAST_LAUNCHED();
-}
 
-void index_directory(const uint64_t* ukeys, int64_t n_unique, int shift, int dir_bits, uint32_t* dir,
-                     cudaStream_t st) {
-  const int64_t nslots = 1ll << dir_bits;
-  k_index_dir<<<blocks_for(nslots + 1, 256), 256, 0, st>>>(ukeys, n_unique, shift, nslots, dir);
-  CLAST_LAUNCHED();
-}
 
-void seed_count(const QueryView& q, const IndexView& ix, int64_t* cnt, unsigned long long* n_kmers,
-                int32_t* kidx, cudaStream_t st) {
-  if (q.nstrands <= 0) return;
-  k_seed_count<<<blocks_for((int64_t)q.nstrands * 32, 256), 256, 0, st>>>(q, ix, cnt, n_kmers, kidx);
-  CLAST_LAUNCHED();
-}
-void seed_write(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
-                const int64_t* off, const int32_t* kidx, uint64_t* skey, uint32_t* sq, int32_t* nvalid,
-                cudaStream_t st) {
-  if (q.nstrands <= 0) return;
-  k_seed_write<<<blocks_for((int64_t)q.nstrands * 32, 256), 256, 0, st>>>(q, ix, t, gap, local, off, kidx, skey,
-                                                                           sq, nvalid);
-  CLAST_LAUNCHED();
-}
 int seed_parts() { return kSeedParts; }
 
 void seed_fused(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
                 unsigned long long* cursors, unsigned long long* n_kmers, int64_t* off, int32_t* cnt, int32_t* nvalid,
                 uint64_t* skey, uint32_t* sq, int64_t part_cap, cudaStream_t st) {
   if (q.nstrands <= 0) return;
-  k_seed_fused<<<blocks_for((int64_t)q.nstrands * 32, kSeedFusedThreads), kSeedFusedThreads, 0, st>>>(
-      q, ix, t, gap, local, cursors, n_kmers, off, cnt, nvalid, skey, sq, part_cap);
+  const unsigned grid = blocks_for((int64_t)q.nstrands * 32, kSeedFusedThreads);
+  if (ix.l <= 16)
+    k_seed_fused<true><<<grid, kSeedFusedThreads, 0, st>>>(q, ix, t, gap, local, cursors, n_kmers, off, cnt, nvalid,
+                                                          skey, sq, part_cap);
+  else
+    k_seed_fused<false><<<grid, kSeedFusedThreads, 0, st>>>(q, ix, t, gap, local, cursors, n_kmers, off, cnt, nvalid,
+                                                           skey, sq, part_cap);
+  CLAST_LAUNCHED();
+}
+
+void index_table(const uint64_t* ukeys, const int32_t* ustart, const int32_t* ucnt, const int2* entries,
+                 int64_t n_unique, ulonglong2* table, uint32_t nbuckets, uint32_t* filter, int fshift,
+                 unsigned long long* failed, cudaStream_t st) {
+  if (n_unique <= 0) return;
+  k_index_table<<<blocks_for(n_unique, 256), 256, 0, st>>>(ukeys, ustart, ucnt, entries, n_unique, table, nbuckets,
+                                                            filter, fshift, failed);
   CLAST_LAUNCHED();
 }
 
@@ -1610,26 +1505,9 @@ void window_first(const int32_t* nvalid, const int32_t* win_start, int n_windows
                                                                             win_first);
   CLAST_LAUNCHED();
 }
-void segmented_sort_u32(Workspace& ws, uint64_t* k1, uint32_t* k2, const int64_t* off, const int32_t* len,
-                        int64_t n_segments, cudaStream_t st, int tag) {
-  seg_sort<uint32_t, false>(ws, k1, k2, nullptr, off, len, n_segments, st, tag);
-}
 void segmented_sort_u64(Workspace& ws, uint64_t* k1, uint64_t* k2, int32_t* payload, const int64_t* off,
                         const int32_t* len, int64_t n_segments, cudaStream_t st, int tag) {
   seg_sort<uint64_t, true>(ws, k1, k2, payload, off, len, n_segments, st, tag);
-}
-void to_i32(const int64_t* in, int64_t n, int32_t* out, cudaStream_t st) {
-  if (n <= 0) return;
-  k_to_i32<<<blocks_for(n, 256), 256, 0, st>>>(in, n, out);
-  CLAST_LAUNCHED();
-}
-void seed_filter(uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t* nvalid, const int32_t* win_start,
-                 int n_windows, const int32_t* win_first, int width, int gap, int64_t nstrands, int32_t* hcnt,
-                 cudaStream_t st) {
-  if (nstrands <= 0) return;
-  k_seed_filter<<<blocks_for(nstrands * 32, 256), 256, 0, st>>>(skey, sq, off, nvalid, win_start, n_windows,
-                                                                 win_first, width, gap, nstrands, hcnt);
-  CLAST_LAUNCHED();
 }
 void seed_sort_filter(Workspace& ws, uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t* cnt,
                       const int32_t* nvalid, const int32_t* win_start, int n_windows, const int32_t* win_first,

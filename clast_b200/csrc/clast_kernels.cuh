@@ -48,20 +48,16 @@ void index_entries(const int32_t* keep, const int64_t* kpos, const int2* resolve
                    int2* entries, cudaStream_t st);
 void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n_unique, int32_t* ustart,
                    int32_t* ucnt, cudaStream_t st);
-void index_directory(const uint64_t* ukeys, int64_t n_unique, int shift, int dir_bits, uint32_t* dir,
-                     cudaStream_t st);
-// Presence filter: bit (key >> fshift) set for every unique key; 2^filter_bits bits.
-void index_filter(const uint64_t* ukeys, int64_t n_unique, int fshift, int filter_bits, uint32_t* filter,
-                  cudaStream_t st);
+// Open-addressing table of every key with entries (payload: its only entry,
+// or kMulti | start << 32 | count) and its blocked Bloom filter words
+// (2^(64 - fshift) 32-bit words, zeroed by the caller; table records set to ~0).
+// *failed counts keys that found no free record (none when the table has
+// more records than keys).
+void index_table(const uint64_t* ukeys, const int32_t* ustart, const int32_t* ucnt, const int2* entries,
+                 int64_t n_unique, ulonglong2* table, uint32_t nbuckets, uint32_t* filter, int fshift,
+                 unsigned long long* failed, cudaStream_t st);
 
 // ---- seeds (CDeviceHitList_createRawSeedList.cu, _deleteSeeds*.cu, _sortSeeds.cu) ----
-// cnt[s] = seeds of strand s before the corner filter; *n_kmers += valid l-mers;
-// kidx[f] = unique-key index of the l-mer at strand position f, -1 when it seeds nothing
-void seed_count(const QueryView& q, const IndexView& ix, int64_t* cnt, unsigned long long* n_kmers,
-                int32_t* kidx, cudaStream_t st);
-void seed_write(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
-                const int64_t* off, const int32_t* kidx, uint64_t* skey, uint32_t* sq, int32_t* nvalid,
-                cudaStream_t st);
 // One-pass seeding (lookups once): off/cnt/nvalid per strand, seeds in skey/sq,
 // which hold seed_parts() partitions of part_cap seeds.  Strand s reserves its
 // range in partition s % seed_parts() through cursors[partition]; a partition
@@ -77,12 +73,8 @@ void window_first(const int32_t* nvalid, const int32_t* win_start, int n_windows
 // Sorts every segment [off[i], off[i]+len[i]) of (k1, k2[, payload]) ascending by
 // (k1, k2).  Segments of <= 32 are sorted by one warp in registers, <= 2048 by one
 // CTA in shared memory, longer ones by one CTA in global memory.
-void segmented_sort_u32(Workspace& ws, uint64_t* k1, uint32_t* k2, const int64_t* off, const int32_t* len,
-                        int64_t n_segments, cudaStream_t st, int tag);
 void segmented_sort_u64(Workspace& ws, uint64_t* k1, uint64_t* k2, int32_t* payload, const int64_t* off,
                         const int32_t* len, int64_t n_segments, cudaStream_t st, int tag);
-// seed counts per strand (int32) from the int64 count array
-void to_i32(const int64_t* in, int64_t n, int32_t* out, cudaStream_t st);
 
 // sortSeeds + deletingIsolateSeeds + deleteDuplicateSeeds per strand: sorts the
 // cnt[s] seeds of strand s by (sequence, diagonal, qIdx) and writes the surviving
@@ -90,9 +82,6 @@ void to_i32(const int64_t* in, int64_t n, int32_t* out, cudaStream_t st);
 void seed_sort_filter(Workspace& ws, uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t* cnt,
                       const int32_t* nvalid, const int32_t* win_start, int n_windows, const int32_t* win_first,
                       int width, int gap, int64_t nstrands, int32_t* hcnt, cudaStream_t st);
-void seed_filter(uint64_t* skey, uint32_t* sq, const int64_t* off, const int32_t* nvalid,
-                 const int32_t* win_start, int n_windows, const int32_t* win_first, int width, int gap,
-                 int64_t nstrands, int32_t* hcnt, cudaStream_t st);
 // also adds band * (qlen - l) DP cells per hit to *cells
 void gather_hits(const uint64_t* skey, const uint32_t* sq, const int64_t* off, const int32_t* hcnt,
                  const int64_t* hoff, int64_t nstrands, uint64_t* hk, int32_t* hq, int32_t* hs,

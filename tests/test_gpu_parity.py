@@ -39,7 +39,7 @@ def test_gap_and_mode(engine, gap, local):
     compare(got, want)
 
 
-@pytest.mark.parametrize("lmer,stride", [(8, 3), (11, 1), (20, 7), (31, 5)])
+@pytest.mark.parametrize("lmer,stride", [(8, 3), (11, 1), (16, 4), (17, 2), (20, 7), (31, 5)])
 def test_lmer_stride(engine, lmer, stride):
     s, tl, ql = make_case(20 + lmer, setting=api.Setting(lmer=lmer, stride=stride))
     got, want = run_pair(engine, s, tl, ql)
