@@ -1043,7 +1043,7 @@ size_t fixed_scratch_bytes(int64_t n, int64_t ns, int parts) {
   const size_t nb = (size_t)n, s = (size_t)ns;
   return r(nb + 2 * kPad) + r(8 * s) + r(4 * s) + r(4 * s) + r(8) + r(8 * (nb / 32 + 4)) + r(8 * (nb / 64 + 4)) +
          r(8 * (s + 1)) + r(4 * s) + r(4 * s) + r(8 * (2 + (size_t)parts)) + r(4 * s) + r(8 * (s + 1)) +
-         r(12 * s) + (64 << 10);
+         r(16 * s) + (64 << 10);
 }
 
 // Clears the busy flag of a device's scratch once the call's stream work has

@@ -11,6 +11,7 @@
 //   resultSorting + deleteHits_duplicateResult                          -> final_* (per read)
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cstdint>
 #include <stdexcept>
@@ -393,9 +394,7 @@ __global__ void k_index_table(const uint64_t* __restrict__ ukeys, const int32_t*
 // so one strand waits for about one latency of each level instead of one per
 // chunk.  The strand's seeds get one contiguous range from an atomic cursor; if
 // the range would pass `cap`, nothing is written and the host reruns with a
-// larger buffer (the cursor then holds the exact total).  Seeds are written in
-// the reference's order: l-mer position ascending, then bucket order (window
-// position ascending).
+// larger buffer (the cursor then holds the exact total).
 constexpr int kSeedRegChunks = 5;
 constexpr int kSeedParts = 32;
 
@@ -409,50 +408,47 @@ __device__ __forceinline__ uint64_t seed_lookup(const QueryView& q, const IndexV
   return kNoPayload;
 }
 
-// Writes the seeds of one chunk of 32 l-mers (lane = l-mer qi, payload pl) at
-// w onwards and advances w past the chunk's seeds.
-__device__ __forceinline__ void seed_emit(const IndexView& ix, const TargetView& t, int gap, int local, int qlen,
-                                          int qi, uint64_t pl, int lane, int64_t& w, int& valid,
-                                          uint64_t* __restrict__ skey, uint32_t* __restrict__ sq) {
+// Writes the c = payload_count(pl) seeds of l-mer qi at w onwards.
+__device__ __forceinline__ void seed_put(const IndexView& ix, const TargetView& t, int gap, int local, int qlen,
+                                         int qi, uint64_t pl, int64_t w, int& valid, uint64_t* __restrict__ skey,
+                                         uint32_t* __restrict__ sq) {
   const int c = payload_count(pl);
-  int excl, chunk_total;
-  if (!__any_sync(kFull, c > 1)) {  // common case: at most one entry per l-mer
-    const unsigned b = __ballot_sync(kFull, c > 0);
-    excl = __popc(b & lanemask_lt());
-    chunk_total = __popc(b);
-  } else {
-    int incl = c;
+  const bool multi = (pl & kMulti) != 0;
+  const int us = (int)(pl >> 32) & 0x7fffffff;
+  for (int i = 0; i < c; ++i) {
+    const int2 e = multi ? __ldcs(ix.entries + us + i) : make_int2((int)(pl >> 32), (int)(uint32_t)pl);
+    const int s0 = e.y - qi;  // tHitStartIdx, is_onCorner
+    const bool drop = !local && ((s0 + gap < 0) || (s0 + qlen - gap > t.lengths[e.x]));
+    // streaming stores: the seeds must not evict the filter from L2
+    __stcs(reinterpret_cast<unsigned long long*>(skey + w + i),
+           drop ? kDroppedSeed : (((uint64_t)(uint32_t)e.x << 32) | ((uint32_t)s0 ^ 0x80000000u)));
+    __stcs(sq + w + i, (uint32_t)qi);
+    valid += drop ? 0 : 1;
+  }
+}
+
+// Exclusive prefix sum over the warp; *total = the warp's sum.
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
+  int incl = v;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += y;
-    }
-    excl = incl - c;
-    chunk_total = __shfl_sync(kFull, incl, 31);
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
   }
-  if (c) {
-    const int64_t w0 = w + excl;
-    const bool multi = (pl & kMulti) != 0;
-    const int us = (int)(pl >> 32) & 0x7fffffff;
-    for (int i = 0; i < c; ++i) {
-      const int2 e = multi ? __ldcs(ix.entries + us + i) : make_int2((int)(pl >> 32), (int)(uint32_t)pl);
-      const int s0 = e.y - qi;  // tHitStartIdx, is_onCorner
-      const bool drop = !local && ((s0 + gap < 0) || (s0 + qlen - gap > t.lengths[e.x]));
-      // streaming stores: the seeds must not evict the filter from L2
-      __stcs(reinterpret_cast<unsigned long long*>(skey + w0 + i),
-             drop ? kDroppedSeed : (((uint64_t)(uint32_t)e.x << 32) | ((uint32_t)s0 ^ 0x80000000u)));
-      __stcs(sq + w0 + i, (uint32_t)qi);
-      valid += drop ? 0 : 1;
-    }
-  }
-  w += chunk_total;
+  *total = __shfl_sync(kFull, incl, 31);
+  return incl - v;
 }
 
 constexpr int kSeedFusedThreads = 128;
 
 // The seed buffer is split into kSeedParts partitions of part_cap seeds, each
 // with its own cursor; strand s takes its range in partition s % kSeedParts, so
-// the range reservations of neighbouring warps hit different counters.
+// the range reservations of neighbouring warps hit different counters.  The
+// seed sort that follows orders a strand's seeds totally, so their order in
+// the range only has to be cheap to sort: l-mer order when every l-mer of the
+// register chunks has at most one entry, otherwise lane by lane; the seeds of
+// later chunks follow.  A warp loops over strands s,
+// s + (warps in the grid), ...; the launch gives every strand its own warp.
 // SMALL: l <= 16, keys read with 32-bit funnel shifts.
 template <bool SMALL>
 __global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, IndexView ix, TargetView t, int gap,
@@ -463,102 +459,139 @@ __global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, I
                                                                    uint64_t* __restrict__ skey,
                                                                    uint32_t* __restrict__ sq, int64_t part_cap) {
   constexpr int R = kSeedRegChunks;
-  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (s >= q.nstrands) return;
-  const int64_t st = q.start[s];
-  const int qlen = q.len[s];
-  const int nk = qlen - ix.l + 1;
-  // does the strand hold any non-ACGT base?  (one vote over its mask words)
-  bool any_n = false;
-  if (qlen > 0) {
-    const int64_t w0 = st >> 6, w1 = (st + qlen - 1) >> 6;
-    for (int64_t w = w0 + lane; w <= w1; w += 32) {
-      uint64_t m = ld_stream(q.nmask + w);
-      if (w == w0) m &= ~0ull >> (st & 63);
-      if (w == w1) m &= ~0ull << (63 - ((st + qlen - 1) & 63));
-      any_n |= m != 0;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < q.nstrands; s += nwarps) {
+    const int64_t st = q.start[s];
+    const int qlen = q.len[s];
+    const int nk = qlen - ix.l + 1;
+    // the strand's N-mask words (lane i: word i), loaded next to the key words
+    const int64_t nw0 = st >> 6, nw1 = (st + (qlen > 0 ? qlen : 1) - 1) >> 6;
+    uint64_t nword = 0;
+    if (qlen > 0 && nw0 + lane <= nw1) {
+      nword = ld_stream(q.nmask + nw0 + lane);
+      if (lane == 0) nword &= ~0ull >> (st & 63);
+      if (nw0 + lane == nw1) nword &= ~0ull << (63 - ((st + qlen - 1) & 63));
     }
-    any_n = __any_sync(kFull, any_n);
-  }
-  uint64_t preg[R];
-  uint32_t vmask = 0;
-  {
-    uint64_t hh[R];
+    uint64_t preg[R];
+    uint32_t vmask = 0;
+    {
+      uint64_t hh[R];
 #pragma unroll
-    for (int ci = 0; ci < R; ++ci) {
-      const int qi = ci * 32 + lane;
-      const int64_t f = st + qi;
-      bool v = qi < nk;
-      uint64_t key = 0;
-      if (SMALL) {
-        v = v && !(any_n && kmer_has_n16(reinterpret_cast<const uint32_t*>(q.nmask), f, ix.l));
-        if (v) key = kmer_key16(reinterpret_cast<const uint32_t*>(q.packed), f, ix.l);
-      } else {
-        v = v && !(any_n && kmer_has_n(q.nmask, f, ix.l));
-        if (v) key = kmer_key(q.packed, f, ix.l);
+      for (int ci = 0; ci < R; ++ci) {
+        const int qi = ci * 32 + lane;
+        const bool v = qi < nk;
+        uint64_t key = 0;
+        if (v) key = SMALL ? kmer_key16(reinterpret_cast<const uint32_t*>(q.packed), st + qi, ix.l)
+                           : kmer_key(q.packed, st + qi, ix.l);
+        hh[ci] = key_hash(key);
+        vmask |= (uint32_t)v << ci;
       }
-      hh[ci] = key_hash(key);
-      vmask |= (uint32_t)v << ci;
-    }
-    uint32_t fw[R];
+      uint32_t fw[R];
 #pragma unroll
-    for (int ci = 0; ci < R; ++ci) fw[ci] = ((vmask >> ci) & 1u) ? __ldg(ix.filter + filter_word(hh[ci], ix.fshift)) : 0u;
-    ulonglong2 rec[R];
-    uint32_t pmask = 0;
-#pragma unroll
-    for (int ci = 0; ci < R; ++ci) {
-      const bool pass = ((vmask >> ci) & 1u) && filter_pass(fw[ci], hh[ci]);
-      pmask |= (uint32_t)pass << ci;
-      rec[ci] = make_ulonglong2(0ull, kNoPayload);
-      if (pass) rec[ci] = __ldcs(ix.table + 2 * (size_t)bucket_of(hh[ci], ix.nbuckets));
-    }
-#pragma unroll
-    for (int ci = 0; ci < R; ++ci) {
-      uint64_t pl = kNoPayload;
-      if ((pmask >> ci) & 1u) {
-        if (rec[ci].x == hh[ci]) pl = rec[ci].y;
-        else if (rec[ci].y != kNoPayload) pl = table_probe(ix, hh[ci], bucket_of(hh[ci], ix.nbuckets), 1);
+      for (int ci = 0; ci < R; ++ci)
+        fw[ci] = ((vmask >> ci) & 1u) ? __ldg(ix.filter + filter_word(hh[ci], ix.fshift)) : 0u;
+      // l-mers with a non-ACGT base are not looked up (SRepelHasOddBase)
+      bool any_n = nword != 0;
+      for (int64_t w = nw0 + 32 + lane; w <= nw1; w += 32) {
+        uint64_t m = ld_stream(q.nmask + w);
+        if (w == nw1) m &= ~0ull << (63 - ((st + qlen - 1) & 63));
+        any_n |= m != 0;
       }
-      preg[ci] = pl;
+      if (__any_sync(kFull, any_n)) {
+#pragma unroll
+        for (int ci = 0; ci < R; ++ci) {
+          const int qi = ci * 32 + lane;
+          if (((vmask >> ci) & 1u) &&
+              (SMALL ? kmer_has_n16(reinterpret_cast<const uint32_t*>(q.nmask), st + qi, ix.l)
+                     : kmer_has_n(q.nmask, st + qi, ix.l)))
+            vmask &= ~(1u << ci);
+        }
+      }
+      ulonglong2 rec[R];
+      uint32_t pmask = 0;
+#pragma unroll
+      for (int ci = 0; ci < R; ++ci) {
+        const bool pass = ((vmask >> ci) & 1u) && filter_pass(fw[ci], hh[ci]);
+        pmask |= (uint32_t)pass << ci;
+        rec[ci] = make_ulonglong2(0ull, kNoPayload);
+        if (pass) rec[ci] = __ldcs(ix.table + 2 * (size_t)bucket_of(hh[ci], ix.nbuckets));
+      }
+#pragma unroll
+      for (int ci = 0; ci < R; ++ci) {
+        uint64_t pl = kNoPayload;
+        if ((pmask >> ci) & 1u) {
+          if (rec[ci].x == hh[ci]) pl = rec[ci].y;
+          else if (rec[ci].y != kNoPayload) pl = table_probe(ix, hh[ci], bucket_of(hh[ci], ix.nbuckets), 1);
+        }
+        preg[ci] = pl;
+      }
     }
-  }
-  int total = 0, valid_kmers = __popc(vmask);
+    int lane_cnt = 0;
 #pragma unroll
-  for (int ci = 0; ci < R; ++ci) total += payload_count(preg[ci]);
-  for (int c0 = R * 32; c0 < nk; c0 += 32)
-    total += payload_count(seed_lookup(q, ix, st, c0 + lane, nk, valid_kmers));
-  total = (int)__reduce_add_sync(kFull, (unsigned)total);
-  valid_kmers = (int)__reduce_add_sync(kFull, (unsigned)valid_kmers);
-  const int part = (int)(s % kSeedParts);
-  unsigned long long rel = 0;
-  if (lane == 0) {
-    if (valid_kmers) atomicAdd(n_kmers, (unsigned long long)valid_kmers);
-    rel = total ? atomicAdd(&cursor[part], (unsigned long long)total) : 0ull;
-  }
-  rel = __shfl_sync(kFull, rel, 0);
-  const unsigned long long base = (unsigned long long)part * (unsigned long long)part_cap + rel;
-  if (lane == 0) {
-    off[s] = (int64_t)base;
-    cnt[s] = total;
-  }
-  const int64_t cap = (int64_t)(part + 1) * part_cap;
-  if (total == 0 || (int64_t)(base + total) > cap) {
-    if (lane == 0) nvalid[s] = 0;
-    return;
-  }
-  int64_t w = (int64_t)base;
-  int valid = 0;
+    for (int ci = 0; ci < R; ++ci) lane_cnt += payload_count(preg[ci]);
+    int later = 0, valid_kmers = __popc(vmask);
+    for (int c0 = R * 32; c0 < nk; c0 += 32)
+      later += payload_count(seed_lookup(q, ix, st, c0 + lane, nk, valid_kmers));
+    const int reg_total = (int)__reduce_add_sync(kFull, (unsigned)lane_cnt);
+    const int total = reg_total + (int)__reduce_add_sync(kFull, (unsigned)later);
+    valid_kmers = (int)__reduce_add_sync(kFull, (unsigned)valid_kmers);
+    const int part = (int)(s % kSeedParts);
+    unsigned long long rel = 0;
+    if (lane == 0) {
+      if (valid_kmers) atomicAdd(n_kmers, (unsigned long long)valid_kmers);
+      rel = total ? atomicAdd(&cursor[part], (unsigned long long)total) : 0ull;
+    }
+    rel = __shfl_sync(kFull, rel, 0);
+    const unsigned long long base = (unsigned long long)part * (unsigned long long)part_cap + rel;
+    if (lane == 0) {
+      off[s] = (int64_t)base;
+      cnt[s] = total;
+    }
+    const int64_t cap = (int64_t)(part + 1) * part_cap;
+    if (total == 0 || (int64_t)(base + total) > cap) {
+      if (lane == 0) nvalid[s] = 0;
+      continue;
+    }
+    int valid = 0;
+    bool lane_multi = false;
 #pragma unroll
-  for (int ci = 0; ci < R; ++ci)
-    if (ci * 32 < nk) seed_emit(ix, t, gap, local, qlen, ci * 32 + lane, preg[ci], lane, w, valid, skey, sq);
-  for (int c0 = R * 32; c0 < nk; c0 += 32) {
-    int dummy = 0;
-    const uint64_t pl = seed_lookup(q, ix, st, c0 + lane, nk, dummy);
-    seed_emit(ix, t, gap, local, qlen, c0 + lane, pl, lane, w, valid, skey, sq);
+    for (int ci = 0; ci < R; ++ci) lane_multi |= payload_count(preg[ci]) > 1;
+    if (!__any_sync(kFull, lane_multi)) {
+      // one seed per l-mer at most: l-mer order (chunk, then lane), so that the
+      // seeds of a strand on a single diagonal arrive already sorted
+      const unsigned lt = lanemask_lt();
+      int64_t w = (int64_t)base;
+#pragma unroll
+      for (int ci = 0; ci < R; ++ci) {
+        const unsigned b = __ballot_sync(kFull, preg[ci] != kNoPayload);
+        if (preg[ci] != kNoPayload)
+          seed_put(ix, t, gap, local, qlen, ci * 32 + lane, preg[ci], w + __popc(b & lt), valid, skey, sq);
+        w += __popc(b);
+      }
+    } else {
+      int unused;
+      int64_t w = (int64_t)base + warp_excl_scan(lane_cnt, lane, &unused);
+#pragma unroll
+      for (int ci = 0; ci < R; ++ci)
+        if (preg[ci] != kNoPayload) {
+          seed_put(ix, t, gap, local, qlen, ci * 32 + lane, preg[ci], w, valid, skey, sq);
+          w += payload_count(preg[ci]);
+        }
+    }
+    int64_t w = (int64_t)base + reg_total;
+    for (int c0 = R * 32; c0 < nk; c0 += 32) {
+      int dummy = 0;
+      const uint64_t pl = seed_lookup(q, ix, st, c0 + lane, nk, dummy);
+      const int c = payload_count(pl);
+      int chunk_total;
+      const int e = warp_excl_scan(c, lane, &chunk_total);
+      if (c) seed_put(ix, t, gap, local, qlen, c0 + lane, pl, w + e, valid, skey, sq);
+      w += chunk_total;
+    }
+    valid = (int)__reduce_add_sync(kFull, (unsigned)valid);
+    if (lane == 0) nvalid[s] = valid;
   }
-  valid = (int)__reduce_add_sync(kFull, (unsigned)valid);
-  if (lane == 0) nvalid[s] = valid;
 }
 
 __global__ void k_window_first(const int32_t* __restrict__ nvalid, const int32_t* __restrict__ wstart, int nwin,
@@ -830,31 +863,51 @@ __device__ __forceinline__ void filter_chunk(int c0, int n, uint64_t k, uint32_t
   }
 }
 
+// Seed-sort tiers by a strand's seed count: <= 32 (one warp, registers),
+// <= kWarpSmemCap (one warp, shared memory), <= kCtaSortCap (one CTA, shared
+// memory), longer (one CTA, global memory).  List entries are the strand index
+// with the window-first flag in bit 31.
+constexpr int kSortTiers = 4;
+constexpr int kWarpSmemCap = 256;
+constexpr uint32_t kWinFirstBit = 0x80000000u;
+
 __global__ void k_seed_classify(SeedFilterCtx c, int64_t ns, int32_t* __restrict__ lists,
                                 int32_t* __restrict__ counts) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int n = (i < ns && c.nvalid[i] > 0) ? c.cnt[i] : 0;
-  const int tier = (n <= 0) ? -1 : ((n <= 32) ? 0 : (n <= kCtaSortCap ? 1 : 2));
+  const int tier = (n <= 0) ? -1 : (n <= 32 ? 0 : (n <= kWarpSmemCap ? 1 : (n <= kCtaSortCap ? 2 : 3)));
   const int lane = threadIdx.x & 31;
+  const uint32_t entry = (uint32_t)i | ((tier >= 0 && window_first_strand(i, c)) ? kWinFirstBit : 0u);
 #pragma unroll
-  for (int t = 0; t < 3; ++t) {
+  for (int t = 0; t < kSortTiers; ++t) {
     const unsigned m = __ballot_sync(kFull, tier == t);
     if (!m) continue;
     int base = 0;
     if (lane == __ffs(m) - 1) base = atomicAdd(&counts[t], __popc(m));
     base = __shfl_sync(kFull, base, __ffs(m) - 1);
-    if (tier == t) lists[(int64_t)t * ns + base + __popc(m & lanemask_lt())] = (int32_t)i;
+    if (tier == t) lists[(int64_t)t * ns + base + __popc(m & lanemask_lt())] = (int32_t)entry;
   }
 }
 
-// <= 32 seeds: one warp, sorted in registers and filtered from registers.
+// Compare-exchange of a warp-wide bitonic network step held one element per
+// lane: the lower lane of the pair keeps the smaller element.
+__device__ __forceinline__ void warp_cx(uint64_t& a1, uint32_t& a2, int lane, int partner) {
+  const uint64_t b1 = __shfl_sync(kFull, a1, partner);
+  const uint32_t b2 = __shfl_sync(kFull, a2, partner);
+  const bool b_less = less2(b1, b2, a1, a2);
+  if (lane < partner ? b_less : !b_less && (b1 != a1 || b2 != a2)) { a1 = b1; a2 = b2; }
+}
+
+// <= 32 seeds: one warp sorts in registers (network sized to the count,
+// skipped when the seeds already ascend) and filters from registers.
 __global__ void k_seed_sort_filter_warp(uint64_t* __restrict__ skey, uint32_t* __restrict__ sq, SeedFilterCtx c,
                                         const int32_t* __restrict__ list, const int32_t* __restrict__ count) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int total = *count;
   for (int64_t li = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; li < total; li += nwarps) {
-    const int s = list[li];
+    const uint32_t e = (uint32_t)list[li];
+    const int s = (int)(e & ~kWinFirstBit);
     const int64_t o = c.off[s];
     const int n = c.cnt[s];
     uint64_t a1 = ~0ull;
@@ -863,30 +916,93 @@ __global__ void k_seed_sort_filter_warp(uint64_t* __restrict__ skey, uint32_t* _
       a1 = skey[o + lane];
       a2 = sq[o + lane];
     }
-    for (int size = 2; size <= 32; size <<= 1) {
-      {
-        const int partner = lane ^ (size - 1);
-        const uint64_t b1 = __shfl_sync(kFull, a1, partner);
-        const uint32_t b2 = __shfl_sync(kFull, a2, partner);
-        const bool b_less = less2(b1, b2, a1, a2);
-        if (lane < partner ? b_less : !b_less && (b1 != a1 || b2 != a2)) { a1 = b1; a2 = b2; }
-      }
-      for (int stride = size >> 2; stride > 0; stride >>= 1) {
-        const int partner = lane ^ stride;
-        const uint64_t b1 = __shfl_sync(kFull, a1, partner);
-        const uint32_t b2 = __shfl_sync(kFull, a2, partner);
-        const bool b_less = less2(b1, b2, a1, a2);
-        if (lane < partner ? b_less : !b_less && (b1 != a1 || b2 != a2)) { a1 = b1; a2 = b2; }
+    const uint64_t n1 = __shfl_down_sync(kFull, a1, 1);
+    const uint32_t n2 = __shfl_down_sync(kFull, a2, 1);
+    if (__any_sync(kFull, lane + 1 < n && less2(n1, n2, a1, a2))) {
+      int np = 2;
+      while (np < n) np <<= 1;
+      for (int size = 2; size <= np; size <<= 1) {
+        warp_cx(a1, a2, lane, lane ^ (size - 1));
+        for (int stride = size >> 2; stride > 0; stride >>= 1) warp_cx(a1, a2, lane, lane ^ stride);
       }
     }
     FilterState f;
     f.out = o;
-    filter_chunk(0, c.nvalid[s], a1, a2, window_first_strand(s, c), c.width, c.gap, f, skey, sq);
+    filter_chunk(0, c.nvalid[s], a1, a2, (e & kWinFirstBit) != 0, c.width, c.gap, f, skey, sq);
     if (lane == 0) c.hcnt[s] = (int32_t)(f.out - o);
   }
 }
 
-// <= 2048 seeds: one CTA sorts in shared memory, warp 0 filters from there.
+// Bitonic network over n <= np elements in shared memory, run by one warp.
+__device__ __forceinline__ void warp_smem_network(uint64_t* s1, uint32_t* s2, int n) {
+  const int lane = threadIdx.x & 31;
+  int np = 64;
+  while (np < n) np <<= 1;
+  for (int size = 2; size <= np; size <<= 1) {
+    for (int i = lane; i < np / 2; i += 32) {  // flip stage
+      const int blk = i / (size / 2), r = i % (size / 2);
+      const int a = blk * size + r, b = blk * size + size - 1 - r;
+      if (b < n && less2(s1[b], s2[b], s1[a], s2[a])) {
+        const uint64_t t1 = s1[a]; s1[a] = s1[b]; s1[b] = t1;
+        const uint32_t t2 = s2[a]; s2[a] = s2[b]; s2[b] = t2;
+      }
+    }
+    __syncwarp();
+    for (int stride = size >> 2; stride > 0; stride >>= 1) {
+      for (int i = lane; i < np / 2; i += 32) {
+        const int blk = i / stride, r = i % stride;
+        const int a = blk * 2 * stride + r, b = a + stride;
+        if (b < n && less2(s1[b], s2[b], s1[a], s2[a])) {
+          const uint64_t t1 = s1[a]; s1[a] = s1[b]; s1[b] = t1;
+          const uint32_t t2 = s2[a]; s2[a] = s2[b]; s2[b] = t2;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+constexpr int kWarpSmemThreads = 128;
+
+// 33..kWarpSmemCap seeds: one warp sorts in its own slice of shared memory
+// (skipped when the seeds already ascend) and filters from there.
+__global__ void __launch_bounds__(kWarpSmemThreads) k_seed_sort_filter_warp_smem(
+    uint64_t* __restrict__ skey, uint32_t* __restrict__ sq, SeedFilterCtx c, const int32_t* __restrict__ list,
+    const int32_t* __restrict__ count) {
+  __shared__ uint64_t sh1[kWarpSmemThreads / 32][kWarpSmemCap];
+  __shared__ uint32_t sh2[kWarpSmemThreads / 32][kWarpSmemCap];
+  const int lane = threadIdx.x & 31;
+  uint64_t* s1 = sh1[threadIdx.x >> 5];
+  uint32_t* s2 = sh2[threadIdx.x >> 5];
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int total = *count;
+  for (int64_t li = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; li < total; li += nwarps) {
+    const uint32_t e = (uint32_t)list[li];
+    const int s = (int)(e & ~kWinFirstBit);
+    const int64_t o = c.off[s];
+    const int n = c.cnt[s];
+    for (int i = lane; i < n; i += 32) {
+      s1[i] = skey[o + i];
+      s2[i] = sq[o + i];
+    }
+    __syncwarp();
+    bool unsorted = false;
+    for (int i = lane; i + 1 < n; i += 32) unsorted |= less2(s1[i + 1], s2[i + 1], s1[i], s2[i]);
+    if (__any_sync(kFull, unsorted)) warp_smem_network(s1, s2, n);
+    const int nv = c.nvalid[s];
+    const bool wf = (e & kWinFirstBit) != 0;
+    FilterState f;
+    f.out = o;
+    for (int c0 = 0; c0 < nv; c0 += 32) {
+      const int j = c0 + lane;
+      filter_chunk(c0, nv, j < nv ? s1[j] : 0ull, j < nv ? s2[j] : 0u, wf, c.width, c.gap, f, skey, sq);
+    }
+    if (lane == 0) c.hcnt[s] = (int32_t)(f.out - o);
+    __syncwarp();
+  }
+}
+
+// <= kCtaSortCap seeds: one CTA sorts in shared memory, warp 0 filters from there.
 __global__ void __launch_bounds__(256) k_seed_sort_filter_cta(uint64_t* __restrict__ skey, uint32_t* __restrict__ sq,
                                                               SeedFilterCtx c, const int32_t* __restrict__ list,
                                                               const int32_t* __restrict__ count) {
@@ -894,7 +1010,8 @@ __global__ void __launch_bounds__(256) k_seed_sort_filter_cta(uint64_t* __restri
   __shared__ uint32_t s2[kCtaSortCap];
   const int total = *count;
   for (int li = blockIdx.x; li < total; li += gridDim.x) {
-    const int s = list[li];
+    const uint32_t e = (uint32_t)list[li];
+    const int s = (int)(e & ~kWinFirstBit);
     const int64_t o = c.off[s];
     const int n = c.cnt[s];
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -905,7 +1022,7 @@ __global__ void __launch_bounds__(256) k_seed_sort_filter_cta(uint64_t* __restri
     cta_network<uint32_t, false>(s1, s2, nullptr, n);
     if (threadIdx.x < 32) {
       const int nv = c.nvalid[s];
-      const bool wf = window_first_strand(s, c);
+      const bool wf = (e & kWinFirstBit) != 0;
       FilterState f;
       f.out = o;
       for (int c0 = 0; c0 < nv; c0 += 32) {
@@ -925,13 +1042,14 @@ __global__ void __launch_bounds__(1024) k_seed_sort_filter_global(uint64_t* __re
                                                                   const int32_t* __restrict__ count) {
   const int total = *count;
   for (int li = blockIdx.x; li < total; li += gridDim.x) {
-    const int s = list[li];
+    const uint32_t e = (uint32_t)list[li];
+    const int s = (int)(e & ~kWinFirstBit);
     const int64_t o = c.off[s];
     cta_network<uint32_t, false>(skey + o, sq + o, nullptr, c.cnt[s]);
     __syncthreads();
     if (threadIdx.x < 32) {
       const int nv = c.nvalid[s];
-      const bool wf = window_first_strand(s, c);
+      const bool wf = (e & kWinFirstBit) != 0;
       FilterState f;
       f.out = o;
       for (int c0 = 0; c0 < nv; c0 += 32) {
@@ -1479,6 +1597,7 @@ void seed_fused(const QueryView& q, const IndexView& ix, const TargetView& t, in
                 unsigned long long* cursors, unsigned long long* n_kmers, int64_t* off, int32_t* cnt, int32_t* nvalid,
                 uint64_t* skey, uint32_t* sq, int64_t part_cap, cudaStream_t st) {
   if (q.nstrands <= 0) return;
+  // one warp per strand (one resident wave looping over the strands measured slower)
   const unsigned grid = blocks_for((int64_t)q.nstrands * 32, kSeedFusedThreads);
   if (ix.l <= 16)
     k_seed_fused<true><<<grid, kSeedFusedThreads, 0, st>>>(q, ix, t, gap, local, cursors, n_kmers, off, cnt, nvalid,
@@ -1514,19 +1633,23 @@ void seed_sort_filter(Workspace& ws, uint64_t* skey, uint32_t* sq, const int64_t
                       int width, int gap, int64_t nstrands, int32_t* hcnt, cudaStream_t st) {
   if (nstrands <= 0) return;
   SeedFilterCtx c{off, cnt, nvalid, win_start, n_windows, win_first, width, gap, hcnt};
-  int32_t* lists = ws.get<int32_t>("ssf_lists", 3 * nstrands);
-  int32_t* counts = ws.get<int32_t>("ssf_counts", 3);
-  CLAST_CK(cudaMemsetAsync(counts, 0, 3 * sizeof(int32_t), st));
+  if (nstrands >= (int64_t)kWinFirstBit) throw std::invalid_argument("more than 2^31 strands in one batch");
+  int32_t* lists = ws.get<int32_t>("ssf_lists", kSortTiers * nstrands);
+  int32_t* counts = ws.get<int32_t>("ssf_counts", kSortTiers);
+  CLAST_CK(cudaMemsetAsync(counts, 0, kSortTiers * sizeof(int32_t), st));
   CLAST_CK(cudaMemsetAsync(hcnt, 0, nstrands * sizeof(int32_t), st));
   k_seed_classify<<<blocks_for(nstrands, 256), 256, 0, st>>>(c, nstrands, lists, counts);
   CLAST_LAUNCHED();
   k_seed_sort_filter_warp<<<grid_cap((nstrands * 32 + 255) / 256), 256, 0, st>>>(skey, sq, c, lists, counts);
   CLAST_LAUNCHED();
+  k_seed_sort_filter_warp_smem<<<grid_cap(std::min<int64_t>(nstrands, 65536) * 32 / kWarpSmemThreads + 1),
+                                 kWarpSmemThreads, 0, st>>>(skey, sq, c, lists + nstrands, counts + 1);
+  CLAST_LAUNCHED();
   k_seed_sort_filter_cta<<<grid_cap(nstrands < 4096 ? nstrands : 4096), 256, 0, st>>>(skey, sq, c,
-                                                                                     lists + nstrands, counts + 1);
+                                                                                     lists + 2 * nstrands, counts + 2);
   CLAST_LAUNCHED();
   k_seed_sort_filter_global<<<grid_cap(nstrands < 1024 ? nstrands : 1024), 1024, 0, st>>>(
-      skey, sq, c, lists + 2 * nstrands, counts + 2);
+      skey, sq, c, lists + 3 * nstrands, counts + 3);
   CLAST_LAUNCHED();
 }
 
