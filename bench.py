@@ -41,6 +41,9 @@ import numpy as np  # noqa: E402
 from clast_b200 import api, synth  # noqa: E402
 
 METRIC = "query Mbp/s (bit-exact hits)"
+# DRAM bytes (read + write) per looked-up l-mer of k_seed_fused, from an ncu
+# capture on the half-size medium workload (profiles/k_seed_fused_medium_half.md)
+SEED_DRAM_BYTES_PER_KMER = 13.3
 T_RAM, Q_RAM, T_VRAM, Q_VRAM = 64e6, 64e6, 64e6, 2e6  # common.hpp:12-15, x 1e6 (CHostSetting.cu:133-136)
 
 
@@ -281,9 +284,11 @@ def run_ours(args):
         "bound": "hbm", "achieved": round(seed_gbs, 1), "peak": hbm_peak, "unit": "GB/s",
         "frac": round(seed_gbs / hbm_peak, 4),
         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-        "bytes_per_step": int(seed_bytes), "ms_per_step": round(st["seed_ms"], 3),
+        "bytes_per_launch": int(seed_bytes / max(1, st["seed_launches"])),
+        "ms_per_launch": round(st["seed_ms"] / max(1, st["seed_launches"]), 3),
         "launches_per_step": st["seed_launches"],
-        "traffic": None,
+        "traffic": int(SEED_DRAM_BYTES_PER_KMER * st["query_kmers"] / max(1, st["seed_launches"])),
+        "traffic_source": "ncu DRAM bytes per l-mer on the half-size workload x l-mers per launch",
         "stage_ms_per_step": {k: round(v, 3) for k, v in stages.items()},
         "step_device_ms": round(st["index_ms"] + st["map_ms"], 3),
         "index_ms": round(st["index_ms"], 3), "map_ms": round(st["map_ms"], 3),
