@@ -17,20 +17,25 @@ constexpr uint64_t kDroppedSeed = ~0ull;
 
 // Resident index of one target window: the tables of CDeviceHashTable
 // (CDeviceHashTable.cuh:13-16) reorganised for one-probe lookup.  Every key
-// that keeps at least one entry after the repeat cut is a record {hash of
-// the key, payload} of an open-addressing table of 32-byte buckets (two records,
-// linear probing); payload is the key's only entry (sequence within window
-// << 32 | index within sequence) or, for keys with several entries, kMulti |
-// start << 32 | count into `entries`.  A blocked Bloom filter (3 bits in one
-// 32-bit word per key) answers most absent keys from L2.
+// that keeps at least one entry after the repeat cut is a 16-byte record
+// {code of the key, payload} of a linear-probing table: the code is
+// order_code(key), a bijection of the 2l-bit keys; a key's home record is
+// 2 * floor(code * nbuckets / 4^l), so home records rise with the code, and the
+// records are placed in code order at max(home, previous + 1) (the layout
+// linear probing gives in any insertion order).  Payload: the key's only entry
+// (sequence within window << 32 | index within sequence) or, for keys with
+// several entries, kMulti | start << 32 | count into `entries`.  A blocked
+// Bloom filter (3 bits in one 32-bit word per key) answers most absent keys
+// from L2.
 struct IndexView {
   int l;
-  int fshift;                // filter word = hash >> fshift (fshift >= 32)
+  int fshift;                // filter word = key_hash(code) >> fshift (fshift >= 32)
   const uint32_t* filter;
-  const ulonglong2* table;   // 2 * nbuckets records; payload ~0 = free
-  uint32_t nbuckets;
+  const ulonglong2* table;   // n_records records; payload ~0 = free
+  uint32_t nbuckets;         // home records are 2 * [0, nbuckets)
+  int64_t n_records;         // >= 2 * nbuckets; the last record is always free
   const int2* entries;       // (sequence within window, index within sequence), non-joint only
-  int64_t n_keys;            // records in the table
+  int64_t n_keys;            // records in use
 };
 // Target window for the DP and the corner filter.
 struct TargetView {
@@ -109,13 +114,20 @@ __device__ __forceinline__ bool kmer_at(const uint64_t* packed, const uint64_t* 
 constexpr uint64_t kMulti = 1ull << 63;
 constexpr uint64_t kNoPayload = ~0ull;  // also the payload of an empty record
 
-// Hash of an l-mer key: an xorshift then a multiply by an odd constant
-// (Fibonacci hashing), both invertible, so distinct keys have distinct hashes
-// and the table stores and compares hashes instead of keys.  The top bits
-// select the 32-bit filter word and the bucket, bits 16..30 the three filter
-// bits.
-__host__ __device__ __forceinline__ uint64_t key_hash(uint64_t key) {
-  return (key ^ (key >> 31)) * 0x9E3779B97F4A7C15ull;
+// Code of an l-mer key: the key times an odd constant modulo 4^l, a
+// bijection of the 2l-bit keys whose high bits depend on every base.
+__host__ __device__ __forceinline__ uint64_t order_code(uint64_t key, int l) {
+  return (key * 0xD6E8FEB86659FD93ull) & ((1ull << (2 * l)) - 1);
+}
+// Home record of a code: 2 * floor(code * nbuckets / 4^l).
+__device__ __forceinline__ int64_t record_home(uint64_t code, int l, uint32_t nbuckets) {
+  return 2 * (int64_t)__umul64hi(code << (64 - 2 * l), (uint64_t)nbuckets);
+}
+// Filter hash of a code: an xorshift then a multiply by an odd constant
+// (Fibonacci hashing).  The top bits select the 32-bit filter word, bits
+// 16..30 the three filter bits.
+__host__ __device__ __forceinline__ uint64_t key_hash(uint64_t code) {
+  return (code ^ (code >> 31)) * 0x9E3779B97F4A7C15ull;
 }
 // fshift >= 32: filter word = (h >> 32) >> (fshift - 32)
 __host__ __device__ __forceinline__ uint32_t filter_word(uint64_t h, int fshift) {
@@ -129,26 +141,19 @@ __device__ __forceinline__ bool filter_pass(uint32_t word, uint64_t h) {
   const uint32_t m = filter_mask(h);
   return (word & m) == m;
 }
-__device__ __forceinline__ uint32_t bucket_of(uint64_t h, uint32_t nbuckets) {
-  return __umulhi((uint32_t)(h >> 32), nbuckets);
-}
 // Entries of a payload (0 for none).
 __host__ __device__ __forceinline__ int payload_count(uint64_t p) {
   return p == kNoPayload ? 0 : ((p & kMulti) ? (int)(uint32_t)p : 1);
 }
 
-// Linear probing from record j of bucket b for the key of hash h.  Records
-// are {hash, payload}; a free record has payload kNoPayload (no real payload
-// has that value), so an absent key ends at the first free record.  Loads are
+// Linear probing from record r for the key of code c.  A free record has
+// payload kNoPayload (no real payload has that value), so an absent key ends
+// at the first free record; the table's last record is always free.  Loads are
 // evict-first so that the filter stays in L2.
-__device__ __forceinline__ uint64_t table_probe(const IndexView& ix, uint64_t h, uint32_t b, int j) {
-  for (uint32_t probe = 0; probe <= ix.nbuckets; ++probe) {
-    for (; j < 2; ++j) {
-      const ulonglong2 r = __ldcs(ix.table + 2 * (size_t)b + j);
-      if (r.x == h || r.y == kNoPayload) return r.y;
-    }
-    j = 0;
-    b = (b + 1 == ix.nbuckets) ? 0 : b + 1;
+__device__ __forceinline__ uint64_t table_probe(const IndexView& ix, uint64_t c, int64_t r) {
+  for (; r < ix.n_records; ++r) {
+    const ulonglong2 rec = __ldcs(ix.table + r);
+    if (rec.x == c || rec.y == kNoPayload) return rec.y;
   }
   return kNoPayload;
 }
@@ -156,9 +161,10 @@ __device__ __forceinline__ uint64_t table_probe(const IndexView& ix, uint64_t h,
 // Payload of key, or kNoPayload (krnlBinarySearch.cu:3-33 followed by the
 // bucket lookup of writeSeedList).
 __device__ __forceinline__ uint64_t index_find(const IndexView& ix, uint64_t key) {
-  const uint64_t h = key_hash(key);
+  const uint64_t c = order_code(key, ix.l);
+  const uint64_t h = key_hash(c);
   if (!filter_pass(__ldg(ix.filter + filter_word(h, ix.fshift)), h)) return kNoPayload;
-  return table_probe(ix, h, bucket_of(h, ix.nbuckets), 0);
+  return table_probe(ix, c, record_home(c, ix.l, ix.nbuckets));
 }
 
 }  // namespace clast

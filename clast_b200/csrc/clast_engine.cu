@@ -187,6 +187,7 @@ struct clast_index {
   DevArray<int2> entries;
   int64_t n_unique = 0, n_keys = 0, n_entries = 0;
   uint32_t nbuckets = 1;
+  int64_t n_records = 2;
   int fshift = 63;
 
   IndexView view() const {
@@ -196,6 +197,7 @@ struct clast_index {
     v.filter = filter.p;
     v.table = table.p;
     v.nbuckets = nbuckets;
+    v.n_records = n_records;
     v.entries = entries.p;
     v.n_keys = n_keys;
     return v;
@@ -259,30 +261,42 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix) {
   int32_t* ustart = ws.get<int32_t>("ix_ustart", nu);
   int32_t* ucnt = ws.get<int32_t>("ix_ucnt", nu);
   index_buckets(ufirst, kpos, nu, ustart, ucnt, st);
-  // One record per unique key is an upper bound on the keys that keep entries;
-  // buckets of two records at most 70% full.
-  const int64_t nb = std::max<int64_t>(1, (nu * 10 + 13) / 14);
+  // Hash table: buckets of two records, at most half of the records used (one
+  // record per unique key is an upper bound on the keys that keep entries):
+  // 84 % of the keys then sit in their home bucket
+  const int64_t nb = std::max<int64_t>(1, nu);
   if (nb >= (int64_t)UINT32_MAX) throw std::invalid_argument("window has too many distinct l-mers");
   ix->nbuckets = (uint32_t)nb;
-  ix->table.alloc((size_t)2 * nb);
-  CLAST_CK(cudaMemsetAsync(ix->table.p, 0xff, (size_t)2 * nb * sizeof(ulonglong2), st));
+  int32_t* kept = ws.get<int32_t>("ix_kept", nu);
+  int64_t* rank = ws.get<int64_t>("ix_rank", nu + 1);
+  table_kept(ucnt, nu, kept, st);
+  scan_i32(ws, kept, nu, rank, st);
+  const int64_t nk = read_scalar(rank + nu, st);
+  int64_t* slack = ws.get<int64_t>("ix_slack", nk);
+  int64_t* run_max = ws.get<int64_t>("ix_runmax", nk);
+  table_slack(ukeys, ucnt, rank, nu, l, ix->nbuckets, slack, st);
+  maxscan_i64(ws, slack, nk, run_max, st);
+  // the last kept code sits at nk - 1 + run_max[nk - 1]; one free record after it
+  const int64_t last = nk > 0 ? nk - 1 + read_scalar(run_max + nk - 1, st) : -1;
+  ix->n_records = std::max<int64_t>(2 * nb, last + 2);
+  ix->table.alloc((size_t)ix->n_records);
+  CLAST_CK(cudaMemsetAsync(ix->table.p, 0xff, (size_t)ix->n_records * sizeof(ulonglong2), st));
   // Bloom filter: about 24 bits per key, between 2^12 and 2^F bits; F = 28
   // (32 MB, L2-resident next to the streams that pass through L2 while
   // seeding) unless CLAST_FILTER_BITS says otherwise (16..32)
   int fbits = 28;
   if (const char* e = std::getenv("CLAST_FILTER_BITS")) fbits = std::max(16, std::min(32, std::atoi(e)));
   int bits = 12;
-  while (bits < fbits && (1ll << bits) < nu * 24) ++bits;
+  while (bits < fbits && (1ll << bits) < nk * 24) ++bits;
   ix->fshift = 64 - (bits - 5);
   ix->filter.alloc((size_t)1 << (bits - 5));
   CLAST_CK(cudaMemsetAsync(ix->filter.p, 0, ((size_t)1 << (bits - 5)) * sizeof(uint32_t), st));
   unsigned long long* failed = reinterpret_cast<unsigned long long*>(ws.get<int64_t>("ix_failed", 1));
   CLAST_CK(cudaMemsetAsync(failed, 0, sizeof(unsigned long long), st));
-  index_table(ukeys, ustart, ucnt, ix->entries.p, nu, ix->table.p, ix->nbuckets, ix->filter.p, ix->fshift, failed,
-              st);
-  const int64_t nfail = read_scalar(reinterpret_cast<int64_t*>(failed), st);
-  if (nfail != 0) throw std::runtime_error("index table overflow");
-  ix->n_keys = nu;
+  table_place(ukeys, ustart, ucnt, ix->entries.p, rank, run_max, nu, ix->table.p, ix->n_records, ix->filter.p,
+              ix->fshift, failed, st);
+  if (read_scalar(reinterpret_cast<int64_t*>(failed), st) != 0) throw std::runtime_error("index table overflow");
+  ix->n_keys = nk;
 }
 
 // Index of a window whose padded base array is already on the device.

@@ -210,8 +210,7 @@ __global__ void k_sample_keys(const uint64_t* __restrict__ packed, const uint64_
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ns) return;
   uint64_t key;
-  if (!kmer_at(packed, nmask, j * stride, l, key)) key = 1ull << (2 * l);
-  keys[j] = key;
+  keys[j] = kmer_at(packed, nmask, j * stride, l, key) ? order_code(key, l) : (1ull << (2 * l));
   vals[j] = (int32_t)j;
 }
 
@@ -346,19 +345,35 @@ __global__ void k_index_buckets(const int64_t* __restrict__ ufirst, const int64_
   ucnt[k] = (int32_t)(b - a);
 }
 
-// Inserts every key that keeps entries into the open-addressing table and
-// its three bits into the blocked Bloom filter.  Placement within a probe
-// chain depends on thread timing; lookups match the exact key, so results do
-// not.
-__global__ void k_index_table(const uint64_t* __restrict__ ukeys, const int32_t* __restrict__ ustart,
-                              const int32_t* __restrict__ ucnt, const int2* __restrict__ entries, int64_t nu,
-                              ulonglong2* __restrict__ table, uint32_t nbuckets, uint32_t* __restrict__ filter,
+// ---- hash table of the index, placed without atomics ----
+// The unique codes arrive ascending, so their home records do too; with
+// r = rank among the kept codes, linear probing puts code r at
+// max(home_r, pos_{r-1} + 1) = r + max_{j <= r}(home_j - j).
+
+__global__ void k_table_kept(const int32_t* __restrict__ ucnt, int64_t nu, int32_t* __restrict__ kept) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nu) kept[k] = ucnt[k] > 0 ? 1 : 0;  // 0: removed by the repeat cut, or joints only
+}
+
+__global__ void k_table_slack(const uint64_t* __restrict__ ucode, const int32_t* __restrict__ ucnt,
+                              const int64_t* __restrict__ rank, int64_t nu, int l, uint32_t nbuckets,
+                              int64_t* __restrict__ slack) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nu || ucnt[k] <= 0) return;
+  slack[rank[k]] = record_home(ucode[k], l, nbuckets) - rank[k];
+}
+
+__global__ void k_table_place(const uint64_t* __restrict__ ucode, const int32_t* __restrict__ ustart,
+                              const int32_t* __restrict__ ucnt, const int2* __restrict__ entries,
+                              const int64_t* __restrict__ rank, const int64_t* __restrict__ run_max, int64_t nu,
+                              ulonglong2* __restrict__ table, int64_t n_records, uint32_t* __restrict__ filter,
                               int fshift, unsigned long long* __restrict__ failed) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nu) return;
   const int c = ucnt[k];
-  if (c <= 0) return;  // removed by the repeat cut, or joints only
-  const uint64_t h = key_hash(ukeys[k]);
+  if (c <= 0) return;
+  const uint64_t code = ucode[k];
+  const uint64_t h = key_hash(code);
   atomicOr(filter + filter_word(h, fshift), filter_mask(h));
   uint64_t payload;
   if (c == 1) {
@@ -367,21 +382,59 @@ __global__ void k_index_table(const uint64_t* __restrict__ ukeys, const int32_t*
   } else {
     payload = kMulti | ((uint64_t)(uint32_t)ustart[k] << 32) | (uint32_t)c;
   }
-  // a record is claimed through its payload (free = kNoPayload); the hash is
-  // written after the claim, before any lookup kernel runs
-  uint32_t b = bucket_of(h, nbuckets);
-  for (uint32_t probe = 0; probe < nbuckets; ++probe) {
-    for (int j = 0; j < 2; ++j) {
-      ulonglong2* r = table + 2 * (size_t)b + j;
-      if (atomicCAS(reinterpret_cast<unsigned long long*>(&r->y), (unsigned long long)kNoPayload,
-                    (unsigned long long)payload) == (unsigned long long)kNoPayload) {
-        r->x = h;
-        return;
-      }
-    }
-    b = (b + 1 == nbuckets) ? 0 : b + 1;
+  const int64_t r = rank[k];
+  const int64_t pos = r + run_max[r];
+  if (pos >= 0 && pos < n_records) table[pos] = make_ulonglong2(code, payload);
+  else atomicAdd(failed, 1ull);  // unreachable: positions rise to the last one, which the table holds
+}
+
+// ---- inclusive running maximum (int64) ----
+__global__ void __launch_bounds__(kScanThreads) k_maxscan_tiles(const int64_t* __restrict__ in, int64_t n,
+                                                                int64_t* __restrict__ out,
+                                                                int64_t* __restrict__ tile_max) {
+  __shared__ int64_t warp_max[kScanThreads / 32];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int64_t v[kScanItems];
+  int64_t m = INT64_MIN;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int64_t idx = base + i;
+    v[i] = (idx < n) ? in[idx] : INT64_MIN;
+    m = v[i] > m ? v[i] : m;
   }
-  atomicAdd(failed, 1ull);  // unreachable: the table always has free records
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t incl = m;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o && y > incl) incl = y;
+  }
+  if (lane == 31) warp_max[warp] = incl;
+  __syncthreads();
+  int64_t wpre = INT64_MIN, tot = INT64_MIN;
+#pragma unroll
+  for (int w = 0; w < kScanThreads / 32; ++w) {
+    const int64_t t = warp_max[w];
+    if (w < warp && t > wpre) wpre = t;
+    if (t > tot) tot = t;
+  }
+  int64_t run = __shfl_up_sync(kFull, incl, 1);
+  if (lane == 0) run = INT64_MIN;
+  if (wpre > run) run = wpre;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int64_t idx = base + i;
+    if (v[i] > run) run = v[i];
+    if (idx < n) out[idx] = run;
+  }
+  if (threadIdx.x == 0) tile_max[blockIdx.x] = tot;
+}
+
+__global__ void k_maxscan_apply(int64_t* __restrict__ out, int64_t n, const int64_t* __restrict__ tile_run) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t t = i / kScanTile;
+  if (t > 0 && tile_run[t - 1] > out[i]) out[i] = tile_run[t - 1];
 }
 
 // ------------------------------------------------------------------------
@@ -484,13 +537,13 @@ __global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, I
         uint64_t key = 0;
         if (v) key = SMALL ? kmer_key16(reinterpret_cast<const uint32_t*>(q.packed), st + qi, ix.l)
                            : kmer_key(q.packed, st + qi, ix.l);
-        hh[ci] = key_hash(key);
+        hh[ci] = order_code(key, ix.l);
         vmask |= (uint32_t)v << ci;
       }
       uint32_t fw[R];
 #pragma unroll
       for (int ci = 0; ci < R; ++ci)
-        fw[ci] = ((vmask >> ci) & 1u) ? __ldg(ix.filter + filter_word(hh[ci], ix.fshift)) : 0u;
+        fw[ci] = ((vmask >> ci) & 1u) ? __ldg(ix.filter + filter_word(key_hash(hh[ci]), ix.fshift)) : 0u;
       // l-mers with a non-ACGT base are not looked up (SRepelHasOddBase)
       bool any_n = nword != 0;
       for (int64_t w = nw0 + 32 + lane; w <= nw1; w += 32) {
@@ -512,19 +565,33 @@ __global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, I
       uint32_t pmask = 0;
 #pragma unroll
       for (int ci = 0; ci < R; ++ci) {
-        const bool pass = ((vmask >> ci) & 1u) && filter_pass(fw[ci], hh[ci]);
+        const bool pass = ((vmask >> ci) & 1u) && filter_pass(fw[ci], key_hash(hh[ci]));
         pmask |= (uint32_t)pass << ci;
         rec[ci] = make_ulonglong2(0ull, kNoPayload);
-        if (pass) rec[ci] = __ldcs(ix.table + 2 * (size_t)bucket_of(hh[ci], ix.nbuckets));
+        if (pass) rec[ci] = __ldcs(ix.table + record_home(hh[ci], ix.l, ix.nbuckets));
       }
+      // resolve from the home records; the keys displaced further read the
+      // next record (the home bucket's second, same 32-byte sector) together
+      uint32_t more = 0;
 #pragma unroll
       for (int ci = 0; ci < R; ++ci) {
         uint64_t pl = kNoPayload;
         if ((pmask >> ci) & 1u) {
           if (rec[ci].x == hh[ci]) pl = rec[ci].y;
-          else if (rec[ci].y != kNoPayload) pl = table_probe(ix, hh[ci], bucket_of(hh[ci], ix.nbuckets), 1);
+          else if (rec[ci].y != kNoPayload) more |= 1u << ci;
         }
         preg[ci] = pl;
+      }
+      if (__any_sync(kFull, more != 0)) {
+#pragma unroll
+        for (int ci = 0; ci < R; ++ci)
+          if ((more >> ci) & 1u) rec[ci] = __ldcs(ix.table + record_home(hh[ci], ix.l, ix.nbuckets) + 1);
+#pragma unroll
+        for (int ci = 0; ci < R; ++ci)
+          if ((more >> ci) & 1u) {
+            if (rec[ci].x == hh[ci] || rec[ci].y == kNoPayload) preg[ci] = rec[ci].y;
+            else preg[ci] = table_probe(ix, hh[ci], record_home(hh[ci], ix.l, ix.nbuckets) + 2);
+          }
       }
     }
     int lane_cnt = 0;
@@ -1608,12 +1675,40 @@ void seed_fused(const QueryView& q, const IndexView& ix, const TargetView& t, in
   CLAST_LAUNCHED();
 }
 
-void index_table(const uint64_t* ukeys, const int32_t* ustart, const int32_t* ucnt, const int2* entries,
-                 int64_t n_unique, ulonglong2* table, uint32_t nbuckets, uint32_t* filter, int fshift,
-                 unsigned long long* failed, cudaStream_t st) {
+void maxscan_i64(Workspace& ws, const int64_t* in, int64_t n, int64_t* out, cudaStream_t st, int level) {
+  if (n <= 0) return;
+  const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+  const std::string tag = "maxscan" + std::to_string(level);
+  int64_t* tmax = ws.get<int64_t>(tag + "m", tiles);
+  k_maxscan_tiles<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, out, tmax);
+  CLAST_LAUNCHED();
+  if (tiles > 1) {
+    int64_t* trun = ws.get<int64_t>(tag + "r", tiles);
+    maxscan_i64(ws, tmax, tiles, trun, st, level + 1);
+    k_maxscan_apply<<<blocks_for(n, 256), 256, 0, st>>>(out, n, trun);
+    CLAST_LAUNCHED();
+  }
+}
+
+void table_kept(const int32_t* ucnt, int64_t n_unique, int32_t* kept, cudaStream_t st) {
   if (n_unique <= 0) return;
-  k_index_table<<<blocks_for(n_unique, 256), 256, 0, st>>>(ukeys, ustart, ucnt, entries, n_unique, table, nbuckets,
-                                                            filter, fshift, failed);
+  k_table_kept<<<blocks_for(n_unique, 256), 256, 0, st>>>(ucnt, n_unique, kept);
+  CLAST_LAUNCHED();
+}
+
+void table_slack(const uint64_t* ucode, const int32_t* ucnt, const int64_t* rank, int64_t n_unique, int l,
+                 uint32_t nbuckets, int64_t* slack, cudaStream_t st) {
+  if (n_unique <= 0) return;
+  k_table_slack<<<blocks_for(n_unique, 256), 256, 0, st>>>(ucode, ucnt, rank, n_unique, l, nbuckets, slack);
+  CLAST_LAUNCHED();
+}
+
+void table_place(const uint64_t* ucode, const int32_t* ustart, const int32_t* ucnt, const int2* entries,
+                 const int64_t* rank, const int64_t* run_max, int64_t n_unique, ulonglong2* table, int64_t n_records,
+                 uint32_t* filter, int fshift, unsigned long long* failed, cudaStream_t st) {
+  if (n_unique <= 0) return;
+  k_table_place<<<blocks_for(n_unique, 256), 256, 0, st>>>(ucode, ustart, ucnt, entries, rank, run_max, n_unique,
+                                                            table, n_records, filter, fshift, failed);
   CLAST_LAUNCHED();
 }
 

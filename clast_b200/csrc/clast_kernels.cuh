@@ -48,14 +48,19 @@ void index_entries(const int32_t* keep, const int64_t* kpos, const int2* resolve
                    int2* entries, cudaStream_t st);
 void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n_unique, int32_t* ustart,
                    int32_t* ucnt, cudaStream_t st);
-// Open-addressing table of every key with entries (payload: its only entry,
-// or kMulti | start << 32 | count) and its blocked Bloom filter words
-// (2^(64 - fshift) 32-bit words, zeroed by the caller; table records set to ~0).
-// *failed counts keys that found no free record (none when the table has
-// more records than keys).
-void index_table(const uint64_t* ukeys, const int32_t* ustart, const int32_t* ucnt, const int2* entries,
-                 int64_t n_unique, ulonglong2* table, uint32_t nbuckets, uint32_t* filter, int fshift,
-                 unsigned long long* failed, cudaStream_t st);
+// Hash table of the index without atomics (layout: IndexView).  kept[k] =
+// whether unique code k keeps entries; rank = exclusive scan of kept;
+// slack[rank] = home - rank of every kept code; run_max = running maximum of
+// slack; table_place writes every kept code's record at rank + run_max[rank]
+// and sets its filter bits (filter zeroed, table records set to ~0 by the
+// caller); *failed counts records that would fall outside the table (none).
+void table_kept(const int32_t* ucnt, int64_t n_unique, int32_t* kept, cudaStream_t st);
+void table_slack(const uint64_t* ucode, const int32_t* ucnt, const int64_t* rank, int64_t n_unique, int l,
+                 uint32_t nbuckets, int64_t* slack, cudaStream_t st);
+void maxscan_i64(Workspace& ws, const int64_t* in, int64_t n, int64_t* out, cudaStream_t st, int level = 0);
+void table_place(const uint64_t* ucode, const int32_t* ustart, const int32_t* ucnt, const int2* entries,
+                 const int64_t* rank, const int64_t* run_max, int64_t n_unique, ulonglong2* table, int64_t n_records,
+                 uint32_t* filter, int fshift, unsigned long long* failed, cudaStream_t st);
 
 // ---- seeds (CDeviceHitList_createRawSeedList.cu, _deleteSeeds*.cu, _sortSeeds.cu) ----
 // One-pass seeding (lookups once): off/cnt/nvalid per strand, seeds in skey/sq,
