@@ -401,8 +401,8 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   int32_t* len32 = ws.get<int32_t>("s_len32", ns);
   int32_t* nvalid = ws.get<int32_t>("s_nvalid", ns);
   const int parts = seed_parts();
-  // k-mers, DP cells, then one seed cursor per partition
-  unsigned long long* counters = ws.get<unsigned long long>("s_counters", 2 + parts);
+  // [1] DP cells, then one seed cursor and one l-mer count per partition
+  unsigned long long* counters = ws.get<unsigned long long>("s_counters", 2 + 2 * parts);
   StageTimer& tm = c->timer;
   int64_t part_cap = std::max<int64_t>(c->seed_hint, qb.n / 16 + (1 << 20)) / parts + 1;
   int64_t S = 0;
@@ -411,29 +411,33 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   for (int attempt = 0; attempt < 2; ++attempt) {
     skey = ws.get<uint64_t>("s_key", (size_t)part_cap * parts);
     sq = ws.get<uint32_t>("s_q", (size_t)part_cap * parts);
-    CLAST_CK(cudaMemsetAsync(counters, 0, (2 + parts) * sizeof(unsigned long long), st));
+    CLAST_CK(cudaMemsetAsync(counters, 0, (2 + 2 * parts) * sizeof(unsigned long long), st));
     tm.begin(st);
-    seed_fused(q, iv, tv, p->gap, p->local, counters + 2, counters, off, len32, nvalid, skey, sq, part_cap, st);
+    seed_fused(q, iv, tv, p->gap, p->local, counters + 2, counters + 2 + parts, off, len32, nvalid, skey, sq,
+               part_cap, st);
     tm.end(StageTimer::SEED, st);
-    unsigned long long cur[64];
-    CLAST_CK(cudaMemcpyAsync(cur, counters + 2, parts * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    unsigned long long cur[128];
+    CLAST_CK(cudaMemcpyAsync(cur, counters + 2, 2 * parts * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     CLAST_CK(cudaStreamSynchronize(st));
     S = 0;
-    int64_t most = 0;
+    int64_t most = 0, kmers = 0;
     for (int i = 0; i < parts; ++i) {
       S += (int64_t)cur[i];
       most = std::max<int64_t>(most, (int64_t)cur[i]);
+      kmers += (int64_t)cur[parts + i];
     }
-    if (most <= part_cap) break;
+    if (most <= part_cap) {
+      c->stats.query_kmers += kmers;
+      break;
+    }
     part_cap = most;  // strands past a full partition wrote nothing: run again
   }
   c->seed_hint = std::max<int64_t>(c->seed_hint, S + S / 4);
   auto add_counters = [&]() {
-    unsigned long long h[2];
-    CLAST_CK(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st));
+    unsigned long long cells = 0;
+    CLAST_CK(cudaMemcpyAsync(&cells, counters + 1, sizeof(cells), cudaMemcpyDeviceToHost, st));
     CLAST_CK(cudaStreamSynchronize(st));
-    c->stats.query_kmers += (int64_t)h[0];
-    c->stats.dp_cells += (int64_t)h[1];
+    c->stats.dp_cells += (int64_t)cells;
     tm.flush();
   };
   c->stats.seeds += S;
@@ -1056,7 +1060,7 @@ size_t fixed_scratch_bytes(int64_t n, int64_t ns, int parts) {
   auto r = [](size_t b) { return ((b ? b : 1) + 255) & ~size_t(255); };
   const size_t nb = (size_t)n, s = (size_t)ns;
   return r(nb + 2 * kPad) + r(8 * s) + r(4 * s) + r(4 * s) + r(8) + r(8 * (nb / 32 + 4)) + r(8 * (nb / 64 + 4)) +
-         r(8 * (s + 1)) + r(4 * s) + r(4 * s) + r(8 * (2 + (size_t)parts)) + r(4 * s) + r(8 * (s + 1)) +
+         r(8 * (s + 1)) + r(4 * s) + r(4 * s) + r(8 * (2 + 2 * (size_t)parts)) + r(4 * s) + r(8 * (s + 1)) +
          r(16 * s) + (64 << 10);
 }
 
@@ -1156,7 +1160,7 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
     int64_t* off = ws.get<int64_t>("s_off", ns + 1);
     int32_t* len32 = ws.get<int32_t>("s_len32", ns);
     int32_t* nvalid = ws.get<int32_t>("s_nvalid", ns);
-    unsigned long long* counters = ws.get<unsigned long long>("s_counters", 2 + parts);
+    unsigned long long* counters = ws.get<unsigned long long>("s_counters", 2 + 2 * parts);
     // the seed partitions take at most half of the scratch still free
     const size_t mark = ws.arena_used;
     const int64_t fit = (int64_t)((ws.arena_cap - mark) / 2 / (12 * (size_t)parts)) - 256;
@@ -1168,8 +1172,9 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
     for (int attempt = 0; attempt < 2; ++attempt) {
       skey = ws.get<uint64_t>("s_key", (size_t)part_cap * parts);
       sq = ws.get<uint32_t>("s_q", (size_t)part_cap * parts);
-      CLAST_CK(cudaMemsetAsync(counters, 0, (2 + parts) * sizeof(unsigned long long), st));
-      seed_fused(q, iv, tv, p->gap, p->local, counters + 2, counters, off, len32, nvalid, skey, sq, part_cap, st);
+      CLAST_CK(cudaMemsetAsync(counters, 0, (2 + 2 * parts) * sizeof(unsigned long long), st));
+      seed_fused(q, iv, tv, p->gap, p->local, counters + 2, counters + 2 + parts, off, len32, nvalid, skey, sq,
+                 part_cap, st);
       unsigned long long cur[64];
       CLAST_CK(cudaMemcpyAsync(cur, counters + 2, parts * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
       CLAST_CK(cudaStreamSynchronize(st));

@@ -440,25 +440,100 @@ __global__ void k_maxscan_apply(int64_t* __restrict__ out, int64_t n, const int6
 // ------------------------------------------------------------------------
 // seeds
 // ------------------------------------------------------------------------
-// Seeding in one pass, one warp per strand: every l-mer is looked up once; the
-// first kSeedRegChunks*32 results stay in registers (longer strands look the
-// rest up again in the second phase).  The lookups of those chunks are issued
-// together, stage by stage (query words, filter words, first table records),
-// so one strand waits for about one latency of each level instead of one per
-// chunk.  The strand's seeds get one contiguous range from an atomic cursor; if
-// the range would pass `cap`, nothing is written and the host reruns with a
-// larger buffer (the cursor then holds the exact total).
-constexpr int kSeedRegChunks = 5;
+// Seeding in one pass, one warp per strand.  The strand's l-mers go in rounds
+// of 32 * kSeedPerLane; in a round lane L takes the kSeedPerLane consecutive
+// l-mers from L * kSeedPerLane, so it reads their 2-bit words once and shifts
+// each key out of them.  The lookups of a round are issued together, level by
+// level (2-bit words → filter words → home records → second records), so a
+// strand waits about one latency per level.  Round 0's results stay in
+// registers for the write pass (one round covers 160 l-mers: a 164 bp strand);
+// later rounds are looked up again when written.  The strand's seeds get one
+// contiguous range from an atomic cursor; if the range would pass `cap`,
+// nothing is written and the host reruns with a larger buffer (the cursor then
+// holds the exact total).  Seeds are written in l-mer order, so the seeds of a
+// strand on one diagonal arrive already sorted.
+constexpr int kSeedPerLane = 5;
+constexpr int kSeedRound = 32 * kSeedPerLane;
 constexpr int kSeedParts = 32;
 
-__device__ __forceinline__ uint64_t seed_lookup(const QueryView& q, const IndexView& ix, int64_t st, int qi,
-                                                int nk, int& valid) {
-  uint64_t key;
-  if (qi < nk && kmer_at(q.packed, q.nmask, st + qi, ix.l, key)) {
-    ++valid;
-    return index_find(ix, key);
+// Payloads of the l-mers qi = r0 + lane * P + i (i < P) of a strand; invalid or
+// absent ones get kNoPayload.  Returns the number of valid l-mers.
+template <bool SMALL>
+__device__ __forceinline__ int round_lookup(const QueryView& q, const IndexView& ix, int64_t st, int nk, int r0,
+                                            int lane, bool any_n, uint64_t (&pl)[kSeedPerLane]) {
+  constexpr int P = kSeedPerLane;
+  const int q0 = r0 + lane * P;
+  const int nv = max(0, min(P, nk - q0));  // valid l-mer slots of this lane
+  uint64_t code[P];
+  uint32_t vmask = 0;
+  if (nv > 0) {
+    const int64_t f = st + q0;
+    if (SMALL) {
+      // the P keys lie in 16-base units j0 .. j0 + 2 (unit j = 32-bit element j ^ 1)
+      const uint32_t* p32 = reinterpret_cast<const uint32_t*>(q.packed);
+      const int64_t j0 = f >> 4;
+      const uint32_t u0 = __ldcs(p32 + (j0 ^ 1)), u1 = __ldcs(p32 + ((j0 + 1) ^ 1)),
+                     u2 = __ldcs(p32 + ((j0 + 2) ^ 1));
+      const int o = 2 * (int)(f & 15);
+      const uint32_t mask = (2 * ix.l == 32) ? ~0u : ((1u << (2 * ix.l)) - 1);
+#pragma unroll
+      for (int i = 0; i < P; ++i) {
+        const int bo = o + 2 * i;
+        const uint32_t x = bo < 32 ? __funnelshift_l(u1, u0, bo) : __funnelshift_l(u2, u1, bo - 32);
+        const uint32_t key = x >> (32 - 2 * ix.l);
+        code[i] = (uint32_t)(key * (uint32_t)0x6659FD93u) & mask;  // order_code for l <= 16
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < P; ++i) code[i] = i < nv ? order_code(kmer_key(q.packed, f + i, ix.l), ix.l) : 0ull;
+    }
+    vmask = (1u << nv) - 1;
+    // l-mers with a non-ACGT base are not looked up (SRepelHasOddBase)
+    if (any_n) {
+#pragma unroll
+      for (int i = 0; i < P; ++i)
+        if (((vmask >> i) & 1u) &&
+            (SMALL ? kmer_has_n16(reinterpret_cast<const uint32_t*>(q.nmask), f + i, ix.l)
+                   : kmer_has_n(q.nmask, f + i, ix.l)))
+          vmask &= ~(1u << i);
+    }
   }
-  return kNoPayload;
+  uint32_t fw[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i)
+    fw[i] = ((vmask >> i) & 1u) ? __ldg(ix.filter + filter_word(key_hash(code[i]), ix.fshift)) : 0u;
+  ulonglong2 rec[P];
+  uint32_t pmask = 0;
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    const bool pass = ((vmask >> i) & 1u) && filter_pass(fw[i], key_hash(code[i]));
+    pmask |= (uint32_t)pass << i;
+    rec[i] = make_ulonglong2(0ull, kNoPayload);
+    if (pass) rec[i] = __ldcs(ix.table + record_home(code[i], ix.l, ix.nbuckets));
+  }
+  // resolve from the home records; the keys displaced further read the next
+  // record (the home bucket's second, same 32-byte sector) together
+  uint32_t more = 0;
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    pl[i] = kNoPayload;
+    if ((pmask >> i) & 1u) {
+      if (rec[i].x == code[i]) pl[i] = rec[i].y;
+      else if (rec[i].y != kNoPayload) more |= 1u << i;
+    }
+  }
+  if (__any_sync(kFull, more != 0)) {
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+      if ((more >> i) & 1u) rec[i] = __ldcs(ix.table + record_home(code[i], ix.l, ix.nbuckets) + 1);
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+      if ((more >> i) & 1u) {
+        if (rec[i].x == code[i] || rec[i].y == kNoPayload) pl[i] = rec[i].y;
+        else pl[i] = table_probe(ix, code[i], record_home(code[i], ix.l, ix.nbuckets) + 2);
+      }
+  }
+  return __popc(vmask);
 }
 
 // Writes the c = payload_count(pl) seeds of l-mer qi at w onwards.
@@ -492,16 +567,30 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
   return incl - v;
 }
 
+// Writes a round's seeds (lane L's l-mers r0 + L*P .. in order, lanes in
+// order) from w onwards and advances w past them.
+__device__ __forceinline__ void round_emit(const IndexView& ix, const TargetView& t, int gap, int local, int qlen,
+                                           int r0, int lane, const uint64_t (&pl)[kSeedPerLane], int64_t& w,
+                                           int& valid, uint64_t* __restrict__ skey, uint32_t* __restrict__ sq) {
+  int cnt = 0;
+#pragma unroll
+  for (int i = 0; i < kSeedPerLane; ++i) cnt += payload_count(pl[i]);
+  int round_total;
+  int64_t wl = w + warp_excl_scan(cnt, lane, &round_total);
+#pragma unroll
+  for (int i = 0; i < kSeedPerLane; ++i)
+    if (pl[i] != kNoPayload) {
+      seed_put(ix, t, gap, local, qlen, r0 + lane * kSeedPerLane + i, pl[i], wl, valid, skey, sq);
+      wl += payload_count(pl[i]);
+    }
+  w += round_total;
+}
+
 constexpr int kSeedFusedThreads = 128;
 
 // The seed buffer is split into kSeedParts partitions of part_cap seeds, each
 // with its own cursor; strand s takes its range in partition s % kSeedParts, so
-// the range reservations of neighbouring warps hit different counters.  The
-// seed sort that follows orders a strand's seeds totally, so their order in
-// the range only has to be cheap to sort: l-mer order when every l-mer of the
-// register chunks has at most one entry, otherwise lane by lane; the seeds of
-// later chunks follow.  A warp loops over strands s,
-// s + (warps in the grid), ...; the launch gives every strand its own warp.
+// the range reservations of neighbouring warps hit different counters.
 // SMALL: l <= 16, keys read with 32-bit funnel shifts.
 template <bool SMALL>
 __global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, IndexView ix, TargetView t, int gap,
@@ -511,154 +600,65 @@ __global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, I
                                                                    int32_t* __restrict__ nvalid,
                                                                    uint64_t* __restrict__ skey,
                                                                    uint32_t* __restrict__ sq, int64_t part_cap) {
-  constexpr int R = kSeedRegChunks;
+  constexpr int P = kSeedPerLane;
+  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < q.nstrands; s += nwarps) {
-    const int64_t st = q.start[s];
-    const int qlen = q.len[s];
-    const int nk = qlen - ix.l + 1;
-    // the strand's N-mask words (lane i: word i), loaded next to the key words
-    const int64_t nw0 = st >> 6, nw1 = (st + (qlen > 0 ? qlen : 1) - 1) >> 6;
-    uint64_t nword = 0;
-    if (qlen > 0 && nw0 + lane <= nw1) {
-      nword = ld_stream(q.nmask + nw0 + lane);
-      if (lane == 0) nword &= ~0ull >> (st & 63);
-      if (nw0 + lane == nw1) nword &= ~0ull << (63 - ((st + qlen - 1) & 63));
+  if (s >= q.nstrands) return;
+  const int64_t st = q.start[s];
+  const int qlen = q.len[s];
+  const int nk = qlen - ix.l + 1;
+  // does the strand hold a non-ACGT base?  (one vote over its mask words)
+  bool any_n = false;
+  if (qlen > 0) {
+    const int64_t w0 = st >> 6, w1 = (st + qlen - 1) >> 6;
+    for (int64_t w = w0 + lane; w <= w1; w += 32) {
+      uint64_t m = ld_stream(q.nmask + w);
+      if (w == w0) m &= ~0ull >> (st & 63);
+      if (w == w1) m &= ~0ull << (63 - ((st + qlen - 1) & 63));
+      any_n |= m != 0;
     }
-    uint64_t preg[R];
-    uint32_t vmask = 0;
-    {
-      uint64_t hh[R];
-#pragma unroll
-      for (int ci = 0; ci < R; ++ci) {
-        const int qi = ci * 32 + lane;
-        const bool v = qi < nk;
-        uint64_t key = 0;
-        if (v) key = SMALL ? kmer_key16(reinterpret_cast<const uint32_t*>(q.packed), st + qi, ix.l)
-                           : kmer_key(q.packed, st + qi, ix.l);
-        hh[ci] = order_code(key, ix.l);
-        vmask |= (uint32_t)v << ci;
-      }
-      uint32_t fw[R];
-#pragma unroll
-      for (int ci = 0; ci < R; ++ci)
-        fw[ci] = ((vmask >> ci) & 1u) ? __ldg(ix.filter + filter_word(key_hash(hh[ci]), ix.fshift)) : 0u;
-      // l-mers with a non-ACGT base are not looked up (SRepelHasOddBase)
-      bool any_n = nword != 0;
-      for (int64_t w = nw0 + 32 + lane; w <= nw1; w += 32) {
-        uint64_t m = ld_stream(q.nmask + w);
-        if (w == nw1) m &= ~0ull << (63 - ((st + qlen - 1) & 63));
-        any_n |= m != 0;
-      }
-      if (__any_sync(kFull, any_n)) {
-#pragma unroll
-        for (int ci = 0; ci < R; ++ci) {
-          const int qi = ci * 32 + lane;
-          if (((vmask >> ci) & 1u) &&
-              (SMALL ? kmer_has_n16(reinterpret_cast<const uint32_t*>(q.nmask), st + qi, ix.l)
-                     : kmer_has_n(q.nmask, st + qi, ix.l)))
-            vmask &= ~(1u << ci);
-        }
-      }
-      ulonglong2 rec[R];
-      uint32_t pmask = 0;
-#pragma unroll
-      for (int ci = 0; ci < R; ++ci) {
-        const bool pass = ((vmask >> ci) & 1u) && filter_pass(fw[ci], key_hash(hh[ci]));
-        pmask |= (uint32_t)pass << ci;
-        rec[ci] = make_ulonglong2(0ull, kNoPayload);
-        if (pass) rec[ci] = __ldcs(ix.table + record_home(hh[ci], ix.l, ix.nbuckets));
-      }
-      // resolve from the home records; the keys displaced further read the
-      // next record (the home bucket's second, same 32-byte sector) together
-      uint32_t more = 0;
-#pragma unroll
-      for (int ci = 0; ci < R; ++ci) {
-        uint64_t pl = kNoPayload;
-        if ((pmask >> ci) & 1u) {
-          if (rec[ci].x == hh[ci]) pl = rec[ci].y;
-          else if (rec[ci].y != kNoPayload) more |= 1u << ci;
-        }
-        preg[ci] = pl;
-      }
-      if (__any_sync(kFull, more != 0)) {
-#pragma unroll
-        for (int ci = 0; ci < R; ++ci)
-          if ((more >> ci) & 1u) rec[ci] = __ldcs(ix.table + record_home(hh[ci], ix.l, ix.nbuckets) + 1);
-#pragma unroll
-        for (int ci = 0; ci < R; ++ci)
-          if ((more >> ci) & 1u) {
-            if (rec[ci].x == hh[ci] || rec[ci].y == kNoPayload) preg[ci] = rec[ci].y;
-            else preg[ci] = table_probe(ix, hh[ci], record_home(hh[ci], ix.l, ix.nbuckets) + 2);
-          }
-      }
-    }
-    int lane_cnt = 0;
-#pragma unroll
-    for (int ci = 0; ci < R; ++ci) lane_cnt += payload_count(preg[ci]);
-    int later = 0, valid_kmers = __popc(vmask);
-    for (int c0 = R * 32; c0 < nk; c0 += 32)
-      later += payload_count(seed_lookup(q, ix, st, c0 + lane, nk, valid_kmers));
-    const int reg_total = (int)__reduce_add_sync(kFull, (unsigned)lane_cnt);
-    const int total = reg_total + (int)__reduce_add_sync(kFull, (unsigned)later);
-    valid_kmers = (int)__reduce_add_sync(kFull, (unsigned)valid_kmers);
-    const int part = (int)(s % kSeedParts);
-    unsigned long long rel = 0;
-    if (lane == 0) {
-      if (valid_kmers) atomicAdd(n_kmers, (unsigned long long)valid_kmers);
-      rel = total ? atomicAdd(&cursor[part], (unsigned long long)total) : 0ull;
-    }
-    rel = __shfl_sync(kFull, rel, 0);
-    const unsigned long long base = (unsigned long long)part * (unsigned long long)part_cap + rel;
-    if (lane == 0) {
-      off[s] = (int64_t)base;
-      cnt[s] = total;
-    }
-    const int64_t cap = (int64_t)(part + 1) * part_cap;
-    if (total == 0 || (int64_t)(base + total) > cap) {
-      if (lane == 0) nvalid[s] = 0;
-      continue;
-    }
-    int valid = 0;
-    bool lane_multi = false;
-#pragma unroll
-    for (int ci = 0; ci < R; ++ci) lane_multi |= payload_count(preg[ci]) > 1;
-    if (!__any_sync(kFull, lane_multi)) {
-      // one seed per l-mer at most: l-mer order (chunk, then lane), so that the
-      // seeds of a strand on a single diagonal arrive already sorted
-      const unsigned lt = lanemask_lt();
-      int64_t w = (int64_t)base;
-#pragma unroll
-      for (int ci = 0; ci < R; ++ci) {
-        const unsigned b = __ballot_sync(kFull, preg[ci] != kNoPayload);
-        if (preg[ci] != kNoPayload)
-          seed_put(ix, t, gap, local, qlen, ci * 32 + lane, preg[ci], w + __popc(b & lt), valid, skey, sq);
-        w += __popc(b);
-      }
-    } else {
-      int unused;
-      int64_t w = (int64_t)base + warp_excl_scan(lane_cnt, lane, &unused);
-#pragma unroll
-      for (int ci = 0; ci < R; ++ci)
-        if (preg[ci] != kNoPayload) {
-          seed_put(ix, t, gap, local, qlen, ci * 32 + lane, preg[ci], w, valid, skey, sq);
-          w += payload_count(preg[ci]);
-        }
-    }
-    int64_t w = (int64_t)base + reg_total;
-    for (int c0 = R * 32; c0 < nk; c0 += 32) {
-      int dummy = 0;
-      const uint64_t pl = seed_lookup(q, ix, st, c0 + lane, nk, dummy);
-      const int c = payload_count(pl);
-      int chunk_total;
-      const int e = warp_excl_scan(c, lane, &chunk_total);
-      if (c) seed_put(ix, t, gap, local, qlen, c0 + lane, pl, w + e, valid, skey, sq);
-      w += chunk_total;
-    }
-    valid = (int)__reduce_add_sync(kFull, (unsigned)valid);
-    if (lane == 0) nvalid[s] = valid;
   }
+  any_n = __any_sync(kFull, any_n);
+  uint64_t pl0[P];
+  int valid_kmers = round_lookup<SMALL>(q, ix, st, nk, 0, lane, any_n, pl0);
+  int lane_cnt = 0;
+#pragma unroll
+  for (int i = 0; i < P; ++i) lane_cnt += payload_count(pl0[i]);
+  for (int r0 = kSeedRound; r0 < nk; r0 += kSeedRound) {
+    uint64_t pl[P];
+    valid_kmers += round_lookup<SMALL>(q, ix, st, nk, r0, lane, any_n, pl);
+#pragma unroll
+    for (int i = 0; i < P; ++i) lane_cnt += payload_count(pl[i]);
+  }
+  const int total = (int)__reduce_add_sync(kFull, (unsigned)lane_cnt);
+  valid_kmers = (int)__reduce_add_sync(kFull, (unsigned)valid_kmers);
+  const int part = (int)(s % kSeedParts);
+  unsigned long long rel = 0;
+  if (lane == 0) {
+    if (valid_kmers) atomicAdd(n_kmers + part, (unsigned long long)valid_kmers);
+    rel = total ? atomicAdd(&cursor[part], (unsigned long long)total) : 0ull;
+  }
+  rel = __shfl_sync(kFull, rel, 0);
+  const unsigned long long base = (unsigned long long)part * (unsigned long long)part_cap + rel;
+  if (lane == 0) {
+    off[s] = (int64_t)base;
+    cnt[s] = total;
+  }
+  const int64_t cap = (int64_t)(part + 1) * part_cap;
+  if (total == 0 || (int64_t)(base + total) > cap) {
+    if (lane == 0) nvalid[s] = 0;
+    return;
+  }
+  int valid = 0;
+  int64_t w = (int64_t)base;
+  round_emit(ix, t, gap, local, qlen, 0, lane, pl0, w, valid, skey, sq);
+  for (int r0 = kSeedRound; r0 < nk; r0 += kSeedRound) {
+    uint64_t pl[P];
+    round_lookup<SMALL>(q, ix, st, nk, r0, lane, any_n, pl);
+    round_emit(ix, t, gap, local, qlen, r0, lane, pl, w, valid, skey, sq);
+  }
+  valid = (int)__reduce_add_sync(kFull, (unsigned)valid);
+  if (lane == 0) nvalid[s] = valid;
 }
 
 __global__ void k_window_first(const int32_t* __restrict__ nvalid, const int32_t* __restrict__ wstart, int nwin,

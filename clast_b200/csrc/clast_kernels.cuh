@@ -67,7 +67,9 @@ void table_place(const uint64_t* ucode, const int32_t* ustart, const int32_t* uc
 // which hold seed_parts() partitions of part_cap seeds.  Strand s reserves its
 // range in partition s % seed_parts() through cursors[partition]; a partition
 // whose cursor ends above part_cap was not fully written and the call must be
-// repeated with part_cap >= the largest cursor.
+// repeated with part_cap >= the largest cursor.  n_kmers holds seed_parts()
+// counters (valid l-mers of the strands of each partition; the caller sums
+// them), so that no single address takes one atomic per strand.
 int seed_parts();
 void seed_fused(const QueryView& q, const IndexView& ix, const TargetView& t, int gap, int local,
                 unsigned long long* cursors, unsigned long long* n_kmers, int64_t* off, int32_t* cnt, int32_t* nvalid,
