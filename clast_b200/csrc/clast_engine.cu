@@ -227,12 +227,28 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix) {
   uint64_t* nmask = ws.get<uint64_t>("ix_nmask", (size_t)(n / 64 + 4));
   pack_bases(bases, n, packed, nmask, st);
   const int64_t ns = n / p->stride;  // CDeviceHashTable.cu:34
-  uint64_t* keys = ws.get<uint64_t>("ix_keys", ns);
-  int32_t* vals = ws.get<int32_t>("ix_vals", ns);
-  uint64_t* keys2 = ws.get<uint64_t>("ix_keys2", ns);
-  int32_t* vals2 = ws.get<int32_t>("ix_vals2", ns);
-  sample_keys(packed, nmask, ns, p->stride, l, keys, vals, st);
-  radix_sort_pairs(ws, keys, vals, keys2, vals2, ns, 2 * l + 1, st);
+  // samples sorted by code (equal keys adjacent, in window-position order):
+  // one word code << pbits | position when both fit in 64 bits, else
+  // (code, position) pairs
+  int pbits = 1;
+  while ((1ll << pbits) < ns) ++pbits;
+  if (2 * l + 1 + pbits > 64) pbits = 0;
+  uint64_t* items = ws.get<uint64_t>("ix_items", ns);
+  uint64_t* items2 = ws.get<uint64_t>("ix_items2", ns);
+  int32_t* pos = pbits ? nullptr : ws.get<int32_t>("ix_pos", ns);
+  int32_t* pos2 = pbits ? nullptr : ws.get<int32_t>("ix_pos2", ns);
+  sample_keys(packed, nmask, ns, p->stride, l, pbits, items, pos, st);
+  const int in_alt = radix_sort_u64(ws, items, pos, items2, pos2, ns, pbits, pbits + 2 * l + 1, st);
+  uint64_t* keys;
+  int32_t* vals;
+  if (pbits) {
+    keys = ws.get<uint64_t>("ix_keys", ns);
+    vals = ws.get<int32_t>("ix_vals", ns);
+    split_items(in_alt ? items2 : items, ns, pbits, keys, vals, st);
+  } else {
+    keys = in_alt ? items2 : items;
+    vals = in_alt ? pos2 : pos;
+  }
   int64_t* scal = ws.get<int64_t>("ix_scalar", 4);
   int64_t nv = 0;
   if (ns > 0) {

@@ -3,7 +3,7 @@
 // Reference (masayano/CLAST) stages and the kernels that replace them:
 //   SRead2bit/SRepelHasOddBase + CDeviceSeqList_query::createHashIndex -> pack_bases, kmer_at
 //   CDeviceHashTable (sort_by_key, unique, reduce_by_key, scan, cut)   -> sample_keys,
-//       radix_sort_pairs, index_* (hash table + Bloom filter for one-probe lookups)
+//       radix_sort_u64, index_*, table_* (hash table + Bloom filter for one-probe lookups)
 //   createRawSeedList (binarySearch, writeSeedList)                     -> seed_fused
 //   deleteSeedsOnSequenceBoundary                                       -> folded into seed_fused
 //   sortSeeds / deletingIsolateSeeds / deleteDuplicateSeeds             -> seed_sort_filter
@@ -204,21 +204,45 @@ __global__ void k_build_window(const char* __restrict__ src, const int64_t* __re
 // ------------------------------------------------------------------------
 // index build
 // ------------------------------------------------------------------------
+// Sample j of the window: its code (4^l for an l-mer with a non-ACGT base).
+// pbits > 0: one sortable word code << pbits | j; pbits = 0: the code, with j
+// in vals.
 __global__ void k_sample_keys(const uint64_t* __restrict__ packed, const uint64_t* __restrict__ nmask,
-                              int64_t ns, int stride, int l, uint64_t* __restrict__ keys,
+                              int64_t ns, int stride, int l, int pbits, uint64_t* __restrict__ items,
                               int32_t* __restrict__ vals) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ns) return;
   uint64_t key;
-  keys[j] = kmer_at(packed, nmask, j * stride, l, key) ? order_code(key, l) : (1ull << (2 * l));
-  vals[j] = (int32_t)j;
+  const uint64_t c = kmer_at(packed, nmask, j * stride, l, key) ? order_code(key, l) : (1ull << (2 * l));
+  if (pbits > 0) {
+    items[j] = (c << pbits) | (uint64_t)j;
+  } else {
+    items[j] = c;
+    vals[j] = (int32_t)j;
+  }
 }
 
-constexpr int kRsThreads = 256, kRsItems = 16, kRsTile = kRsThreads * kRsItems;
+__global__ void k_split_items(const uint64_t* __restrict__ items, int64_t n, int pbits, uint64_t* __restrict__ keys,
+                              int32_t* __restrict__ vals) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t v = items[i];
+  keys[i] = v >> pbits;
+  vals[i] = (int32_t)(v & ((1ull << pbits) - 1));
+}
 
-__global__ void __launch_bounds__(kRsThreads) k_radix_hist(const uint64_t* __restrict__ keys, int64_t n,
-                                                           int shift, uint32_t* __restrict__ hist,
-                                                           int nblocks) {
+// ---- LSD radix sort of 64-bit words by a bit range, 8 bits per pass ----
+// A block takes a tile of kRsTile consecutive words; warp w owns words
+// [w * kRsWarpItems, (w + 1) * kRsWarpItems) of it.  Each pass: per-block digit
+// counts (k_rs_hist), one scan of the counts laid out digit-major, then
+// k_rs_scatter ranks the tile stably in shared memory (warp-private digit
+// counters, ranks inside 32-word steps by match_any) and writes every digit's
+// run out contiguously.
+constexpr int kRsThreads = 256, kRsItems = 16, kRsTile = kRsThreads * kRsItems;
+constexpr int kRsWarps = kRsThreads / 32, kRsWarpItems = 32 * kRsItems;
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint64_t* __restrict__ keys, int64_t n, int shift,
+                                                        uint32_t* __restrict__ hist, int nblocks) {
   __shared__ uint32_t h[256];
   h[threadIdx.x] = 0;
   __syncthreads();
@@ -232,52 +256,89 @@ __global__ void __launch_bounds__(kRsThreads) k_radix_hist(const uint64_t* __res
   hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-__global__ void __launch_bounds__(kRsThreads) k_radix_scatter(const uint64_t* __restrict__ kin,
-                                                              const int32_t* __restrict__ vin,
-                                                              uint64_t* __restrict__ kout,
-                                                              int32_t* __restrict__ vout, int64_t n, int shift,
-                                                              const int64_t* __restrict__ offs, int nblocks) {
-  __shared__ uint32_t wcnt[kRsThreads / 32][256];
-  __shared__ uint32_t run[256];
+// PAY: a 32-bit value travels with every word (vin -> vout).  Dynamic shared
+// memory: the staged tile, kRsTile words (+ kRsTile values).
+template <bool PAY>
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __restrict__ kin,
+                                                           const int32_t* __restrict__ vin,
+                                                           uint64_t* __restrict__ kout, int32_t* __restrict__ vout,
+                                                           int64_t n, int shift, const int64_t* __restrict__ offs,
+                                                           int nblocks) {
+  __shared__ uint32_t wc[kRsWarps][256];  // per-warp digit counters, then running positions
+  __shared__ uint32_t tile_start[256];
+  __shared__ uint32_t wsum[kRsWarps];
   __shared__ int64_t goff[256];
+  extern __shared__ uint64_t stage[];
+  int32_t* stage_v = reinterpret_cast<int32_t*>(stage + kRsTile);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   goff[tid] = offs[(int64_t)tid * nblocks + blockIdx.x];
-  run[tid] = 0;
 #pragma unroll
-  for (int w = 0; w < kRsThreads / 32; ++w) wcnt[w][tid] = 0;
+  for (int w = 0; w < kRsWarps; ++w) wc[w][tid] = 0;
   __syncthreads();
-  const int64_t base = (int64_t)blockIdx.x * kRsTile;
+  const int64_t base = (int64_t)blockIdx.x * kRsTile + (int64_t)warp * kRsWarpItems;
   const unsigned lt = lanemask_lt();
+  uint64_t k[kRsItems];
+  int32_t v[PAY ? kRsItems : 1];
+  // warp-private digit counts, in word order
+#pragma unroll
   for (int r = 0; r < kRsItems; ++r) {
-    const int64_t idx = base + r * kRsThreads + tid;
-    const bool valid = idx < n;
-    const uint64_t k = valid ? kin[idx] : 0;
-    const int32_t v = valid ? vin[idx] : 0;
-    const unsigned d = valid ? (unsigned)((k >> shift) & 255) : 256u;
+    const int64_t idx = base + r * 32 + lane;
+    k[r] = idx < n ? kin[idx] : 0ull;
+    if (PAY) v[r] = idx < n ? vin[idx] : 0;
+    const unsigned d = idx < n ? (unsigned)((k[r] >> shift) & 255) : 256u;
     const unsigned peers = __match_any_sync(kFull, d);
-    const unsigned rank = __popc(peers & lt);
-    if (valid && lane == __ffs(peers) - 1) wcnt[warp][d] = __popc(peers);
-    __syncthreads();
-    {
-      uint32_t acc = run[tid];
+    if (d < 256u && lane == __ffs(peers) - 1) wc[warp][d] += __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // digit d = tid: tile-wide start (exclusive scan over digits), then the
+  // start of each warp's run of that digit
+  uint32_t tot = 0;
 #pragma unroll
-      for (int w = 0; w < kRsThreads / 32; ++w) {
-        const uint32_t c = wcnt[w][tid];
-        wcnt[w][tid] = acc;
-        acc += c;
-      }
-      run[tid] = acc;
-    }
-    __syncthreads();
-    if (valid) {
-      const int64_t pos = goff[d] + wcnt[warp][d] + rank;
-      kout[pos] = k;
-      vout[pos] = v;
-    }
-    __syncthreads();
+  for (int w = 0; w < kRsWarps; ++w) tot += wc[w][tid];
+  uint32_t incl = tot;
 #pragma unroll
-    for (int w = 0; w < kRsThreads / 32; ++w) wcnt[w][tid] = 0;
-    __syncthreads();
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  uint32_t start = incl - tot;
+  for (int w = 0; w < warp; ++w) start += wsum[w];
+  tile_start[tid] = start;
+#pragma unroll
+  for (int w = 0; w < kRsWarps; ++w) {
+    const uint32_t c = wc[w][tid];
+    wc[w][tid] = start;
+    start += c;
+  }
+  __syncthreads();
+  // stable positions inside the tile
+#pragma unroll
+  for (int r = 0; r < kRsItems; ++r) {
+    const int64_t idx = base + r * 32 + lane;
+    const unsigned d = idx < n ? (unsigned)((k[r] >> shift) & 255) : 256u;
+    const unsigned peers = __match_any_sync(kFull, d);
+    if (d < 256u) {
+      const uint32_t at = wc[warp][d] + __popc(peers & lt);
+      stage[at] = k[r];
+      if (PAY) stage_v[at] = v[r];
+    }
+    __syncwarp();
+    if (d < 256u && lane == __ffs(peers) - 1) wc[warp][d] += __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // digit runs out, contiguous
+  const int64_t tile0 = (int64_t)blockIdx.x * kRsTile;
+  const int valid = (int)min((int64_t)kRsTile, n - tile0);
+  for (int i = tid; i < valid; i += kRsThreads) {
+    const uint64_t w = stage[i];
+    const unsigned d = (unsigned)((w >> shift) & 255);
+    const int64_t at = goff[d] + (i - (int)tile_start[d]);
+    kout[at] = w;
+    if (PAY) vout[at] = stage_v[i];
   }
 }
 
@@ -1587,38 +1648,48 @@ void build_window(const char* src, const int64_t* src_off, const int32_t* gatewa
   CLAST_LAUNCHED();
 }
 
-void sample_keys(const uint64_t* packed, const uint64_t* nmask, int64_t n_samples, int stride, int l,
-                 uint64_t* keys, int32_t* vals, cudaStream_t st) {
+void sample_keys(const uint64_t* packed, const uint64_t* nmask, int64_t n_samples, int stride, int l, int pbits,
+                 uint64_t* items, int32_t* vals, cudaStream_t st) {
   if (n_samples <= 0) return;
-  k_sample_keys<<<blocks_for(n_samples, 256), 256, 0, st>>>(packed, nmask, n_samples, stride, l, keys, vals);
+  k_sample_keys<<<blocks_for(n_samples, 256), 256, 0, st>>>(packed, nmask, n_samples, stride, l, pbits, items,
+                                                             vals);
   CLAST_LAUNCHED();
 }
 
-void radix_sort_pairs(Workspace& ws, uint64_t* keys, int32_t* vals, uint64_t* keys_alt, int32_t* vals_alt,
-                      int64_t n, int bits, cudaStream_t st) {
-  if (n <= 1) return;
+void split_items(const uint64_t* items, int64_t n, int pbits, uint64_t* keys, int32_t* vals, cudaStream_t st) {
+  if (n <= 0) return;
+  k_split_items<<<blocks_for(n, 256), 256, 0, st>>>(items, n, pbits, keys, vals);
+  CLAST_LAUNCHED();
+}
+
+int radix_sort_u64(Workspace& ws, uint64_t* keys, int32_t* vals, uint64_t* keys_alt, int32_t* vals_alt, int64_t n,
+                   int lo_bit, int hi_bit, cudaStream_t st) {
+  if (n <= 1) return 0;
   const int nblocks = (int)((n + kRsTile - 1) / kRsTile);
   uint32_t* hist = ws.get<uint32_t>("rs_hist", (size_t)256 * nblocks);
   int64_t* offs = ws.get<int64_t>("rs_offs", (size_t)256 * nblocks + 1);
-  uint64_t* ka = keys;
+  const bool pay = vals != nullptr;
+  const size_t smem = (size_t)kRsTile * (sizeof(uint64_t) + (pay ? sizeof(int32_t) : 0));
+  // more than 48 KB of dynamic shared memory needs the opt-in (per device)
+  if (pay) CLAST_CK(cudaFuncSetAttribute(k_rs_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  else CLAST_CK(cudaFuncSetAttribute(k_rs_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  uint64_t* a = keys;
+  uint64_t* b = keys_alt;
   int32_t* va = vals;
-  uint64_t* kb = keys_alt;
   int32_t* vb = vals_alt;
-  int passes = 0;
-  for (int shift = 0; shift < bits; shift += 8) {
-    k_radix_hist<<<nblocks, kRsThreads, 0, st>>>(ka, n, shift, hist, nblocks);
+  int which = 0;
+  for (int shift = lo_bit; shift < hi_bit; shift += 8) {
+    k_rs_hist<<<nblocks, kRsThreads, 0, st>>>(a, n, shift, hist, nblocks);
     CLAST_LAUNCHED();
     scan_impl<uint32_t>(ws, hist, (int64_t)256 * nblocks, offs, st, 0);
-    k_radix_scatter<<<nblocks, kRsThreads, 0, st>>>(ka, va, kb, vb, n, shift, offs, nblocks);
+    if (pay) k_rs_scatter<true><<<nblocks, kRsThreads, smem, st>>>(a, va, b, vb, n, shift, offs, nblocks);
+    else k_rs_scatter<false><<<nblocks, kRsThreads, smem, st>>>(a, nullptr, b, nullptr, n, shift, offs, nblocks);
     CLAST_LAUNCHED();
-    std::swap(ka, kb);
+    std::swap(a, b);
     std::swap(va, vb);
-    ++passes;
+    which ^= 1;
   }
-  if (passes & 1) {
-    CLAST_CK(cudaMemcpyAsync(keys, ka, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
-    CLAST_CK(cudaMemcpyAsync(vals, va, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
-  }
+  return which;
 }
 
 void count_below(const uint64_t* keys, int64_t n, uint64_t bound, int64_t* out, cudaStream_t st) {

@@ -29,13 +29,18 @@ void build_strands(const char* reads, const int64_t* offsets, int64_t n_reads, i
 // sequence k of the window is src[src_off[k] .. src_off[k]+lengths[k]).
 void build_window(const char* src, const int64_t* src_off, const int32_t* gateway, const int32_t* lengths,
                   int nseqs, int64_t n, char* out, cudaStream_t st);
-// Sampled keys at window positions j*stride; invalid k-mers get key 1<<(2l).
-void sample_keys(const uint64_t* packed, const uint64_t* nmask, int64_t n_samples, int stride, int l,
-                 uint64_t* keys, int32_t* vals, cudaStream_t st);
-// Stable LSD radix sort of (keys, vals) on the low `bits` key bits; the result
-// ends in (keys, vals) (alt buffers are scratch).
-void radix_sort_pairs(Workspace& ws, uint64_t* keys, int32_t* vals, uint64_t* keys_alt, int32_t* vals_alt,
-                      int64_t n, int bits, cudaStream_t st);
+// Samples at window positions j*stride: order_code of the l-mer (4^l when it
+// has a non-ACGT base).  pbits > 0: items[j] = code << pbits | j; pbits = 0:
+// items[j] = code, vals[j] = j.
+void sample_keys(const uint64_t* packed, const uint64_t* nmask, int64_t n_samples, int stride, int l, int pbits,
+                 uint64_t* items, int32_t* vals, cudaStream_t st);
+// keys[i] = items[i] >> pbits, vals[i] = the low pbits bits.
+void split_items(const uint64_t* items, int64_t n, int pbits, uint64_t* keys, int32_t* vals, cudaStream_t st);
+// Stable LSD radix sort of 64-bit words by bits [lo_bit, hi_bit), carrying
+// vals along unless vals is null.  Returns 0 when the result is in (keys,
+// vals), 1 when it is in (keys_alt, vals_alt).
+int radix_sort_u64(Workspace& ws, uint64_t* keys, int32_t* vals, uint64_t* keys_alt, int32_t* vals_alt, int64_t n,
+                   int lo_bit, int hi_bit, cudaStream_t st);
 // *out = number of keys < bound in the sorted array keys[0..n)
 void count_below(const uint64_t* keys, int64_t n, uint64_t bound, int64_t* out, cudaStream_t st);
 void index_heads(const uint64_t* keys, int64_t nv, int32_t* head, cudaStream_t st);
