@@ -373,6 +373,7 @@ struct QueryBatch {
   int32_t nstrands = 0;
   DevArray<int32_t> wstart;  // strand index where each window starts, plus the end
   int32_t nwin = 0;
+  int32_t min_len = 0, max_len = 0;  // strand lengths (the DP orders hits by rows when they differ)
   QueryView view() const {
     QueryView q;
     q.bases = bases.p + kPad;
@@ -491,8 +492,21 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   o.evalue = ws.get<double>("d_e", H);
   o.keep = ws.get<uint8_t>("d_keep", H);
   DpParams dp{p->lmer, p->stride, p->gap, p->local, p->cutoff, p->total_db, p->K, p->lambda};
+  // reads of different lengths: the DP takes the hits longest first, so that a
+  // warp's hits have about the same number of rows (the reference sorts them
+  // by rows before aligning too, CDeviceHitList_alignmentHits.cu:10-58)
+  const uint64_t* order = nullptr;
+  if (qb.max_len != qb.min_len && H > 1) {
+    const int rows_max = std::max(1, qb.max_len - p->lmer + 1);
+    int bits = 1;
+    while ((1ll << bits) <= rows_max) ++bits;
+    uint64_t* ok = ws.get<uint64_t>("h_order", H);
+    uint64_t* ok2 = ws.get<uint64_t>("h_order2", H);
+    dp_order_keys(hs, qb.len.p, H, p->lmer, rows_max, ok, st);
+    order = radix_sort_u64(ws, ok, nullptr, ok2, nullptr, H, 32, 32 + bits, st) ? ok2 : ok;
+  }
   tm.begin(st);
-  banded_dp(tv, q, hk, hq, hs, H, dp, o, st);
+  banded_dp(tv, q, hk, hq, hs, order, H, dp, o, st);
   tm.end(StageTimer::DP, st);
   // resultSorting + deleteHits_duplicateResult, per read
   uint64_t* k1 = ws.get<uint64_t>("f_k1", H);
@@ -685,10 +699,13 @@ int clast_search(clast_ctx* ctx, const clast_index* ix, const clast_params* p, c
     qb.nstrands = n_qseqs;
     upload_padded(q_bases, n_qbases, qb.bases, st);
     std::vector<int64_t> start(n_qseqs);
+    qb.min_len = n_qseqs ? INT32_MAX : 0;
     for (int32_t i = 0; i < n_qseqs; ++i) {
       start[i] = q_gateway[i];
       if (q_gateway[i] < 0 || q_lengths[i] < 0 || (int64_t)q_gateway[i] + q_lengths[i] > n_qbases)
         throw std::invalid_argument("query sequence outside the base array");
+      qb.min_len = std::min(qb.min_len, q_lengths[i]);
+      qb.max_len = std::max(qb.max_len, q_lengths[i]);
     }
     qb.start.alloc(n_qseqs);
     qb.len.alloc(n_qseqs);
@@ -886,6 +903,13 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     QueryBatch qb;
     qb.n = 2 * nb;
     qb.nstrands = (int32_t)(2 * nreads);
+    qb.min_len = nreads ? INT32_MAX : 0;
+    for (int64_t r = 0; r < nreads; ++r) {
+      const int64_t len = reads->offsets[r + 1] - reads->offsets[r];
+      if (len > INT32_MAX) throw std::invalid_argument("read longer than 2^31 bases");
+      qb.min_len = std::min<int32_t>(qb.min_len, (int32_t)len);
+      qb.max_len = std::max<int32_t>(qb.max_len, (int32_t)len);
+    }
     qb.bases.alloc((size_t)qb.n + 2 * kPad);
     qb.start.alloc(2 * nreads);
     qb.len.alloc(2 * nreads);
@@ -1229,7 +1253,7 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
     o.evalue = ws.get<double>("d_e", H);
     o.keep = ws.get<uint8_t>("d_keep", H);
     DpParams dp{p->lmer, p->stride, p->gap, p->local, p->cutoff, p->total_db, p->K, p->lambda};
-    banded_dp(tv, q, hk, hq, hs, H, dp, o, st);
+    banded_dp(tv, q, hk, hq, hs, nullptr, H, dp, o, st);
     // resultSorting + deleteHits_duplicateResult, per read
     uint64_t* k1 = ws.get<uint64_t>("f_k1", H);
     uint64_t* k2 = ws.get<uint64_t>("f_k2", H);

@@ -1230,14 +1230,12 @@ __host__ __device__ constexpr int class_of_letter(int i) {  // i = letter - 'A'
   return i == 0 ? 0 : i == 2 ? 1 : i == 6 ? 2 : i == 19 ? 3 : i == 23 ? kClassX
        : (i == 4 || i == 5 || i == 8 || i == 9 || i == 11 || i == 14 || i == 15 || i == 16 || i == 25) ? 5 : 4;
 }
-// (point << 16) | (match & 0xffff) for target class t, query class q.
-__device__ __forceinline__ int packed_score(int t, int q) {
-  int point, match;
-  if (t == kClassX || q == kClassX) { point = -1000; match = -1000; }
-  else if (t == 5 || q == 5) { point = -1; match = -1; }
-  else if (t == q && t < 4) { point = 1; match = 1; }
-  else { point = -3; match = 0; }
-  return (int)((unsigned)point << 16) | (match & 0xffff);
+// (point, match increment) for target class t, query class q.
+__device__ __forceinline__ int2 cell_score(int t, int q) {
+  if (t == kClassX || q == kClassX) return make_int2(-1000, -1000);
+  if (t == 5 || q == 5) return make_int2(-1, -1);
+  if (t == q && t < 4) return make_int2(1, 1);
+  return make_int2(-3, 0);
 }
 
 // Banded DP of one hit, backward pass then forward pass, in ONE row loop of
@@ -1290,7 +1288,7 @@ struct Band {
 };
 
 template <int GAP, bool LOCAL>
-__device__ __forceinline__ void banded_hit(const int* __restrict__ tab, const char* __restrict__ tb, int64_t tstart,
+__device__ __forceinline__ void banded_hit(const int2* __restrict__ tab, const char* __restrict__ tb, int64_t tstart,
                                            int tlen, const char* __restrict__ qb, int64_t qstart, int qlen, int tidx,
                                            int qidx, int l, int& t_hl, int& q_hl, int& match, int& score,
                                            int& o_tidx, int& o_qidx) {
@@ -1299,18 +1297,20 @@ __device__ __forceinline__ void banded_hit(const int* __restrict__ tab, const ch
   constexpr int kBotA = (GAP + 1) * kGapExtend + kGapOpen + kGapSO;  // fixed band row 2*GAP+2
   constexpr int kBotB = (GAP + 1) * kGapExtend + kGapOpen + kGapOpen + kGapExtend;
   constexpr int kMarginA = kMarginScore + kGapSO, kMarginB = kMarginScore + kGapExtend;
-  constexpr int64_t kNoLow = INT64_MIN / 2, kNoHigh = INT64_MAX / 2;
+  constexpr int kNoLow = INT_MIN / 2, kNoHigh = INT_MAX / 2;
   const int rows_b = qlen - (qidx + l);  // alignmentSize of the backward pass
   const int rows_f = qidx;              // rows of the forward pass
   const int rows = rows_b + rows_f;
   Band<GAP> bd;
+  const char* __restrict__ t_seq = tb + tstart;
   // backward pass (globalAlignBackward / localAlignBackward): target bases
   // tIdx + l - gap + q + c ('X' at or past tLen), query bases qIdx + l + q
-  int64_t q_at = qstart + qidx + l;
+  const char* q_ptr = qb + qstart + qidx + l;  // query base of the current row
   int q_step = 1;
-  int64_t t_at = (int64_t)tidx + l + GAP + 1;  // next target base to shift in after row 0
+  int t_ib = tidx + l + GAP + 1;  // next target base to shift in
   int t_step = 1;
-  int64_t t_lo = kNoLow, t_hi = tlen;
+  int t_lo = kNoLow, t_hi = tlen;
+  int row_end = rows_b;  // last row + 1 of the current pass
   bd.init(tb, tstart, (int64_t)tidx + l - GAP, 1, t_lo, t_hi);
   int bs = 0, bm = 0, calc = -1, ep = GAP, qrow = 0;
   int pass = 0;
@@ -1330,26 +1330,27 @@ __device__ __forceinline__ void banded_hit(const int* __restrict__ tab, const ch
       score += best;
     }
   };
-  char q_cur = (rows_b > 0) ? qb[q_at] : 'N';
+  char q_cur = (rows_b > 0) ? *q_ptr : 'N';
   for (int r = 0; r < rows; ++r) {
     if (r == rows_b) {  // switch to the forward pass (globalAlignForward / localAlignForward)
       finish(rows_b);
       pass = 1;
-      q_at = qstart + qidx - 1;  // query bases qIdx - q - 1
+      q_ptr = qb + qstart + qidx - 1;  // query bases qIdx - q - 1
       q_step = -1;
-      t_at = (int64_t)tidx - GAP - 2;  // target bases tIdx + gap - 1 - q - c ('X' below 0)
+      t_ib = tidx - GAP - 2;  // target bases tIdx + gap - 1 - q - c ('X' below 0)
       t_step = -1;
       t_lo = 0;
       t_hi = kNoHigh;
+      row_end = rows;
       bd.init(tb, tstart, (int64_t)tidx + GAP - 1, -1, t_lo, t_hi);
       bs = 0; bm = 0; calc = -1; ep = GAP; qrow = 0;
-      q_cur = qb[q_at];
+      q_cur = *q_ptr;
     }
     // loads for the next row go out first; their latency hides behind this row
-    const int64_t ib = t_at + (int64_t)t_step * qrow;
-    const char t_next = (ib < t_lo || ib >= t_hi) ? 'X' : tb[tstart + ib];
-    const bool more = (pass == 0) ? (r + 1 < rows_b) : (r + 1 < rows);
-    const char q_next = more ? qb[q_at + (int64_t)q_step * (qrow + 1)] : 'N';
+    const char t_next = (t_ib < t_lo || t_ib >= t_hi) ? 'X' : t_seq[t_ib];
+    t_ib += t_step;
+    const char q_next = (r + 1 < row_end) ? q_ptr[q_step] : 'N';
+    q_ptr += q_step;
     const int qc = base_class(q_cur);
     int hA = kMarginA, hB = kMarginB, hM = kMarginScore;  // row 0 of the band (left margin)
 #pragma unroll
@@ -1359,13 +1360,13 @@ __device__ __forceinline__ void banded_hit(const int* __restrict__ tab, const ch
       const int vM = (c + 1 < W) ? bd.M[(c + 1) % W] : 0;
       const int nV = max(vA, vB);
       const int nH = max(hA, hB);
-      const int w = tab[bd.tc[c] | qc];
-      const int pt = bd.A[c] + (w >> 16);
+      const int2 w = tab[bd.tc[c] | qc];  // (POINT + 7, match increment)
+      const int pt = bd.A[c] + w.x;
       bool h_wins, not_diag;
       const int mx = __vibmax_s32(nH, nV, &h_wins);   // h_wins = nH >= nV
       const int nS = __vibmax_s32(mx, pt, &not_diag);  // not_diag = mx >= pt
       const int side_m = h_wins ? hM : vM;
-      const int nM = not_diag ? side_m : (bd.M[c] + ((w << 16) >> 16));
+      const int nM = not_diag ? side_m : (bd.M[c] + w.y);
       const int nA = nS + kGapSO;
       bd.A[c] = nA;
       bd.B[c] = nV + kGapExtend;
@@ -1396,6 +1397,7 @@ struct DpKernelArgs {
   const uint64_t* hk;
   const int32_t* hq;
   const int32_t* hs;
+  const uint64_t* order;
   int64_t n;
   DpParams p;
   DpOut o;
@@ -1403,14 +1405,16 @@ struct DpKernelArgs {
 
 template <int GAP, bool LOCAL>
 __global__ void __launch_bounds__(128) k_banded_dp(DpKernelArgs a) {
-  __shared__ int tab[32 * 32];  // [target letter][query letter], letters 'A'..'Z'
-  for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x)
-    tab[i] = packed_score(class_of_letter((i >> 5) < 26 ? (i >> 5) : kNClass),
-                          class_of_letter((i & 31) < 26 ? (i & 31) : kNClass)) +
-             ((kGapOpen + kGapExtend) * -65536);  // POINT + 7 in the high half
+  __shared__ int2 tab[32 * 32];  // [target letter][query letter], letters 'A'..'Z': (POINT + 7, match)
+  for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
+    const int2 w = cell_score(class_of_letter((i >> 5) < 26 ? (i >> 5) : kNClass),
+                              class_of_letter((i & 31) < 26 ? (i & 31) : kNClass));
+    tab[i] = make_int2(w.x - (kGapOpen + kGapExtend), w.y);
+  }
   __syncthreads();
-  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (h >= a.n) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const int64_t h = a.order ? (int64_t)(uint32_t)a.order[i] : i;
   const uint64_t k = a.hk[h];
   const int qidx = a.hq[h];
   const int s = a.hs[h];
@@ -1828,10 +1832,25 @@ void gather_hits(const uint64_t* skey, const uint32_t* sq, const int64_t* off, c
   CLAST_LAUNCHED();
 }
 
-void banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq, const int32_t* hs,
-               int64_t n_hits, const DpParams& p, const DpOut& o, cudaStream_t st) {
+__global__ void k_dp_order_keys(const int32_t* __restrict__ hs, const int32_t* __restrict__ q_len, int64_t n,
+                                int l, int rows_max, uint64_t* __restrict__ keys) {
+  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= n) return;
+  const int rows = max(0, min(rows_max, q_len[hs[h]] - l + 1));
+  keys[h] = ((uint64_t)(rows_max - rows) << 32) | (uint32_t)h;
+}
+
+void dp_order_keys(const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l, int rows_max, uint64_t* keys,
+                   cudaStream_t st) {
   if (n_hits <= 0) return;
-  DpKernelArgs a{t, q, hk, hq, hs, n_hits, p, o};
+  k_dp_order_keys<<<blocks_for(n_hits, 256), 256, 0, st>>>(hs, q_len, n_hits, l, rows_max, keys);
+  CLAST_LAUNCHED();
+}
+
+void banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq, const int32_t* hs,
+               const uint64_t* order, int64_t n_hits, const DpParams& p, const DpOut& o, cudaStream_t st) {
+  if (n_hits <= 0) return;
+  DpKernelArgs a{t, q, hk, hq, hs, order, n_hits, p, o};
   const bool local = p.local != 0;
   switch (p.gap) {
     case 2: launch_dp_gap<2>(a, local, st); break;

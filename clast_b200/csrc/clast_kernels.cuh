@@ -108,8 +108,15 @@ struct DpParams {
   int l, stride, gap, local;
   double cutoff, total_db, K, lambda;
 };
+// order (may be null): the hits in the order the threads take them, as words
+// whose low 32 bits are hit indices; outputs stay at the hit's own index.
 void banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq,
-               const int32_t* hs, int64_t n_hits, const DpParams& p, const DpOut& o, cudaStream_t st);
+               const int32_t* hs, const uint64_t* order, int64_t n_hits, const DpParams& p, const DpOut& o,
+               cudaStream_t st);
+// keys[h] = (rows_max - rows of hit h) << 32 | h, rows = q_len[hs[h]] - l + 1:
+// ascending keys take the hits longest first.
+void dp_order_keys(const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l, int rows_max, uint64_t* keys,
+                   cudaStream_t st);
 
 // ---- per-read result order and duplicate removal (utilResultSorting.cuh, CDeviceHitList.cu:32-128) ----
 void final_keys(const uint64_t* hk, const int32_t* hq, const int32_t* hs, const DpOut& o, int64_t n_hits,

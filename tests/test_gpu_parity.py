@@ -86,3 +86,16 @@ def test_empty_query_hits(engine):
     s, tl, ql = make_case(80, decoy_frac=1.0)
     got, want = run_pair(engine, s, tl, ql)
     compare(got, want)
+
+
+@pytest.mark.parametrize("local", [0, 1])
+def test_uneven_read_lengths(engine, local):
+    # log-uniform read lengths 50 bp - 4 kbp with per-read error rates 1-12 %
+    # (the batched uneven-reads shape, scaled down for the oracle)
+    s, tl, ql = make_case(61 + local, target_bp=300_000, n_contigs=4, n_reads=50,
+                          setting=api.Setting(local=local), log_uniform=(50, 4000), err_range=(0.01, 0.12),
+                          decoy_frac=0.0)
+    assert max(ql.lengths) > 1000 and min(ql.lengths) < 200
+    got, want = run_pair(engine, s, tl, ql)
+    assert len(want["t_id"]) > 20
+    compare(got, want)
