@@ -217,7 +217,9 @@ namespace {
 
 // CDeviceHashTable::CDeviceHashTable (CDeviceHashTable.cu:143-174) for the
 // window whose padded bases are already in ix->bases.
-void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix) {
+// *failed (zeroed by the caller, read once all windows are queued) counts
+// table records that fell outside the table.
+void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix, unsigned long long* failed) {
   cudaStream_t st = c->st;
   Workspace& ws = c->ws;
   const int l = p->lmer;
@@ -249,76 +251,69 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix) {
     keys = in_alt ? items2 : items;
     vals = in_alt ? pos2 : pos;
   }
-  int64_t* scal = ws.get<int64_t>("ix_scalar", 4);
-  int64_t nv = 0;
-  if (ns > 0) {
-    count_below(keys, ns, 1ull << (2 * l), scal, st);
-    nv = read_scalar(scal, st);
-  }
-  int32_t* head = ws.get<int32_t>("ix_head", nv);
-  int64_t* hpos = ws.get<int64_t>("ix_hpos", nv + 1);
-  index_heads(keys, nv, head, st);
-  scan_i32(ws, head, nv, hpos, st);
-  const int64_t nu = read_scalar(hpos + nv, st);
-  ix->n_unique = nu;
-  uint64_t* ukeys = ws.get<uint64_t>("ix_ukeys", nu);
-  int64_t* ufirst = ws.get<int64_t>("ix_ufirst", nu + 1);
-  index_unique(keys, head, hpos, nv, ukeys, ufirst, st);
-  int32_t* keep = ws.get<int32_t>("ix_keep", nv);
-  int2* resolved = ws.get<int2>("ix_resolved", nv);
-  int64_t* kpos = ws.get<int64_t>("ix_kpos", nv + 1);
-  index_keep(vals, hpos, ufirst, nv, p->stride, l, p->cut_repeat, ix->gateway.p, ix->lengths.p, ix->nseqs, keep,
-             resolved, st);
-  scan_i32(ws, keep, nv, kpos, st);
-  const int64_t ne = read_scalar(kpos + nv, st);
-  ix->n_entries = ne;
-  ix->entries.alloc(ne);
-  index_entries(keep, kpos, resolved, nv, ix->entries.p, st);
-  int32_t* ustart = ws.get<int32_t>("ix_ustart", nu);
-  int32_t* ucnt = ws.get<int32_t>("ix_ucnt", nu);
-  index_buckets(ufirst, kpos, nu, ustart, ucnt, st);
-  // Hash table: buckets of two records, at most half of the records used (one
-  // record per unique key is an upper bound on the keys that keep entries):
-  // 84 % of the keys then sit in their home bucket
-  const int64_t nb = std::max<int64_t>(1, nu);
-  if (nb >= (int64_t)UINT32_MAX) throw std::invalid_argument("window has too many distinct l-mers");
+  // From here on no host synchronisation: every array is sized for the ns
+  // samples (an upper bound of the valid samples nv, the unique keys nu and
+  // the entries); nv = *nv_dev and nu = hpos[ns] stay on the device.
+  int64_t* nv_dev = ws.get<int64_t>("ix_nv", 1);
+  if (ns > 0) count_below(keys, ns, 1ull << (2 * l), nv_dev, st);
+  else CLAST_CK(cudaMemsetAsync(nv_dev, 0, sizeof(int64_t), st));
+  int32_t* head = ws.get<int32_t>("ix_head", ns);
+  int64_t* hpos = ws.get<int64_t>("ix_hpos", ns + 1);
+  index_heads(keys, ns, nv_dev, head, st);
+  scan_i32(ws, head, ns, hpos, st);
+  const int64_t* nu_dev = hpos + ns;
+  uint64_t* ukeys = ws.get<uint64_t>("ix_ukeys", ns);
+  int64_t* ufirst = ws.get<int64_t>("ix_ufirst", ns + 1);
+  index_unique(keys, head, hpos, ns, nv_dev, ukeys, ufirst, st);
+  int32_t* keep = ws.get<int32_t>("ix_keep", ns);
+  int2* resolved = ws.get<int2>("ix_resolved", ns);
+  int64_t* kpos = ws.get<int64_t>("ix_kpos", ns + 1);
+  index_keep(vals, hpos, ufirst, ns, nv_dev, p->stride, l, p->cut_repeat, ix->gateway.p, ix->lengths.p, ix->nseqs,
+             keep, resolved, st);
+  scan_i32(ws, keep, ns, kpos, st);
+  ix->entries.alloc(ns);
+  index_entries(keep, kpos, resolved, ns, ix->entries.p, st);
+  int32_t* ustart = ws.get<int32_t>("ix_ustart", ns);
+  int32_t* ucnt = ws.get<int32_t>("ix_ucnt", ns);
+  index_buckets(ufirst, kpos, ns, nu_dev, ustart, ucnt, st);
+  // Hash table: buckets of two records, one bucket per sample, so at most half
+  // of the records are used (84 % of the keys then sit in their home bucket),
+  // plus a tail for the probe run past the last bucket
+  const int64_t nb = std::max<int64_t>(1, ns);
+  if (nb >= (int64_t)UINT32_MAX) throw std::invalid_argument("window has too many sampled l-mers");
   ix->nbuckets = (uint32_t)nb;
-  int32_t* kept = ws.get<int32_t>("ix_kept", nu);
-  int64_t* rank = ws.get<int64_t>("ix_rank", nu + 1);
-  table_kept(ucnt, nu, kept, st);
-  scan_i32(ws, kept, nu, rank, st);
-  const int64_t nk = read_scalar(rank + nu, st);
-  int64_t* slack = ws.get<int64_t>("ix_slack", nk);
-  int64_t* run_max = ws.get<int64_t>("ix_runmax", nk);
-  table_slack(ukeys, ucnt, rank, nu, l, ix->nbuckets, slack, st);
-  maxscan_i64(ws, slack, nk, run_max, st);
-  // the last kept code sits at nk - 1 + run_max[nk - 1]; one free record after it
-  const int64_t last = nk > 0 ? nk - 1 + read_scalar(run_max + nk - 1, st) : -1;
-  ix->n_records = std::max<int64_t>(2 * nb, last + 2);
+  int32_t* kept = ws.get<int32_t>("ix_kept", ns);
+  int64_t* rank = ws.get<int64_t>("ix_rank", ns + 1);
+  table_kept(ucnt, ns, kept, st);
+  scan_i32(ws, kept, ns, rank, st);
+  int64_t* slack = ws.get<int64_t>("ix_slack", ns);
+  int64_t* run_max = ws.get<int64_t>("ix_runmax", ns);
+  // past the kept codes the slack stays far below any home record (0x80... bytes)
+  CLAST_CK(cudaMemsetAsync(slack, 0x80, (size_t)std::max<int64_t>(ns, 1) * sizeof(int64_t), st));
+  table_slack(ukeys, ucnt, rank, ns, l, ix->nbuckets, slack, st);
+  maxscan_i64(ws, slack, ns, run_max, st);
+  ix->n_records = 2 * nb + (1 << 16);
   ix->table.alloc((size_t)ix->n_records);
   CLAST_CK(cudaMemsetAsync(ix->table.p, 0xff, (size_t)ix->n_records * sizeof(ulonglong2), st));
-  // Bloom filter: about 24 bits per key, between 2^12 and 2^F bits; F = 28
+  // Bloom filter: about 24 bits per sample, between 2^12 and 2^F bits; F = 28
   // (32 MB, L2-resident next to the streams that pass through L2 while
   // seeding) unless CLAST_FILTER_BITS says otherwise (16..32)
   int fbits = 28;
   if (const char* e = std::getenv("CLAST_FILTER_BITS")) fbits = std::max(16, std::min(32, std::atoi(e)));
   int bits = 12;
-  while (bits < fbits && (1ll << bits) < nk * 24) ++bits;
+  while (bits < fbits && (1ll << bits) < ns * 24) ++bits;
   ix->fshift = 64 - (bits - 5);
   ix->filter.alloc((size_t)1 << (bits - 5));
   CLAST_CK(cudaMemsetAsync(ix->filter.p, 0, ((size_t)1 << (bits - 5)) * sizeof(uint32_t), st));
-  unsigned long long* failed = reinterpret_cast<unsigned long long*>(ws.get<int64_t>("ix_failed", 1));
-  CLAST_CK(cudaMemsetAsync(failed, 0, sizeof(unsigned long long), st));
-  table_place(ukeys, ustart, ucnt, ix->entries.p, rank, run_max, nu, ix->table.p, ix->n_records, ix->filter.p,
+  table_place(ukeys, ustart, ucnt, ix->entries.p, rank, run_max, ns, ix->table.p, ix->n_records, ix->filter.p,
               ix->fshift, failed, st);
-  if (read_scalar(reinterpret_cast<int64_t*>(failed), st) != 0) throw std::runtime_error("index table overflow");
-  ix->n_keys = nk;
+  ix->n_keys = ns;
 }
 
 // Index of a window whose padded base array is already on the device.
 clast_index* make_index_resident(clast_ctx* c, const clast_params* p, DevArray<char>&& padded, int64_t n_bases,
                                  DevArray<int32_t>&& gateway, DevArray<int32_t>&& lengths, int32_t n_seqs,
-                                 int32_t t_begin) {
+                                 int32_t t_begin, unsigned long long* failed) {
   std::unique_ptr<clast_index> ix(new clast_index());
   ix->l = p->lmer;
   ix->stride = p->stride;
@@ -329,7 +324,7 @@ clast_index* make_index_resident(clast_ctx* c, const clast_params* p, DevArray<c
   ix->bases = std::move(padded);
   ix->gateway = std::move(gateway);
   ix->lengths = std::move(lengths);
-  build_index_device(c, p, ix.get());
+  build_index_device(c, p, ix.get(), failed);
   return ix.release();
 }
 
@@ -350,17 +345,20 @@ clast_index* make_index(clast_ctx* c, const clast_params* p, const char* bases, 
   }
   CLAST_CK(cudaEventRecord(c->ev1, c->st));
   const int64_t k0 = g_kernel_launches;
-  clast_index* ix = make_index_resident(c, p, std::move(padded), n_bases, std::move(gw), std::move(ln), n_seqs,
-                                        t_begin);
+  unsigned long long* failed = reinterpret_cast<unsigned long long*>(c->ws.get<int64_t>("ix_failed", 1));
+  CLAST_CK(cudaMemsetAsync(failed, 0, sizeof(unsigned long long), c->st));
+  std::unique_ptr<clast_index> ix(make_index_resident(c, p, std::move(padded), n_bases, std::move(gw), std::move(ln),
+                                                      n_seqs, t_begin, failed));
   CLAST_CK(cudaEventRecord(c->ev2, c->st));
   CLAST_CK(cudaEventSynchronize(c->ev2));
+  if (read_scalar(reinterpret_cast<int64_t*>(failed), c->st) != 0) throw std::runtime_error("index table overflow");
   float up = 0, bd = 0;
   CLAST_CK(cudaEventElapsedTime(&up, c->ev0, c->ev1));
   CLAST_CK(cudaEventElapsedTime(&bd, c->ev1, c->ev2));
   c->stats.index_upload_ms += up;
   c->stats.index_ms += bd;
   c->stats.index_launches += g_kernel_launches - k0;
-  return ix;
+  return ix.release();
 }
 
 // Device-resident query strands of one batch, packed once for every index.
@@ -779,14 +777,20 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
       src = traw.p;
     }
     CLAST_CK(cudaEventRecord(ctx->ev1, st));
-    CLAST_CK(cudaEventSynchronize(ctx->ev1));
-    float up = 0;
-    CLAST_CK(cudaEventElapsedTime(&up, ctx->ev0, ctx->ev1));
-    ctx->stats.index_upload_ms += up;
+    // the windows are indexed back to back on the stream with no host
+    // synchronisation; the table-overflow flag is read once at the end
+    unsigned long long* failed = reinterpret_cast<unsigned long long*>(ctx->ws.get<int64_t>("ix_failed", 1));
+    CLAST_CK(cudaMemsetAsync(failed, 0, sizeof(unsigned long long), st));
+    const int64_t k0 = g_kernel_launches;
     const int64_t base0 = nt ? targets->offsets[0] : 0;
-    int64_t rec = 0;
+    // the windows of every load (moveTargetWindow, CHostSchedular.cu:25-35) and
+    // their sequence tables, planned on the host and uploaded in one go: a copy
+    // from pageable memory waits for the stream, so none happens per window
+    struct Plan { int32_t load, first, nseqs; int64_t n, meta; };
+    std::vector<Plan> plan;
     std::vector<int32_t> gw, ln;
     std::vector<int64_t> so;
+    int64_t rec = 0;
     for (int32_t k = 0; k < n_loads; ++k) {
       const int64_t r0 = rec, r1 = rec + load_sizes[k];
       rec = r1;
@@ -795,47 +799,54 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
       for (int64_t i = r0; i < r1; ++i)
         lg[i - r0 + 1] = lg[i - r0] + (targets->offsets[i + 1] - targets->offsets[i]) + (l - 1);
       const int64_t tEnd = r1 - r0;
-      for (int64_t tb = 0, te = 1; tb < tEnd; tb = te++) {  // moveTargetWindow, CHostSchedular.cu:25-35
+      for (int64_t tb = 0, te = 1; tb < tEnd; tb = te++) {
         while (te < tEnd && lg[te + 1] - lg[tb] < (int64_t)t_vram) ++te;
         const int64_t wn = lg[te] - lg[tb];
         if (wn >= (int64_t)INT32_MAX) throw std::invalid_argument("target window larger than 2^31 bases");
-        gw.clear();
-        ln.clear();
-        so.clear();
+        plan.push_back(Plan{k, (int32_t)tb, (int32_t)(te - tb), wn, (int64_t)gw.size()});
         for (int64_t i = r0 + tb; i < r0 + te; ++i) {
           gw.push_back((int32_t)(lg[i - r0] - lg[tb]));
           ln.push_back((int32_t)(targets->offsets[i + 1] - targets->offsets[i]));
           so.push_back(targets->offsets[i] - base0);
         }
-        const int32_t wseqs = (int32_t)gw.size();
-        DevArray<char> padded;
-        DevArray<int32_t> dgw, dln;
-        DevArray<int64_t> dso;
-        padded.alloc((size_t)wn + 2 * kPad);
-        dgw.alloc(wseqs);
-        dln.alloc(wseqs);
-        dso.alloc(wseqs);
-        CLAST_CK(cudaEventRecord(ctx->ev1, st));
-        const int64_t k0 = g_kernel_launches;
-        CLAST_CK(cudaMemcpyAsync(dgw.p, gw.data(), wseqs * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-        CLAST_CK(cudaMemcpyAsync(dln.p, ln.data(), wseqs * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-        CLAST_CK(cudaMemcpyAsync(dso.p, so.data(), wseqs * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-        CLAST_CK(cudaMemsetAsync(padded.p, 'N', (size_t)wn + 2 * kPad, st));
-        build_window(src, dso.p, dgw.p, dln.p, wseqs, wn, padded.p + kPad, st);
-        clast_targets::Win w;
-        w.load = k;
-        w.first = (int32_t)tb;
-        w.ix.reset(make_index_resident(ctx, p, std::move(padded), wn, std::move(dgw), std::move(dln), wseqs,
-                                       (int32_t)tb));
-        CLAST_CK(cudaEventRecord(ctx->ev2, st));
-        CLAST_CK(cudaEventSynchronize(ctx->ev2));
-        float bd = 0;
-        CLAST_CK(cudaEventElapsedTime(&bd, ctx->ev1, ctx->ev2));
-        ctx->stats.index_ms += bd;
-        ctx->stats.index_launches += g_kernel_launches - k0;
-        T->wins.push_back(std::move(w));
       }
     }
+    DevArray<int32_t> all_gw, all_ln;
+    DevArray<int64_t> all_so;
+    all_gw.alloc(gw.size());
+    all_ln.alloc(ln.size());
+    all_so.alloc(so.size());
+    if (!gw.empty()) {
+      CLAST_CK(cudaMemcpyAsync(all_gw.p, gw.data(), gw.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+      CLAST_CK(cudaMemcpyAsync(all_ln.p, ln.data(), ln.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+      CLAST_CK(cudaMemcpyAsync(all_so.p, so.data(), so.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    }
+    for (const Plan& w : plan) {
+      DevArray<char> padded;
+      DevArray<int32_t> dgw, dln;
+      padded.alloc((size_t)w.n + 2 * kPad);
+      dgw.alloc(w.nseqs);
+      dln.alloc(w.nseqs);
+      CLAST_CK(cudaMemcpyAsync(dgw.p, all_gw.p + w.meta, w.nseqs * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+      CLAST_CK(cudaMemcpyAsync(dln.p, all_ln.p + w.meta, w.nseqs * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+      CLAST_CK(cudaMemsetAsync(padded.p, 'N', (size_t)w.n + 2 * kPad, st));
+      build_window(src, all_so.p + w.meta, dgw.p, dln.p, w.nseqs, w.n, padded.p + kPad, st);
+      clast_targets::Win win;
+      win.load = w.load;
+      win.first = w.first;
+      win.ix.reset(make_index_resident(ctx, p, std::move(padded), w.n, std::move(dgw), std::move(dln), w.nseqs,
+                                       w.first, failed));
+      T->wins.push_back(std::move(win));
+    }
+    CLAST_CK(cudaEventRecord(ctx->ev2, st));
+    CLAST_CK(cudaEventSynchronize(ctx->ev2));
+    if (read_scalar(reinterpret_cast<int64_t*>(failed), st) != 0) throw std::runtime_error("index table overflow");
+    float up = 0, bd = 0;
+    CLAST_CK(cudaEventElapsedTime(&up, ctx->ev0, ctx->ev1));
+    CLAST_CK(cudaEventElapsedTime(&bd, ctx->ev1, ctx->ev2));
+    ctx->stats.index_upload_ms += up;
+    ctx->stats.index_ms += bd;
+    ctx->stats.index_launches += g_kernel_launches - k0;
     ctx->stats.index_wall_ms = wall_ms() - w0;
     *out = T.release();
     return CLAST_OK;

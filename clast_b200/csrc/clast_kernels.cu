@@ -353,16 +353,22 @@ __global__ void k_count_below(const uint64_t* __restrict__ keys, int64_t n, uint
   *out = lo;
 }
 
-__global__ void k_index_heads(const uint64_t* __restrict__ k, int64_t nv, int32_t* __restrict__ head) {
+// The index build runs without host synchronisation: kernels cover the n
+// samples (an upper bound) and read the counts that matter from the device
+// (*nv valid samples; *nu = hpos[n] unique keys, as the scans end with the
+// total and every flag past the valid range is 0).
+__global__ void k_index_heads(const uint64_t* __restrict__ k, int64_t n, const int64_t* __restrict__ nv_dev,
+                              int32_t* __restrict__ head) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nv) head[i] = (i == 0 || k[i] != k[i - 1]) ? 1 : 0;
+  if (i < n) head[i] = (i < *nv_dev && (i == 0 || k[i] != k[i - 1])) ? 1 : 0;
 }
 
 __global__ void k_index_unique(const uint64_t* __restrict__ k, const int32_t* __restrict__ head,
-                               const int64_t* __restrict__ hpos, int64_t nv, uint64_t* __restrict__ ukeys,
-                               int64_t* __restrict__ ufirst) {
+                               const int64_t* __restrict__ hpos, int64_t n, const int64_t* __restrict__ nv_dev,
+                               uint64_t* __restrict__ ukeys, int64_t* __restrict__ ufirst) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nv && head[i]) {
+  const int64_t nv = *nv_dev;
+  if (i < n && head[i]) {
     ukeys[hpos[i]] = k[i];
     ufirst[hpos[i]] = i;
   }
@@ -370,11 +376,16 @@ __global__ void k_index_unique(const uint64_t* __restrict__ k, const int32_t* __
 }
 
 __global__ void k_index_keep(const int32_t* __restrict__ vals, const int64_t* __restrict__ hpos,
-                             const int64_t* __restrict__ ufirst, int64_t nv, int stride, int l, int cut,
-                             const int32_t* __restrict__ gw, const int32_t* __restrict__ len, int nseqs,
-                             int32_t* __restrict__ keep, int2* __restrict__ resolved) {
+                             const int64_t* __restrict__ ufirst, int64_t n, const int64_t* __restrict__ nv_dev,
+                             int stride, int l, int cut, const int32_t* __restrict__ gw,
+                             const int32_t* __restrict__ len, int nseqs, int32_t* __restrict__ keep,
+                             int2* __restrict__ resolved) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nv) return;
+  if (i >= n) return;
+  if (i >= *nv_dev) {
+    keep[i] = 0;
+    return;
+  }
   const int64_t u = hpos[i + 1] - 1;
   const int64_t cnt = ufirst[u + 1] - ufirst[u];
   const bool pass = (cut == -1) || (cnt < (int64_t)cut);  // removeRepeatedSequence
@@ -392,15 +403,20 @@ __global__ void k_index_keep(const int32_t* __restrict__ vals, const int64_t* __
 }
 
 __global__ void k_index_entries(const int32_t* __restrict__ keep, const int64_t* __restrict__ kpos,
-                                const int2* __restrict__ resolved, int64_t nv, int2* __restrict__ entries) {
+                                const int2* __restrict__ resolved, int64_t n, int2* __restrict__ entries) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nv && keep[i]) entries[kpos[i]] = resolved[i];
+  if (i < n && keep[i]) entries[kpos[i]] = resolved[i];
 }
 
 __global__ void k_index_buckets(const int64_t* __restrict__ ufirst, const int64_t* __restrict__ kpos,
-                                int64_t nu, int32_t* __restrict__ ustart, int32_t* __restrict__ ucnt) {
+                                int64_t n, const int64_t* __restrict__ nu_dev, int32_t* __restrict__ ustart,
+                                int32_t* __restrict__ ucnt) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nu) return;
+  if (k >= n) return;
+  if (k >= *nu_dev) {
+    ucnt[k] = 0;
+    return;
+  }
   const int64_t a = kpos[ufirst[k]], b = kpos[ufirst[k + 1]];
   ustart[k] = (int32_t)a;
   ucnt[k] = (int32_t)(b - a);
@@ -411,16 +427,16 @@ __global__ void k_index_buckets(const int64_t* __restrict__ ufirst, const int64_
 // r = rank among the kept codes, linear probing puts code r at
 // max(home_r, pos_{r-1} + 1) = r + max_{j <= r}(home_j - j).
 
-__global__ void k_table_kept(const int32_t* __restrict__ ucnt, int64_t nu, int32_t* __restrict__ kept) {
+__global__ void k_table_kept(const int32_t* __restrict__ ucnt, int64_t n, int32_t* __restrict__ kept) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < nu) kept[k] = ucnt[k] > 0 ? 1 : 0;  // 0: removed by the repeat cut, or joints only
+  if (k < n) kept[k] = ucnt[k] > 0 ? 1 : 0;  // 0: removed by the repeat cut, joints only, or past the keys
 }
 
 __global__ void k_table_slack(const uint64_t* __restrict__ ucode, const int32_t* __restrict__ ucnt,
-                              const int64_t* __restrict__ rank, int64_t nu, int l, uint32_t nbuckets,
+                              const int64_t* __restrict__ rank, int64_t n, int l, uint32_t nbuckets,
                               int64_t* __restrict__ slack) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nu || ucnt[k] <= 0) return;
+  if (k >= n || ucnt[k] <= 0) return;
   slack[rank[k]] = record_home(ucode[k], l, nbuckets) - rank[k];
 }
 
@@ -1701,22 +1717,22 @@ void count_below(const uint64_t* keys, int64_t n, uint64_t bound, int64_t* out, 
   CLAST_LAUNCHED();
 }
 
-void index_heads(const uint64_t* keys, int64_t nv, int32_t* head, cudaStream_t st) {
-  if (nv <= 0) return;
-  k_index_heads<<<blocks_for(nv, 256), 256, 0, st>>>(keys, nv, head);
+void index_heads(const uint64_t* keys, int64_t n, const int64_t* nv_dev, int32_t* head, cudaStream_t st) {
+  if (n <= 0) return;
+  k_index_heads<<<blocks_for(n, 256), 256, 0, st>>>(keys, n, nv_dev, head);
   CLAST_LAUNCHED();
 }
-void index_unique(const uint64_t* keys, const int32_t* head, const int64_t* hpos, int64_t nv, uint64_t* ukeys,
-                  int64_t* ufirst, cudaStream_t st) {
-  k_index_unique<<<blocks_for(nv > 0 ? nv : 1, 256), 256, 0, st>>>(keys, head, hpos, nv, ukeys, ufirst);
+void index_unique(const uint64_t* keys, const int32_t* head, const int64_t* hpos, int64_t n, const int64_t* nv_dev,
+                  uint64_t* ukeys, int64_t* ufirst, cudaStream_t st) {
+  k_index_unique<<<blocks_for(n > 0 ? n : 1, 256), 256, 0, st>>>(keys, head, hpos, n, nv_dev, ukeys, ufirst);
   CLAST_LAUNCHED();
 }
-void index_keep(const int32_t* vals, const int64_t* hpos, const int64_t* ufirst, int64_t nv, int stride, int l,
-                int cut, const int32_t* gateway, const int32_t* lengths, int nseqs, int32_t* keep, int2* resolved,
-                cudaStream_t st) {
-  if (nv <= 0) return;
-  k_index_keep<<<blocks_for(nv, 256), 256, 0, st>>>(vals, hpos, ufirst, nv, stride, l, cut, gateway, lengths,
-                                                    nseqs, keep, resolved);
+void index_keep(const int32_t* vals, const int64_t* hpos, const int64_t* ufirst, int64_t n, const int64_t* nv_dev,
+                int stride, int l, int cut, const int32_t* gateway, const int32_t* lengths, int nseqs, int32_t* keep,
+                int2* resolved, cudaStream_t st) {
+  if (n <= 0) return;
+  k_index_keep<<<blocks_for(n, 256), 256, 0, st>>>(vals, hpos, ufirst, n, nv_dev, stride, l, cut, gateway, lengths,
+                                                   nseqs, keep, resolved);
   CLAST_LAUNCHED();
 }
 void index_entries(const int32_t* keep, const int64_t* kpos, const int2* resolved, int64_t nv, int2* entries,
@@ -1725,10 +1741,10 @@ void index_entries(const int32_t* keep, const int64_t* kpos, const int2* resolve
   k_index_entries<<<blocks_for(nv, 256), 256, 0, st>>>(keep, kpos, resolved, nv, entries);
   CLAST_LAUNCHED();
 }
-void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n_unique, int32_t* ustart, int32_t* ucnt,
-                   cudaStream_t st) {
-  if (n_unique <= 0) return;
-  k_index_buckets<<<blocks_for(n_unique, 256), 256, 0, st>>>(ufirst, kpos, n_unique, ustart, ucnt);
+void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n, const int64_t* nu_dev, int32_t* ustart,
+                   int32_t* ucnt, cudaStream_t st) {
+  if (n <= 0) return;
+  k_index_buckets<<<blocks_for(n, 256), 256, 0, st>>>(ufirst, kpos, n, nu_dev, ustart, ucnt);
   CLAST_LAUNCHED();
 }
 

@@ -43,15 +43,17 @@ int radix_sort_u64(Workspace& ws, uint64_t* keys, int32_t* vals, uint64_t* keys_
                    int lo_bit, int hi_bit, cudaStream_t st);
 // *out = number of keys < bound in the sorted array keys[0..n)
 void count_below(const uint64_t* keys, int64_t n, uint64_t bound, int64_t* out, cudaStream_t st);
-void index_heads(const uint64_t* keys, int64_t nv, int32_t* head, cudaStream_t st);
-void index_unique(const uint64_t* keys, const int32_t* head, const int64_t* hpos, int64_t nv,
+// Index build over n samples with the valid count *nv_dev and the unique
+// count *nu_dev on the device (no host synchronisation).
+void index_heads(const uint64_t* keys, int64_t n, const int64_t* nv_dev, int32_t* head, cudaStream_t st);
+void index_unique(const uint64_t* keys, const int32_t* head, const int64_t* hpos, int64_t n, const int64_t* nv_dev,
                   uint64_t* ukeys, int64_t* ufirst, cudaStream_t st);
-void index_keep(const int32_t* vals, const int64_t* hpos, const int64_t* ufirst, int64_t nv, int stride,
-                int l, int cut, const int32_t* gateway, const int32_t* lengths, int nseqs,
-                int32_t* keep, int2* resolved, cudaStream_t st);
+void index_keep(const int32_t* vals, const int64_t* hpos, const int64_t* ufirst, int64_t n, const int64_t* nv_dev,
+                int stride, int l, int cut, const int32_t* gateway, const int32_t* lengths, int nseqs, int32_t* keep,
+                int2* resolved, cudaStream_t st);
 void index_entries(const int32_t* keep, const int64_t* kpos, const int2* resolved, int64_t nv,
                    int2* entries, cudaStream_t st);
-void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n_unique, int32_t* ustart,
+void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n, const int64_t* nu_dev, int32_t* ustart,
                    int32_t* ucnt, cudaStream_t st);
 // Hash table of the index without atomics (layout: IndexView).  kept[k] =
 // whether unique code k keeps entries; rank = exclusive scan of kept;
