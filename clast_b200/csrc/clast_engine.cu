@@ -578,6 +578,18 @@ struct clast_targets {
   };
   std::vector<Win> wins;
   int32_t n_loads = 0;
+  // The index builds run on the context's stream after clast_targets_create
+  // returns; the first clast_map waits for them, reads the overflow count and
+  // the build time (events) and reports either.
+  DevArray<unsigned long long> failed;
+  cudaEvent_t ev_start = nullptr, ev_up = nullptr, ev_done = nullptr;  // from the context's event pool
+  mutable bool settled = false;
+  int64_t launches = 0;
+  ~clast_targets() {
+    if (ev_done) cudaEventSynchronize(ev_done);
+    for (cudaEvent_t e : {ev_start, ev_up, ev_done})
+      if (e) ctx->timer.pool.push_back(e);
+  }
 };
 
 namespace {
@@ -765,21 +777,25 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
     T->ctx = ctx;
     T->n_loads = n_loads;
     cudaStream_t st = ctx->st;
+    T->ev_start = ctx->timer.take();
+    T->ev_up = ctx->timer.take();
+    T->ev_done = ctx->timer.take();
+    T->failed.alloc(1);
     // the raw target set on the device, uploaded once unless already resident
     const int64_t nt = targets->n_seqs;
     const int64_t tbytes = nt ? targets->offsets[nt] - targets->offsets[0] : 0;
     DevArray<char> traw;
     const char* src = targets->bases + (nt ? targets->offsets[0] : 0);
-    CLAST_CK(cudaEventRecord(ctx->ev0, st));
+    CLAST_CK(cudaEventRecord(T->ev_start, st));
     if (!targets->bases_on_device) {
       traw.alloc((size_t)tbytes + 1);
       if (tbytes) CLAST_CK(cudaMemcpyAsync(traw.p, src, (size_t)tbytes, cudaMemcpyHostToDevice, st));
       src = traw.p;
     }
-    CLAST_CK(cudaEventRecord(ctx->ev1, st));
+    CLAST_CK(cudaEventRecord(T->ev_up, st));
     // the windows are indexed back to back on the stream with no host
-    // synchronisation; the table-overflow flag is read once at the end
-    unsigned long long* failed = reinterpret_cast<unsigned long long*>(ctx->ws.get<int64_t>("ix_failed", 1));
+    // synchronisation; the table-overflow count is read by the first clast_map
+    unsigned long long* failed = T->failed.p;
     CLAST_CK(cudaMemsetAsync(failed, 0, sizeof(unsigned long long), st));
     const int64_t k0 = g_kernel_launches;
     const int64_t base0 = nt ? targets->offsets[0] : 0;
@@ -838,15 +854,10 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
                                        w.first, failed));
       T->wins.push_back(std::move(win));
     }
-    CLAST_CK(cudaEventRecord(ctx->ev2, st));
-    CLAST_CK(cudaEventSynchronize(ctx->ev2));
-    if (read_scalar(reinterpret_cast<int64_t*>(failed), st) != 0) throw std::runtime_error("index table overflow");
-    float up = 0, bd = 0;
-    CLAST_CK(cudaEventElapsedTime(&up, ctx->ev0, ctx->ev1));
-    CLAST_CK(cudaEventElapsedTime(&bd, ctx->ev1, ctx->ev2));
-    ctx->stats.index_upload_ms += up;
-    ctx->stats.index_ms += bd;
-    ctx->stats.index_launches += g_kernel_launches - k0;
+    CLAST_CK(cudaEventRecord(T->ev_done, st));
+    T->launches = g_kernel_launches - k0;
+    // a host source must stay readable until its copy has been made
+    if (!targets->bases_on_device) CLAST_CK(cudaEventSynchronize(T->ev_up));
     ctx->stats.index_wall_ms = wall_ms() - w0;
     *out = T.release();
     return CLAST_OK;
@@ -941,6 +952,19 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     build_strands(rsrc, doff.p, nreads, nb, qb.bases.p + kPad, qb.start.p, qb.len.p, st);
     qb.pack(st);
     S.query_bases = qb.n;
+    // the index builds of clast_targets_create end before the first search
+    if (!T->settled) {
+      CLAST_CK(cudaEventSynchronize(T->ev_done));
+      T->settled = true;
+      float up = 0, bd = 0;
+      CLAST_CK(cudaEventElapsedTime(&up, T->ev_start, T->ev_up));
+      CLAST_CK(cudaEventElapsedTime(&bd, T->ev_up, T->ev_done));
+      S.index_upload_ms = up;
+      S.index_ms = bd;
+      S.index_launches = T->launches;
+      if (read_scalar(reinterpret_cast<const int64_t*>(T->failed.p), st) != 0)
+        throw std::runtime_error("index table overflow");
+    }
     // every target window, in holder order (target load, window)
     std::vector<DevHits> per_win(T->wins.size());
     for (size_t w = 0; w < T->wins.size(); ++w) search_batch(ctx, T->wins[w].ix.get(), p, qb, 0, per_win[w]);

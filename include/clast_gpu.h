@@ -143,7 +143,11 @@ typedef struct clast_seqs {
 /* Builds and keeps in HBM the index of every target window.  The target
  * records are split into RAM loads (load_sizes[k] records each, in order, as
  * CFASTALoader hands them out) and each load into windows by the rule of
- * moveTargetWindow (CHostSchedular.cu:25-35) with budget t_vram (bases). */
+ * moveTargetWindow (CHostSchedular.cu:25-35) with budget t_vram (bases).
+ * The index builds are queued on the context's stream and run after the
+ * call returns (it waits only for the copy of host-resident bases); the first
+ * clast_map on the targets waits for them and reports an index failure, and
+ * clast_get_stats shows their times from then on. */
 int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram,
                          const clast_seqs* targets, int32_t n_loads, const int64_t* load_sizes,
                          clast_targets** out);
@@ -185,8 +189,9 @@ void clast_map_result_free(clast_map_result* r);
  * copies on the context's stream), and how many kernels it launched. */
 int clast_last_map_stats(const clast_ctx* ctx, double* device_ms, int64_t* kernel_launches);
 
-/* Measurements of the last clast_targets_create and clast_map calls, taken
- * with CUDA events on the context's stream.  Units: milliseconds and counts. */
+/* Measurements of the last clast_targets_create (as of the first clast_map on
+ * its targets) and clast_map calls, taken with CUDA events on the context's
+ * stream.  Units: milliseconds and counts. */
 typedef struct clast_stats {
   double index_ms;           /* index builds, target upload excluded          */
   double index_upload_ms;    /* target host-to-device copies                  */
