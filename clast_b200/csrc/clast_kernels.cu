@@ -108,27 +108,65 @@ void scan_impl(Workspace& ws, const T* in, int64_t n, int64_t* out, cudaStream_t
 // ------------------------------------------------------------------------
 // packing and query strands
 // ------------------------------------------------------------------------
+// 2-bit codes and non-ACGT flags of 8 bases (x: 8 bytes, first base in the
+// low byte), eight at a time in 64-bit words.  code = ((b >> 1) ^ (b >> 2)) & 3
+// maps A C G T to 0 1 2 3; a byte is A/C/G/T iff it equals "ACGT"[code].
+// codes16: first base in bits 15..14; bad8: first base in bit 7.
+__device__ __forceinline__ void pack8(uint64_t x, uint32_t& codes16, uint32_t& bad8) {
+  const uint64_t c = ((x >> 1) ^ (x >> 2)) & 0x0303030303030303ull;
+  const uint32_t clo = (uint32_t)c, chi = (uint32_t)(c >> 32);
+  // byte-reverse so that the first base ends in the top bits, then gather the
+  // eight 2-bit fields
+  uint64_t y = ((uint64_t)__byte_perm(clo, 0, 0x0123) << 32) | __byte_perm(chi, 0, 0x0123);
+  y = (y | (y >> 6)) & 0x000F000F000F000Full;
+  y = (y | (y >> 12)) & 0x000000FF000000FFull;
+  codes16 = (uint32_t)((y | (y >> 24)) & 0xFFFF);
+  uint32_t bad = 0;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t ch = h ? chi : clo;
+    const uint32_t sel = (ch & 3u) | ((ch >> 4) & 0x30u) | ((ch >> 8) & 0x300u) | ((ch >> 12) & 0x3000u);
+    const uint32_t d = __byte_perm(0x54474341u, 0, sel) ^ (uint32_t)(x >> (32 * h));  // "ACGT"[code] ^ byte
+    const uint32_t nz = ((((d & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | d) & 0x80808080u) >> 7;  // 1 per nonzero byte
+    bad |= ((nz * 0x08040201u) >> 24 & 0xFu) << (4 * (1 - h));                        // first byte -> bit 3
+  }
+  bad8 = bad;
+}
+
+// One 64-base word per thread: 2-bit codes (first base in the top bits, 32
+// per word) and the non-ACGT mask (first base in the top bit).  bases must be
+// 16-byte aligned with at least 63 readable bytes past n; bases at or past n
+// count as 'N'.
 __global__ void k_pack(const char* __restrict__ bases, int64_t n, uint64_t* __restrict__ packed,
                        uint64_t* __restrict__ nmask, int64_t nwords) {
   const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= nwords) return;
-  uint64_t m = 0, p0 = 0, p1 = 0;
   const int64_t f0 = w * 64;
-#pragma unroll 8
-  for (int i = 0; i < 64; ++i) {
-    const int64_t f = f0 + i;
-    const char c = (f < n) ? bases[f] : 'N';
-    uint64_t code = 0, isn = 0;
-    switch (c) {
-      case 'A': code = 0; break;
-      case 'C': code = 1; break;
-      case 'G': code = 2; break;
-      case 'T': code = 3; break;
-      default: isn = 1;
+  uint64_t m = 0, p0 = 0, p1 = 0;
+  if (f0 < n) {
+    const uint4* src = reinterpret_cast<const uint4*>(bases + f0);
+    uint64_t g[8];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const uint4 q = __ldcs(src + v);
+      g[2 * v] = ((uint64_t)q.y << 32) | q.x;
+      g[2 * v + 1] = ((uint64_t)q.w << 32) | q.z;
     }
-    m |= isn << (63 - i);
-    if (i < 32) p0 |= code << (62 - 2 * i);
-    else p1 |= code << (62 - 2 * (i - 32));
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int64_t valid = n - (f0 + 8 * k);  // bytes of this group before n
+      if (valid < 8) {
+        const uint64_t keep = valid <= 0 ? 0ull : ((1ull << (8 * valid)) - 1);
+        g[k] = (g[k] & keep) | (0x4E4E4E4E4E4E4E4Eull & ~keep);  // 'N'
+      }
+      uint32_t c16, b8;
+      pack8(g[k], c16, b8);
+      m |= (uint64_t)b8 << (56 - 8 * k);
+      if (k < 4) p0 |= (uint64_t)c16 << (48 - 16 * k);
+      else p1 |= (uint64_t)c16 << (48 - 16 * (k - 4));
+    }
+  } else {
+    m = ~0ull;
   }
   nmask[w] = m;
   packed[2 * w] = p0;
@@ -177,9 +215,10 @@ __global__ void k_strands(const char* __restrict__ reads, const int64_t* __restr
 __global__ void k_build_window(const char* __restrict__ src, const int64_t* __restrict__ src_off,
                                const int32_t* __restrict__ gw, const int32_t* __restrict__ len, int nseqs,
                                int64_t n, char* __restrict__ out) {
+  // 16 output bytes per thread, written as one 16-byte store (out is 16-byte aligned)
   __shared__ int first_seq;
-  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x;
-  if (threadIdx.x == 0) {  // sequence of the block's first base; others walk forward from it
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x * 16;
+  if (threadIdx.x == 0) {  // sequence of the block's first base; threads walk forward from it
     int lo = 0, hi = nseqs;
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
@@ -189,16 +228,34 @@ __global__ void k_build_window(const char* __restrict__ src, const int64_t* __re
     first_seq = lo;
   }
   __syncthreads();
-  const int64_t i = i0 + threadIdx.x;
-  if (i >= n) return;
+  const int64_t b0 = i0 + (int64_t)threadIdx.x * 16;
+  if (b0 >= n) return;
   int lo = first_seq;
-  while (lo + 1 < nseqs && (int64_t)gw[lo + 1] <= i) ++lo;
-  const int64_t j = i - gw[lo];
-  const int64_t L = len[lo];
-  char c;
-  if (j < L) c = src[src_off[lo] + j];
-  else c = (j - L < L) ? src[src_off[lo] + (j - L)] : 'N';
-  out[i] = c;
+  while (lo + 1 < nseqs && (int64_t)gw[lo + 1] <= b0) ++lo;
+  unsigned char c[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const int64_t i = b0 + k;
+    while (lo + 1 < nseqs && (int64_t)gw[lo + 1] <= i) ++lo;
+    const int64_t j = i - gw[lo];
+    const int64_t L = len[lo];
+    char v = 'N';
+    if (i < n) {
+      if (j < L) v = src[src_off[lo] + j];
+      else if (j - L < L) v = src[src_off[lo] + (j - L)];
+    }
+    c[k] = (unsigned char)v;
+  }
+  if (b0 + 16 <= n) {
+    uint4 q;
+    q.x = c[0] | (c[1] << 8) | (c[2] << 16) | ((uint32_t)c[3] << 24);
+    q.y = c[4] | (c[5] << 8) | (c[6] << 16) | ((uint32_t)c[7] << 24);
+    q.z = c[8] | (c[9] << 8) | (c[10] << 16) | ((uint32_t)c[11] << 24);
+    q.w = c[12] | (c[13] << 8) | (c[14] << 16) | ((uint32_t)c[15] << 24);
+    *reinterpret_cast<uint4*>(out + b0) = q;
+  } else {
+    for (int k = 0; k < 16 && b0 + k < n; ++k) out[b0 + k] = (char)c[k];
+  }
 }
 
 // ------------------------------------------------------------------------
@@ -1664,7 +1721,7 @@ void build_strands(const char* reads, const int64_t* offsets, int64_t n_reads, i
 void build_window(const char* src, const int64_t* src_off, const int32_t* gateway, const int32_t* lengths,
                   int nseqs, int64_t n, char* out, cudaStream_t st) {
   if (n <= 0 || nseqs <= 0) return;
-  k_build_window<<<blocks_for(n, 256), 256, 0, st>>>(src, src_off, gateway, lengths, nseqs, n, out);
+  k_build_window<<<blocks_for((n + 15) / 16, 256), 256, 0, st>>>(src, src_off, gateway, lengths, nseqs, n, out);
   CLAST_LAUNCHED();
 }
 
