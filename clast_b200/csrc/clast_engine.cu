@@ -90,7 +90,8 @@ struct clast_ctx {
   std::vector<std::unique_ptr<PinnedArena>> arenas;
   int device = 0;
   cudaStream_t st = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  cudaStream_t st_copy = nullptr;  // query uploads, overlapping index builds still running on st
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
   Workspace ws;
   std::string err;
   double last_ms = 0;
@@ -633,6 +634,7 @@ int clast_ctx_create(int device, clast_ctx** out) {
   if (device < 0 || device >= ndev) return CLAST_ERR_ARG;
   if (cudaSetDevice(device) != cudaSuccess) return CLAST_ERR_CUDA;
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
+  if (cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
   {  // keep freed pool memory for reuse by later calls of this process
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -642,7 +644,7 @@ int clast_ctx_create(int device, clast_ctx** out) {
     (void)cudaGetLastError();
   }
   if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaEventCreate(&c->ev2) != cudaSuccess)
+      cudaEventCreate(&c->ev2) != cudaSuccess || cudaEventCreate(&c->ev3) != cudaSuccess)
     return CLAST_ERR_CUDA;
   *out = c.release();
   return CLAST_OK;
@@ -658,6 +660,11 @@ void clast_ctx_destroy(clast_ctx* ctx) {
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->ev2) cudaEventDestroy(ctx->ev2);
+  if (ctx->ev3) cudaEventDestroy(ctx->ev3);
+  if (ctx->st_copy) {
+    cudaStreamSynchronize(ctx->st_copy);
+    cudaStreamDestroy(ctx->st_copy);
+  }
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
 }
@@ -918,11 +925,18 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
       for (int64_t i = 0; i <= nreads; ++i) off0[i] = reads->offsets[i] - reads->offsets[0];
       offs_rel = off0.data();
     }
+    // uploads go on the copy stream (allocated there, so nothing waits for the
+    // compute stream, which may still be building the target indexes); the
+    // compute stream waits for them below and frees the buffers in its order
     DevArray<char> draw;
     DevArray<int64_t> doff;
+    g_alloc_stream = ctx->st_copy;
     if (!reads->bases_on_device) draw.alloc((size_t)nb + 64);
     doff.alloc((size_t)nreads + 1);
     QueryBatch qb;
+    qb.wstart.alloc(wstart.size());
+    g_alloc_stream = st;
+    draw.st = doff.st = qb.wstart.st = st;
     qb.n = 2 * nb;
     qb.nstrands = (int32_t)(2 * nreads);
     qb.min_len = nreads ? INT32_MAX : 0;
@@ -936,18 +950,20 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     qb.start.alloc(2 * nreads);
     qb.len.alloc(2 * nreads);
     qb.nwin = (int32_t)wfirst.size() - 1;
-    qb.wstart.alloc(wstart.size());
     S.map_prep_ms = wall_ms() - w0;
-    CLAST_CK(cudaEventRecord(ctx->ev0, st));
+    cudaStream_t cs = ctx->st_copy;
+    CLAST_CK(cudaEventRecord(ctx->ev0, cs));
     const char* rsrc = reads->bases + reads->offsets[0];
     if (!reads->bases_on_device) {
-      if (nb) CLAST_CK(cudaMemcpyAsync(draw.p, rsrc, nb, cudaMemcpyHostToDevice, st));
+      if (nb) CLAST_CK(cudaMemcpyAsync(draw.p, rsrc, nb, cudaMemcpyHostToDevice, cs));
       rsrc = draw.p;
     }
-    CLAST_CK(cudaMemcpyAsync(doff.p, offs_rel, (nreads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    CLAST_CK(cudaMemcpyAsync(doff.p, offs_rel, (nreads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, cs));
     CLAST_CK(cudaMemcpyAsync(qb.wstart.p, wstart.data(), wstart.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
-                             st));
-    CLAST_CK(cudaEventRecord(ctx->ev1, st));
+                             cs));
+    CLAST_CK(cudaEventRecord(ctx->ev3, cs));
+    CLAST_CK(cudaStreamWaitEvent(st, ctx->ev3, 0));
+    CLAST_CK(cudaEventRecord(ctx->ev1, st));  // the reads are resident and the compute stream is free
     CLAST_CK(cudaMemsetAsync(qb.bases.p, 'N', (size_t)qb.n + 2 * kPad, st));
     build_strands(rsrc, doff.p, nreads, nb, qb.bases.p + kPad, qb.start.p, qb.len.p, st);
     qb.pack(st);
@@ -1046,7 +1062,7 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     CLAST_CK(cudaEventRecord(ctx->ev2, st));
     CLAST_CK(cudaEventSynchronize(ctx->ev2));
     float up = 0, ms = 0;
-    CLAST_CK(cudaEventElapsedTime(&up, ctx->ev0, ctx->ev1));
+    CLAST_CK(cudaEventElapsedTime(&up, ctx->ev0, ctx->ev3));
     CLAST_CK(cudaEventElapsedTime(&ms, ctx->ev1, ctx->ev2));
     ctx->timer.flush();
     S.map_upload_ms = up;
