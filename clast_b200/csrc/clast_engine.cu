@@ -791,15 +791,23 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
     // the raw target set on the device, uploaded once unless already resident
     const int64_t nt = targets->n_seqs;
     const int64_t tbytes = nt ? targets->offsets[nt] - targets->offsets[0] : 0;
+    // host-resident bases go up on the copy stream window by window, so that a
+    // window's index build starts as soon as its bytes have arrived
+    const bool host_src = !targets->bases_on_device;
+    const char* hsrc = targets->bases + (nt ? targets->offsets[0] : 0);
     DevArray<char> traw;
-    const char* src = targets->bases + (nt ? targets->offsets[0] : 0);
-    CLAST_CK(cudaEventRecord(T->ev_start, st));
-    if (!targets->bases_on_device) {
+    cudaStream_t cs = host_src ? ctx->st_copy : st;
+    if (host_src) {
+      g_alloc_stream = ctx->st_copy;
       traw.alloc((size_t)tbytes + 1);
-      if (tbytes) CLAST_CK(cudaMemcpyAsync(traw.p, src, (size_t)tbytes, cudaMemcpyHostToDevice, st));
-      src = traw.p;
+      g_alloc_stream = st;
+      traw.st = st;  // freed in the compute stream's order, after the builds
     }
-    CLAST_CK(cudaEventRecord(T->ev_up, st));
+    const char* src = host_src ? traw.p : hsrc;
+    CLAST_CK(cudaEventRecord(T->ev_start, cs));
+    if (!host_src) CLAST_CK(cudaEventRecord(T->ev_up, cs));  // nothing to upload
+    int64_t copied = 0;  // source bytes already queued for upload
+    std::vector<cudaEvent_t> win_ev;
     // the windows are indexed back to back on the stream with no host
     // synchronisation; the table-overflow count is read by the first clast_map
     unsigned long long* failed = T->failed.p;
@@ -845,6 +853,17 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
       CLAST_CK(cudaMemcpyAsync(all_so.p, so.data(), so.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
     }
     for (const Plan& w : plan) {
+      if (host_src) {  // the window's records: source bytes up to the end of its last record
+        const int64_t last = so[w.meta + w.nseqs - 1] + ln[w.meta + w.nseqs - 1];
+        if (last > copied) {
+          CLAST_CK(cudaMemcpyAsync(traw.p + copied, hsrc + copied, (size_t)(last - copied), cudaMemcpyHostToDevice,
+                                   cs));
+          copied = last;
+        }
+        win_ev.push_back(ctx->timer.take());
+        CLAST_CK(cudaEventRecord(win_ev.back(), cs));
+        CLAST_CK(cudaStreamWaitEvent(st, win_ev.back(), 0));
+      }
       DevArray<char> padded;
       DevArray<int32_t> dgw, dln;
       padded.alloc((size_t)w.n + 2 * kPad);
@@ -861,10 +880,17 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
                                        w.first, failed));
       T->wins.push_back(std::move(win));
     }
+    if (host_src) {
+      if (tbytes > copied)
+        CLAST_CK(cudaMemcpyAsync(traw.p + copied, hsrc + copied, (size_t)(tbytes - copied), cudaMemcpyHostToDevice,
+                                 cs));
+      CLAST_CK(cudaEventRecord(T->ev_up, cs));
+    }
     CLAST_CK(cudaEventRecord(T->ev_done, st));
     T->launches = g_kernel_launches - k0;
     // a host source must stay readable until its copy has been made
-    if (!targets->bases_on_device) CLAST_CK(cudaEventSynchronize(T->ev_up));
+    if (host_src) CLAST_CK(cudaEventSynchronize(T->ev_up));
+    for (cudaEvent_t e : win_ev) ctx->timer.pool.push_back(e);
     ctx->stats.index_wall_ms = wall_ms() - w0;
     *out = T.release();
     return CLAST_OK;
