@@ -123,6 +123,10 @@ __host__ __device__ __forceinline__ uint64_t order_code(uint64_t key, int l) {
 __device__ __forceinline__ int64_t record_home(uint64_t code, int l, uint32_t nbuckets) {
   return 2 * (int64_t)__umul64hi(code << (64 - 2 * l), (uint64_t)nbuckets);
 }
+// The same for l <= 16 in 32-bit arithmetic.
+__device__ __forceinline__ int64_t record_home16(uint32_t code, int l, uint32_t nbuckets) {
+  return 2 * (int64_t)__umulhi(code << (32 - 2 * l), nbuckets);
+}
 // Filter hash of a code: an xorshift then a multiply by an odd constant
 // (Fibonacci hashing).  The top bits select the 32-bit filter word, bits
 // 16..30 the three filter bits.

@@ -632,18 +632,23 @@ __device__ __forceinline__ int round_lookup(const QueryView& q, const IndexView&
           vmask &= ~(1u << i);
     }
   }
-  uint32_t fw[P];
+  uint32_t fw[P], fm[P];
 #pragma unroll
-  for (int i = 0; i < P; ++i)
-    fw[i] = ((vmask >> i) & 1u) ? __ldg(ix.filter + filter_word(key_hash(code[i]), ix.fshift)) : 0u;
+  for (int i = 0; i < P; ++i) {
+    const uint64_t h = key_hash(code[i]);
+    fm[i] = filter_mask(h);
+    fw[i] = ((vmask >> i) & 1u) ? __ldg(ix.filter + filter_word(h, ix.fshift)) : 0u;
+  }
   ulonglong2 rec[P];
   uint32_t pmask = 0;
 #pragma unroll
   for (int i = 0; i < P; ++i) {
-    const bool pass = ((vmask >> i) & 1u) && filter_pass(fw[i], key_hash(code[i]));
+    const bool pass = ((vmask >> i) & 1u) && (fw[i] & fm[i]) == fm[i];
     pmask |= (uint32_t)pass << i;
     rec[i] = make_ulonglong2(0ull, kNoPayload);
-    if (pass) rec[i] = __ldcs(ix.table + record_home(code[i], ix.l, ix.nbuckets));
+    if (pass)
+      rec[i] = __ldcs(ix.table + (SMALL ? record_home16((uint32_t)code[i], ix.l, ix.nbuckets)
+                                        : record_home(code[i], ix.l, ix.nbuckets)));
   }
   // resolve from the home records; the keys displaced further read the next
   // record (the home bucket's second, same 32-byte sector) together
@@ -659,7 +664,9 @@ __device__ __forceinline__ int round_lookup(const QueryView& q, const IndexView&
   if (__any_sync(kFull, more != 0)) {
 #pragma unroll
     for (int i = 0; i < P; ++i)
-      if ((more >> i) & 1u) rec[i] = __ldcs(ix.table + record_home(code[i], ix.l, ix.nbuckets) + 1);
+      if ((more >> i) & 1u)
+        rec[i] = __ldcs(ix.table + 1 + (SMALL ? record_home16((uint32_t)code[i], ix.l, ix.nbuckets)
+                                              : record_home(code[i], ix.l, ix.nbuckets)));
 #pragma unroll
     for (int i = 0; i < P; ++i)
       if ((more >> i) & 1u) {
@@ -702,21 +709,46 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
 }
 
 // Writes a round's seeds (lane L's l-mers r0 + L*P .. in order, lanes in
-// order) from w onwards and advances w past them.
+// order) from w onwards and advances w past them.  When every l-mer of the
+// round has at most one entry, the payloads go through the warp's slice of
+// shared memory (stage_pl / stage_qi, kSeedRound entries) so that lane j
+// writes seed j; otherwise each lane writes its own.
 __device__ __forceinline__ void round_emit(const IndexView& ix, const TargetView& t, int gap, int local, int qlen,
                                            int r0, int lane, const uint64_t (&pl)[kSeedPerLane], int64_t& w,
-                                           int& valid, uint64_t* __restrict__ skey, uint32_t* __restrict__ sq) {
+                                           int& valid, uint64_t* __restrict__ skey, uint32_t* __restrict__ sq,
+                                           uint64_t* stage_pl, int32_t* stage_qi) {
   int cnt = 0;
+  bool multi = false;
 #pragma unroll
-  for (int i = 0; i < kSeedPerLane; ++i) cnt += payload_count(pl[i]);
+  for (int i = 0; i < kSeedPerLane; ++i) {
+    const int c = payload_count(pl[i]);
+    cnt += c;
+    multi |= c > 1;
+  }
   int round_total;
-  int64_t wl = w + warp_excl_scan(cnt, lane, &round_total);
+  const int excl = warp_excl_scan(cnt, lane, &round_total);
+  if (!__any_sync(kFull, multi)) {
+    int k = excl;
 #pragma unroll
-  for (int i = 0; i < kSeedPerLane; ++i)
-    if (pl[i] != kNoPayload) {
-      seed_put(ix, t, gap, local, qlen, r0 + lane * kSeedPerLane + i, pl[i], wl, valid, skey, sq);
-      wl += payload_count(pl[i]);
-    }
+    for (int i = 0; i < kSeedPerLane; ++i)
+      if (pl[i] != kNoPayload) {
+        stage_pl[k] = pl[i];
+        stage_qi[k] = r0 + lane * kSeedPerLane + i;
+        ++k;
+      }
+    __syncwarp();
+    for (int j = lane; j < round_total; j += 32) seed_put(ix, t, gap, local, qlen, stage_qi[j], stage_pl[j], w + j,
+                                                         valid, skey, sq);
+    __syncwarp();
+  } else {
+    int64_t wl = w + excl;
+#pragma unroll
+    for (int i = 0; i < kSeedPerLane; ++i)
+      if (pl[i] != kNoPayload) {
+        seed_put(ix, t, gap, local, qlen, r0 + lane * kSeedPerLane + i, pl[i], wl, valid, skey, sq);
+        wl += payload_count(pl[i]);
+      }
+  }
   w += round_total;
 }
 
@@ -727,7 +759,7 @@ constexpr int kSeedFusedThreads = 128;
 // the range reservations of neighbouring warps hit different counters.
 // SMALL: l <= 16, keys read with 32-bit funnel shifts.
 template <bool SMALL>
-__global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, IndexView ix, TargetView t, int gap,
+__global__ void __launch_bounds__(kSeedFusedThreads, SMALL ? 8 : 6) k_seed_fused(QueryView q, IndexView ix, TargetView t, int gap,
                                                                    int local, unsigned long long* __restrict__ cursor,
                                                                    unsigned long long* __restrict__ n_kmers,
                                                                    int64_t* __restrict__ off, int32_t* __restrict__ cnt,
@@ -735,8 +767,11 @@ __global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, I
                                                                    uint64_t* __restrict__ skey,
                                                                    uint32_t* __restrict__ sq, int64_t part_cap) {
   constexpr int P = kSeedPerLane;
+  __shared__ uint64_t stage_pl[kSeedFusedThreads / 32][kSeedRound];
+  __shared__ int32_t stage_qi[kSeedFusedThreads / 32][kSeedRound];
   const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
   if (s >= q.nstrands) return;
   const int64_t st = q.start[s];
   const int qlen = q.len[s];
@@ -785,11 +820,11 @@ __global__ void __launch_bounds__(kSeedFusedThreads) k_seed_fused(QueryView q, I
   }
   int valid = 0;
   int64_t w = (int64_t)base;
-  round_emit(ix, t, gap, local, qlen, 0, lane, pl0, w, valid, skey, sq);
+  round_emit(ix, t, gap, local, qlen, 0, lane, pl0, w, valid, skey, sq, stage_pl[wib], stage_qi[wib]);
   for (int r0 = kSeedRound; r0 < nk; r0 += kSeedRound) {
     uint64_t pl[P];
     round_lookup<SMALL>(q, ix, st, nk, r0, lane, any_n, pl);
-    round_emit(ix, t, gap, local, qlen, r0, lane, pl, w, valid, skey, sq);
+    round_emit(ix, t, gap, local, qlen, r0, lane, pl, w, valid, skey, sq, stage_pl[wib], stage_qi[wib]);
   }
   valid = (int)__reduce_add_sync(kFull, (unsigned)valid);
   if (lane == 0) nvalid[s] = valid;
