@@ -1512,7 +1512,7 @@ struct DpKernelArgs {
 };
 
 template <int GAP, bool LOCAL>
-__global__ void __launch_bounds__(128) k_banded_dp(DpKernelArgs a) {
+__global__ void __launch_bounds__(128, GAP <= 9 ? 4 : (GAP <= 12 ? 3 : 2)) k_banded_dp(DpKernelArgs a) {
   __shared__ int2 tab[32 * 32];  // [target letter][query letter], letters 'A'..'Z': (POINT + 7, match)
   for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
     const int2 w = cell_score(class_of_letter((i >> 5) < 26 ? (i >> 5) : kNClass),
