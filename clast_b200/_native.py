@@ -66,6 +66,8 @@ SIGNATURES = {
     "clast_targets_create": (C.c_int, [C.c_void_p, C.POINTER(clast_params), C.c_int32, C.POINTER(clast_seqs),
                                        C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
     "clast_targets_free": (None, [C.c_void_p]),
+    "clast_targets_save": (C.c_int, [C.c_void_p, C.c_void_p, C.c_char_p]),
+    "clast_targets_load": (C.c_int, [C.c_void_p, C.POINTER(clast_params), C.c_char_p, C.POINTER(C.c_void_p)]),
     "clast_map": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(clast_params), C.c_int32, C.POINTER(clast_seqs),
                             C.c_int32, C.c_void_p, C.POINTER(clast_map_result)]),
     "clast_map_result_free": (None, [C.POINTER(clast_map_result)]),

@@ -21,6 +21,7 @@ that fails raises :class:`ClastError` with the library's message.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import dataclasses
 import time
 
@@ -323,6 +324,18 @@ class Engine:
         p = s.c()
         self._check(self._lib.clast_targets_create(self.ctx, C.byref(p), int(t_vram), C.byref(seqs), len(ls),
                                                    ls.ctypes.data, C.byref(out)))
+        return Targets(out.value, self)
+
+    def save_targets(self, targets: Targets, path: str) -> None:
+        """clast_targets_save: every resident window index to one file."""
+        self._check(self._lib.clast_targets_save(self.ctx, targets.handle, os.fsencode(path)))
+
+    def load_targets(self, s: Setting, path: str) -> Targets:
+        """clast_targets_load: indexes written by save_targets, for settings
+        with the same lmer / stride / cut_repeat."""
+        out = C.c_void_p()
+        p = s.c()
+        self._check(self._lib.clast_targets_load(self.ctx, C.byref(p), os.fsencode(path), C.byref(out)))
         return Targets(out.value, self)
 
     def map(self, s: Setting, targets: Targets, bases, offsets: np.ndarray, load_sizes, q_vram: int) -> dict:

@@ -13,6 +13,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -595,6 +596,23 @@ struct clast_targets {
 
 namespace {
 
+// Waits for the index builds of clast_targets_create (once), records their
+// time in the context's stats and reports a table overflow.
+void settle_targets(clast_ctx* ctx, const clast_targets* T) {
+  if (T->settled) return;
+  CLAST_CK(cudaEventSynchronize(T->ev_done));
+  T->settled = true;
+  float up = 0, bd = 0;
+  CLAST_CK(cudaEventElapsedTime(&up, T->ev_start, T->ev_up));
+  CLAST_CK(cudaEventElapsedTime(&bd, T->ev_up, T->ev_done));
+  ctx->stats.index_upload_ms = up;
+  ctx->stats.index_ms = bd;
+  ctx->stats.index_launches = T->launches;
+  if (read_scalar(reinterpret_cast<const int64_t*>(T->failed.p), ctx->st) != 0)
+    throw std::runtime_error("index table overflow");
+}
+
+
 // One read window list per query load (moveQueryWindow, CHostSchedular.cu:12-23):
 // the window [qb, qe) grows while gateway(2*qe+2) - gateway(2*qb) < q_vram,
 // where every read adds two strands of len + l - 1 bases.  With the prefix
@@ -995,18 +1013,7 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     qb.pack(st);
     S.query_bases = qb.n;
     // the index builds of clast_targets_create end before the first search
-    if (!T->settled) {
-      CLAST_CK(cudaEventSynchronize(T->ev_done));
-      T->settled = true;
-      float up = 0, bd = 0;
-      CLAST_CK(cudaEventElapsedTime(&up, T->ev_start, T->ev_up));
-      CLAST_CK(cudaEventElapsedTime(&bd, T->ev_up, T->ev_done));
-      S.index_upload_ms = up;
-      S.index_ms = bd;
-      S.index_launches = T->launches;
-      if (read_scalar(reinterpret_cast<const int64_t*>(T->failed.p), st) != 0)
-        throw std::runtime_error("index table overflow");
-    }
+    settle_targets(ctx, T);
     // every target window, in holder order (target load, window)
     std::vector<DevHits> per_win(T->wins.size());
     for (size_t w = 0; w < T->wins.size(); ++w) search_batch(ctx, T->wins[w].ix.get(), p, qb, 0, per_win[w]);
@@ -1363,5 +1370,166 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
       CLAST_CK(cudaMemcpyAsync(dst[k], src[k], F * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     CLAST_CK(cudaMemcpyAsync(out->evalue, fo.evalue, F * sizeof(double), cudaMemcpyDeviceToHost, st));
     return finish(F);
+  });
+}
+
+// ----------------------------------------------------------------------------
+// Index persistence: every window of a clast_targets in one file.
+// ----------------------------------------------------------------------------
+namespace {
+
+constexpr char kIndexMagic[8] = {'C', 'L', 'A', 'S', 'T', 'I', 'X', '1'};
+
+struct FileCloser {
+  FILE* f;
+  ~FileCloser() {
+    if (f) std::fclose(f);
+  }
+};
+
+template <class T>
+void put(FILE* f, const T& v) {
+  if (std::fwrite(&v, sizeof(T), 1, f) != 1) throw std::runtime_error("index file write failed");
+}
+template <class T>
+T get(FILE* f) {
+  T v;
+  if (std::fread(&v, sizeof(T), 1, f) != 1) throw std::invalid_argument("index file truncated");
+  return v;
+}
+
+// Device array -> file, through a host bounce buffer.
+template <class T>
+void put_array(FILE* f, const T* dev, int64_t count, std::vector<char>& buf, cudaStream_t st) {
+  const int64_t bytes = count * (int64_t)sizeof(T);
+  for (int64_t off = 0; off < bytes; off += (int64_t)buf.size()) {
+    const size_t len = (size_t)std::min<int64_t>((int64_t)buf.size(), bytes - off);
+    CLAST_CK(cudaMemcpyAsync(buf.data(), reinterpret_cast<const char*>(dev) + off, len, cudaMemcpyDeviceToHost, st));
+    CLAST_CK(cudaStreamSynchronize(st));
+    if (std::fwrite(buf.data(), 1, len, f) != len) throw std::runtime_error("index file write failed");
+  }
+}
+template <class T>
+void get_array(FILE* f, DevArray<T>& dev, int64_t count, std::vector<char>& buf, cudaStream_t st) {
+  if (count < 0 || count > ((int64_t)1 << 40)) throw std::invalid_argument("index file holds a bad array size");
+  dev.alloc((size_t)count);
+  const int64_t bytes = count * (int64_t)sizeof(T);
+  for (int64_t off = 0; off < bytes; off += (int64_t)buf.size()) {
+    const size_t len = (size_t)std::min<int64_t>((int64_t)buf.size(), bytes - off);
+    if (std::fread(buf.data(), 1, len, f) != len) throw std::invalid_argument("index file truncated");
+    CLAST_CK(cudaMemcpyAsync(reinterpret_cast<char*>(dev.p) + off, buf.data(), len, cudaMemcpyHostToDevice, st));
+    CLAST_CK(cudaStreamSynchronize(st));  // the bounce buffer is reused
+  }
+}
+
+}  // namespace
+
+extern "C" int clast_targets_save(clast_ctx* ctx, const clast_targets* T, const char* path) {
+  if (!ctx || !T || !path) return CLAST_ERR_ARG;
+  return guarded(ctx, [&]() -> int {
+    CLAST_CK(cudaSetDevice(ctx->device));
+    settle_targets(ctx, T);
+    FileCloser fc{std::fopen(path, "wb")};
+    if (!fc.f) throw std::invalid_argument(std::string("cannot open ") + path + " for writing");
+    FILE* f = fc.f;
+    cudaStream_t st = ctx->st;
+    std::vector<char> buf((size_t)64 << 20);
+    std::fwrite(kIndexMagic, 1, sizeof(kIndexMagic), f);
+    const clast_index* first = T->wins.empty() ? nullptr : T->wins[0].ix.get();
+    put<int32_t>(f, first ? first->l : 0);
+    put<int32_t>(f, first ? first->stride : 0);
+    put<int32_t>(f, first ? first->cut : 0);
+    put<int32_t>(f, T->n_loads);
+    put<int64_t>(f, (int64_t)T->wins.size());
+    for (const auto& w : T->wins) {
+      const clast_index& ix = *w.ix;
+      put<int32_t>(f, w.load);
+      put<int32_t>(f, w.first);
+      put<int32_t>(f, ix.t_begin);
+      put<int32_t>(f, ix.nseqs);
+      put<int64_t>(f, ix.n);
+      put<uint32_t>(f, ix.nbuckets);
+      put<int32_t>(f, ix.fshift);
+      put<int64_t>(f, ix.n_records);
+      put<int64_t>(f, (int64_t)ix.filter.n);
+      put<int64_t>(f, (int64_t)ix.entries.n);
+      put<int64_t>(f, ix.n_keys);
+      put_array(f, ix.bases.p, ix.n + 2 * kPad, buf, st);
+      put_array(f, ix.gateway.p, ix.nseqs, buf, st);
+      put_array(f, ix.lengths.p, ix.nseqs, buf, st);
+      put_array(f, ix.entries.p, (int64_t)ix.entries.n, buf, st);
+      put_array(f, ix.table.p, ix.n_records, buf, st);
+      put_array(f, ix.filter.p, (int64_t)ix.filter.n, buf, st);
+    }
+    if (std::fflush(f) != 0) throw std::runtime_error("index file write failed");
+    return CLAST_OK;
+  });
+}
+
+extern "C" int clast_targets_load(clast_ctx* ctx, const clast_params* p, const char* path, clast_targets** out) {
+  if (!ctx || !out || !path) return CLAST_ERR_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&]() -> int {
+    check_params(p);
+    CLAST_CK(cudaSetDevice(ctx->device));
+    g_alloc_stream = ctx->st;
+    FileCloser fc{std::fopen(path, "rb")};
+    if (!fc.f) throw std::invalid_argument(std::string("cannot open ") + path);
+    FILE* f = fc.f;
+    char magic[sizeof(kIndexMagic)];
+    if (std::fread(magic, 1, sizeof(magic), f) != sizeof(magic) || std::memcmp(magic, kIndexMagic, sizeof(magic)))
+      throw std::invalid_argument(std::string(path) + " is not a clast index file");
+    const int32_t l = get<int32_t>(f), stride = get<int32_t>(f), cut = get<int32_t>(f);
+    const int32_t n_loads = get<int32_t>(f);
+    const int64_t n_wins = get<int64_t>(f);
+    if (n_wins > 0 && (l != p->lmer || stride != p->stride || cut != p->cut_repeat))
+      throw std::invalid_argument("the index was built with other lMer / stride / repeat settings");
+    if (n_loads < 0 || n_wins < 0 || n_wins > (int64_t)1 << 24) throw std::invalid_argument("bad index file header");
+    cudaStream_t st = ctx->st;
+    std::vector<char> buf((size_t)64 << 20);
+    std::unique_ptr<clast_targets> T(new clast_targets());
+    T->ctx = ctx;
+    T->n_loads = n_loads;
+    for (int64_t k = 0; k < n_wins; ++k) {
+      clast_targets::Win w;
+      w.load = get<int32_t>(f);
+      w.first = get<int32_t>(f);
+      std::unique_ptr<clast_index> ix(new clast_index());
+      ix->l = l;
+      ix->stride = stride;
+      ix->cut = cut;
+      ix->t_begin = get<int32_t>(f);
+      ix->nseqs = get<int32_t>(f);
+      ix->n = get<int64_t>(f);
+      ix->nbuckets = get<uint32_t>(f);
+      ix->fshift = get<int32_t>(f);
+      ix->n_records = get<int64_t>(f);
+      const int64_t n_filter = get<int64_t>(f), n_entries = get<int64_t>(f);
+      ix->n_keys = get<int64_t>(f);
+      if (ix->n < 0 || ix->nseqs < 0 || ix->nbuckets == 0 || ix->fshift < 32 || ix->fshift > 63 ||
+          ix->n_records < 2 * (int64_t)ix->nbuckets || n_filter != ((int64_t)1 << (64 - ix->fshift)))
+        throw std::invalid_argument("bad index file window header");
+      get_array(f, ix->bases, ix->n + 2 * kPad, buf, st);
+      get_array(f, ix->gateway, ix->nseqs, buf, st);
+      get_array(f, ix->lengths, ix->nseqs, buf, st);
+      get_array(f, ix->entries, n_entries, buf, st);
+      get_array(f, ix->table, ix->n_records, buf, st);
+      get_array(f, ix->filter, n_filter, buf, st);
+      w.ix = std::move(ix);
+      T->wins.push_back(std::move(w));
+    }
+    // nothing left to wait for: the targets are settled
+    T->failed.alloc(1);
+    CLAST_CK(cudaMemsetAsync(T->failed.p, 0, sizeof(unsigned long long), st));
+    T->ev_start = ctx->timer.take();
+    T->ev_up = ctx->timer.take();
+    T->ev_done = ctx->timer.take();
+    CLAST_CK(cudaEventRecord(T->ev_start, st));
+    CLAST_CK(cudaEventRecord(T->ev_up, st));
+    CLAST_CK(cudaEventRecord(T->ev_done, st));
+    CLAST_CK(cudaStreamSynchronize(st));
+    T->settled = true;
+    *out = T.release();
+    return CLAST_OK;
   });
 }

@@ -153,6 +153,15 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram,
                          clast_targets** out);
 void clast_targets_free(clast_targets* t);
 
+/* Index persistence (no counterpart in the reference, which rebuilds every
+ * index for every query RAM load, main.cu:63-89).  clast_targets_save waits for the index builds and
+ * writes every window (bases, sequence tables, entries, hash table, filter) to
+ * one file; clast_targets_load reads it back onto the context's GPU, ready for
+ * clast_map.  Loading fails with CLAST_ERR_ARG when the file was built with
+ * other lmer / stride / cut_repeat settings or is not an index file. */
+int clast_targets_save(clast_ctx* ctx, const clast_targets* t, const char* path);
+int clast_targets_load(clast_ctx* ctx, const clast_params* p, const char* path, clast_targets** out);
+
 /* Result of clast_map: hits of every query load in the order
  * CHostResultHolder::fixResult leaves them (load by load).  read = record
  * index in the query set; strand 0 '+', 1 '-'; t_load / t_seq locate the
