@@ -8,6 +8,7 @@
 #include "clast_host.h"
 
 #include <cerrno>
+#include <chrono>
 #include <climits>
 #include <cstdint>
 #include <cstdio>
@@ -16,6 +17,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #ifdef _OPENMP
@@ -67,28 +69,149 @@ bool read_file(const std::string& path, std::string& data) {
   FILE* f = std::fopen(path.c_str(), "rb");
   if (!f) return false;
   data.clear();
-  char buf[1 << 16];
+  if (std::fseek(f, 0, SEEK_END) == 0) {
+    const long size = std::ftell(f);
+    if (size > 0 && std::fseek(f, 0, SEEK_SET) == 0) {
+      data.resize((size_t)size);
+      const size_t got = std::fread(&data[0], 1, (size_t)size, f);
+      data.resize(got);
+    }
+  }
+  char buf[1 << 16];  // whatever remains (streams whose size is unknown)
   size_t k;
   while ((k = std::fread(buf, 1, sizeof(buf), f)) > 0) data.append(buf, k);
   std::fclose(f);
   return true;
 }
 
+// One FASTA file split into lines, in parallel, and into records the way
+// CFASTAFileLoader::read walks it (CFASTALoader.cpp:112-170): a record is
+// finalised at the next line holding '>', at an empty line and at the end of
+// the file, and only if its label is not empty; a line holding '@' sets the
+// start index of the record being read (to_int of the rest of the line);
+// sequence lines read while there is no label are ignored.
+struct ParsedFasta {
+  enum : uint8_t { kSeq = 0, kLabel = 1, kAt = 2, kEmpty = 3 };
+  std::string data;
+  std::vector<int64_t> start;  // line i: [start[i], end(i)), '\n' excluded
+  std::vector<uint8_t> type;
+  std::vector<int64_t> kept;   // sequence lines: characters kept (spaces removed)
+  struct Rec {
+    int64_t label_line, first, last;  // sequence lines in [first, last)
+    int64_t len;
+    int32_t start_idx;
+  };
+  std::vector<Rec> recs;
+  int64_t end(int64_t i) const {
+    if (i + 1 < (int64_t)start.size()) return start[i + 1] - 1;
+    const int64_t n = (int64_t)data.size();  // the last line, with or without its '\n'
+    return (n > 0 && data[n - 1] == '\n') ? n - 1 : n;
+  }
+
+  void parse() {
+    const int64_t n = (int64_t)data.size();
+    const char* d = data.data();
+    // line starts: 0 and every position after a '\n' that is inside the file
+    int nt = 1;
+#ifdef _OPENMP
+    nt = std::max(1, omp_get_max_threads());
+#endif
+    std::vector<std::vector<int64_t>> part(nt);
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int t = 0; t < nt; ++t) {
+      const int64_t a = n * t / nt, b = n * (t + 1) / nt;
+      const char* q = d + a;
+      while (q < d + b) {
+        const char* e = (const char*)std::memchr(q, '\n', (size_t)(d + b - q));
+        if (!e) break;
+        if (e + 1 < d + n) part[t].push_back((int64_t)(e + 1 - d));
+        q = e + 1;
+      }
+    }
+    start.clear();
+    if (n > 0) start.push_back(0);
+    for (auto& v : part) start.insert(start.end(), v.begin(), v.end());
+    const int64_t nl = (int64_t)start.size();
+    type.assign(nl, kSeq);
+    kept.assign(nl, 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nl; ++i) {
+      const char* ln = d + start[i];
+      const size_t len = (size_t)(end(i) - start[i]);
+      if (std::memchr(ln, '>', len)) type[i] = kLabel;
+      else if (std::memchr(ln, '@', len)) type[i] = kAt;
+      else if (len == 0) type[i] = kEmpty;
+      else {
+        int64_t spaces = 0;
+        for (size_t k = 0; k < len; ++k) spaces += ln[k] == ' ';
+        kept[i] = (int64_t)len - spaces;
+      }
+    }
+    recs.clear();
+    int64_t label = -1, first = -1, last = -1, len = 0;
+    int32_t start_idx = 0;
+    auto finish = [&](int64_t i) {  // judgeContinueReading on the record read so far
+      if (label < 0) return;
+      recs.push_back(Rec{label, first < 0 ? i : first, first < 0 ? i : last, len, start_idx});
+      label = -1;
+      first = last = -1;
+      len = 0;
+      start_idx = 0;
+    };
+    for (int64_t i = 0; i < nl; ++i) {
+      switch (type[i]) {
+        case kLabel:
+          finish(i);
+          label = (end(i) - start[i] > 1) ? i : -1;  // the label is the line after its first character
+          break;
+        case kAt:
+          try {
+            const int64_t a = start[i] + 1, e = std::max(a, end(i));
+            start_idx = to_int(std::string(d + a, (size_t)(e - a)), "@");
+          } catch (const UsageError&) {
+            throw UsageError(4, "bad file type: something was strange at the line which contains '@'.");
+          }
+          break;
+        case kEmpty:
+          finish(i);
+          break;
+        default:
+          if (label >= 0) {
+            if (first < 0) first = i;
+            last = i + 1;
+            len += kept[i];
+          }
+      }
+    }
+    finish(nl);
+  }
+};
+
 // totalDatabaseSize: characters of every target line that has no '>'
 // (CHostSetting.cu:46-58, std::getline splits on '\n' only).
 long total_db_size(const std::vector<std::string>& files) {
   long total = 0;
-  std::string d;
   for (const auto& f : files) {
-    if (!read_file(f, d)) continue;
-    size_t a = 0;
-    while (a < d.size()) {
-      size_t e = d.find('\n', a);
-      const size_t end = (e == std::string::npos) ? d.size() : e;
-      if (std::memchr(d.data() + a, '>', end - a) == nullptr) total += (long)(end - a);
-      if (e == std::string::npos) break;
-      a = e + 1;
+    ParsedFasta P;
+    if (!read_file(f, P.data)) continue;
+    const int64_t n = (int64_t)P.data.size();
+    const char* d = P.data.data();
+    int64_t sum = 0;
+    // every byte that is not a '\n', minus the lines holding a '>'
+#pragma omp parallel for reduction(+ : sum) schedule(static)
+    for (int64_t i = 0; i < n; ++i) sum += d[i] != '\n';
+    int64_t gt = 0;
+    {
+      int64_t a = 0;
+      while (a < n) {
+        const char* e = (const char*)std::memchr(d + a, '\n', (size_t)(n - a));
+        const int64_t end = e ? (int64_t)(e - d) : n;
+        if (std::memchr(d + a, '>', (size_t)(end - a))) gt += end - a;
+        if (!e) break;
+        a = end + 1;
+      }
     }
+    total += (long)(sum - gt);
   }
   return total;
 }
@@ -191,96 +314,89 @@ class Loader {
  public:
   Loader(const std::vector<std::string>& files, int budget) : files_(files), budget_(budget) {}
 
-  // CFASTALoader::loadFASTA: records until one does not fit the budget.
+  // CFASTALoader::loadFASTA (CFASTALoader.cpp:11-41) with judgeContinueReading
+  // (:43-87): records join the load while the load's bases plus the record's
+  // stay below the budget; a record longer than the budget is skipped; the
+  // load ends at the first record that does not fit, which opens the next
+  // load.  Files are parsed once, in parallel; the bases of a load are
+  // normalised (removeSpace + replaceSmallToBig, :89-106) in parallel.
   bool next(Load& out) {
-    if (index_ < 0) return false;
-    const int before = index_;
-    for (; index_ < (int)files_.size(); ++index_)
-      if (!read_file_part(files_[index_], out)) break;
-    if (index_ == (int)files_.size()) index_ = -1;
-    if (out.size() == 0 && index_ == before && index_ != -1)
-      throw UsageError(2, "a FASTA record is exactly as long as the RAM budget (the reference never terminates)");
+    if (file_ < 0) return false;
+    const int file_before = file_;
+    int64_t sum = 0;
+    std::vector<const ParsedFasta::Rec*> take;  // records of the current file
+    for (; file_ < (int)files_.size(); ++file_, rec_ = 0) {
+      const ParsedFasta& P = parsed(file_);
+      take.clear();
+      for (; rec_ < (int64_t)P.recs.size(); ++rec_) {
+        const ParsedFasta::Rec& r = P.recs[rec_];
+        if (r.len > budget_) continue;  // longer than the budget: skipped
+        if (sum + r.len < budget_) {
+          take.push_back(&r);
+          sum += r.len;
+        } else {
+          if (take.empty() && out.size() == 0 && file_ == file_before)
+            throw UsageError(2, "a FASTA record is exactly as long as the RAM budget (the reference never terminates)");
+          flush(out, take);
+          return true;
+        }
+      }
+      flush(out, take);  // the load goes on in the next file
+    }
+    file_ = -1;
     return true;
   }
-  bool done() const { return index_ < 0; }
+  bool done() const { return file_ < 0; }
 
  private:
-  // judgeContinueReading, CFASTALoader.cpp:43-87
-  bool judge(long pos, std::string& label, std::string& seq, int& start_idx, Load& out) {
-    if (!label.empty()) {
-      const long len = (long)seq.size();
-      if (len > budget_) {  // longer than the budget: skipped
-        label.clear();
-        seq.clear();
-        start_idx = 0;
-        read_pos_ = pos;
-      } else if (sum_ + len < budget_) {
-        out.labels.push_back(label);
-        out.start_idx.push_back(start_idx);
-        out.bases += seq;
-        out.offsets.push_back((int64_t)out.bases.size());
-        sum_ += len;
-        label.clear();
-        seq.clear();
-        start_idx = 0;
-        read_pos_ = pos;
-      } else {
-        sum_ = 0;
-        return false;
-      }
+  const ParsedFasta& parsed(int f) {
+    if (f != cached_) {
+      cache_ = ParsedFasta();
+      if (!read_file(files_[f], cache_.data)) throw UsageError(3, "file \"" + files_[f] + "\" open failed.");
+      cache_.parse();
+      cached_ = f;
     }
-    return true;
+    return cache_;
   }
-
-  // CFASTAFileLoader::read, CFASTALoader.cpp:112-170
-  bool read_file_part(const std::string& path, Load& out) {
-    if (path != cached_path_) {
-      if (!read_file(path, data_)) throw UsageError(3, "file \"" + path + "\" open failed.");
-      cached_path_ = path;
-    }
-    std::string label, seq;
-    int start_idx = 0;
-    size_t a = (size_t)read_pos_;
-    long line_start = read_pos_;
-    while (a < data_.size()) {
-      const size_t e = data_.find('\n', a);
-      const size_t end = (e == std::string::npos) ? data_.size() : e;
-      const char* ln = data_.data() + a;
-      const size_t n = end - a;
-      if (std::memchr(ln, '>', n)) {
-        if (!judge(line_start, label, seq, start_idx, out)) return false;
-        label.assign(n ? ln + 1 : ln, n ? n - 1 : 0);
-      } else if (std::memchr(ln, '@', n)) {
-        try {
-          start_idx = to_int(std::string(ln + 1, n - 1), "@");
-        } catch (const UsageError&) {
-          throw UsageError(4, "bad file type: something was strange at the line which contains '@'.");
-        }
-      } else if (n == 0) {
-        if (!judge(line_start, label, seq, start_idx, out)) return false;
-      } else if (!label.empty()) {  // removeSpace + replaceSmallToBig, :89-106
-        for (size_t i = 0; i < n; ++i) {
-          char c = ln[i];
+  // appends records of the cached file to the load
+  void flush(Load& out, const std::vector<const ParsedFasta::Rec*>& take) {
+    const size_t k0 = out.labels.size();
+    const size_t m = take.size();
+    out.labels.resize(k0 + m);
+    out.start_idx.resize(k0 + m);
+    out.offsets.resize(k0 + m + 1);
+    for (size_t i = 0; i < m; ++i) out.offsets[k0 + i + 1] = out.offsets[k0 + i] + take[i]->len;
+    const size_t b0 = out.bases.size();
+    out.bases.resize((size_t)out.offsets[k0 + m]);
+    const ParsedFasta& P = cache_;
+    const char* d = P.data.data();
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < (int64_t)m; ++i) {
+      const ParsedFasta::Rec& r = *take[i];
+      const int64_t la = P.start[r.label_line] + 1;
+      out.labels[k0 + i].assign(d + la, (size_t)(P.end(r.label_line) - la));
+      out.start_idx[k0 + i] = r.start_idx;
+      char* w = &out.bases[0] + b0 + (out.offsets[k0 + i] - out.offsets[k0]);
+      for (int64_t ln = r.first; ln < r.last; ++ln) {
+        if (P.type[ln] != ParsedFasta::kSeq) continue;
+        const int64_t e = P.end(ln);
+        for (int64_t k = P.start[ln]; k < e; ++k) {
+          char c = d[k];
           if (c == ' ') continue;
           if (c > 'Z') c = (char)(c - 32);
           if (c < 'A' || c > 'Z') c = 'N';
-          seq.push_back(c);
+          *w++ = c;
         }
       }
-      if (e == std::string::npos) break;
-      a = e + 1;
-      line_start = (long)a;
     }
-    if (!judge((long)data_.size(), label, seq, start_idx, out)) return false;
-    read_pos_ = 0;
-    return true;
   }
 
   std::vector<std::string> files_;
   int budget_;
-  int index_ = 0;
-  long read_pos_ = 0, sum_ = 0;
-  std::string cached_path_, data_;
+  int file_ = 0;
+  int64_t rec_ = 0;
+  int cached_ = -1;
+  ParsedFasta cache_;
 };
 
 // ---------------------------------------------------------------------------
@@ -359,14 +475,42 @@ void write_tsv(FILE* f, const Load& q, int64_t read0, const TargetMeta& tm, cons
   for (const auto& o : bufs) std::fwrite(o.data(), 1, o.size(), f);
 }
 
+// Wall-clock phases of one command-line run, printed to stderr when the
+// environment variable CLAST_CLI_TIMING is set.
+struct PhaseClock {
+  bool on = std::getenv("CLAST_CLI_TIMING") != nullptr;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  void mark(const char* what) {
+    const auto now = std::chrono::steady_clock::now();
+    if (on) std::fprintf(stderr, "clast: %-22s %9.1f ms\n", what, std::chrono::duration<double, std::milli>(now - t).count());
+    t = now;
+  }
+};
+
 int run(int argc, const char* const* argv, std::string& err) {
+  PhaseClock clock;
   Settings s = parse_args(argc, argv);
+  // the CUDA context comes up on its own thread while the FASTA files are read
+  clast_ctx* ctx = nullptr;
+  int ctx_rc = CLAST_OK;
+  std::thread ctx_thread([&]() { ctx_rc = clast_ctx_create(s.device, &ctx); });
+  bool adopted = false;  // ctx_guard below owns the context
+  struct Joiner {
+    std::thread& th;
+    clast_ctx*& ctx;
+    bool& adopted;
+    ~Joiner() {  // an early return or error: wait for the context and release it
+      if (th.joinable()) th.join();
+      if (ctx && !adopted) clast_ctx_destroy(ctx);
+    }
+  } joiner{ctx_thread, ctx, adopted};
   for (const auto& f : s.tfiles) {
     FILE* t = std::fopen(f.c_str(), "rb");
     if (!t) throw UsageError(3, "file \"" + f + "\" open failed.");
     std::fclose(t);
   }
   s.totalDB = (double)total_db_size(s.tfiles);
+  clock.mark("database size");
   {  // main.cu:26-27: the output file is truncated first
     FILE* f = std::fopen(s.out.c_str(), "wb");
     if (!f) throw UsageError(3, "cannot open output file " + s.out);
@@ -383,6 +527,7 @@ int run(int argc, const char* const* argv, std::string& err) {
       tl.next(tloads.back());
     }
   }
+  clock.mark("target FASTA");
   std::vector<Load> qloads;
   {
     Loader ql(s.qfiles, q_budget);
@@ -391,6 +536,7 @@ int run(int argc, const char* const* argv, std::string& err) {
       ql.next(qloads.back());
     }
   }
+  clock.mark("query FASTA");
   clast_params p;
   p.lmer = s.lmer;
   p.stride = s.stride;
@@ -402,33 +548,42 @@ int run(int argc, const char* const* argv, std::string& err) {
   p.total_db = s.totalDB;
   p.K = 0.71;       // common.hpp:42
   p.lambda = 1.37;  // common.hpp:43
-  // concatenated targets and reads
+  // concatenated targets and reads (a load's bases are contiguous already)
   std::string tb, qb;
   std::vector<int64_t> toff{0}, qoff{0}, tsizes, qsizes;
   TargetMeta tm;
-  for (const Load& L : tloads) {
-    for (size_t i = 0; i < L.size(); ++i) {
-      tb.append(L.bases, L.offsets[i], L.offsets[i + 1] - L.offsets[i]);
-      toff.push_back((int64_t)tb.size());
+  auto concat = [](const std::vector<Load>& loads, std::string& b, std::vector<int64_t>& off,
+                   std::vector<int64_t>& sizes) {
+    size_t total = 0, recs = 0;
+    for (const Load& L : loads) {
+      total += L.bases.size();
+      recs += L.size();
     }
-    tsizes.push_back((int64_t)L.size());
+    b.reserve(total);
+    off.reserve(recs + 1);
+    for (const Load& L : loads) {
+      const int64_t base = (int64_t)b.size();
+      b.append(L.bases);
+      for (size_t i = 1; i < L.offsets.size(); ++i) off.push_back(base + L.offsets[i]);
+      sizes.push_back((int64_t)L.size());
+    }
+  };
+  concat(tloads, tb, toff, tsizes);
+  concat(qloads, qb, qoff, qsizes);
+  for (const Load& L : tloads) {
     tm.labels.push_back(L.labels);
     tm.start_idx.push_back(L.start_idx);
   }
-  for (const Load& L : qloads) {
-    for (size_t i = 0; i < L.size(); ++i) {
-      qb.append(L.bases, L.offsets[i], L.offsets[i + 1] - L.offsets[i]);
-      qoff.push_back((int64_t)qb.size());
-    }
-    qsizes.push_back((int64_t)L.size());
-  }
-  clast_ctx* ctx = nullptr;
-  int rc = clast_ctx_create(s.device, &ctx);
+  clock.mark("concatenate");
+  ctx_thread.join();
+  clock.mark("CUDA context (wait)");
+  int rc = ctx_rc;
   if (rc != CLAST_OK) {
     err = "cannot create a CUDA context on device " + std::to_string(s.device);
     return 5;
   }
   std::unique_ptr<clast_ctx, void (*)(clast_ctx*)> ctx_guard(ctx, clast_ctx_destroy);
+  adopted = true;
   clast_seqs ts{(int64_t)(toff.size() - 1), tb.data(), toff.data()};
   clast_targets* targets = nullptr;
   rc = clast_targets_create(ctx, &p, t_vram, &ts, (int32_t)tsizes.size(), tsizes.data(), &targets);
@@ -445,6 +600,7 @@ int run(int argc, const char* const* argv, std::string& err) {
     return 6;
   }
   std::unique_ptr<clast_map_result, void (*)(clast_map_result*)> r_guard(&res, clast_map_result_free);
+  clock.mark("GPU search");
   FILE* f = std::fopen(s.out.c_str(), "ab");
   if (!f) throw UsageError(3, "cannot open output file " + s.out);
   int64_t read0 = 0;
@@ -453,6 +609,7 @@ int run(int argc, const char* const* argv, std::string& err) {
     read0 += (int64_t)qloads[k].size();
   }
   std::fclose(f);
+  clock.mark("TSV");
   return 0;
 }
 

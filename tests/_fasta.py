@@ -43,3 +43,43 @@ def write_quirky(tmp, seed):
             f.write(b">read%d\n" % i)
             f.write(s[:50] + b"\n" + s[50:100].replace(b"A", b"a", 3) + b" " + s[100:] + b"\n")
     return tp, [q1, q2]
+
+
+def write_adversarial(tmp, seed):
+    """Loader edge cases: '@' before the first header and between records,
+    an empty header, sequence before any header, a blank line inside a
+    record (the rest of that record is dropped), CR line ends, an over-long
+    query record (skipped under a small -qRAM) and queries split over three
+    files so that RAM loads span files."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t = synth.make_target(rng, 40_000, n_contigs=4, median=9000)
+    q = synth.make_reads(rng, t, 150)
+    tp = os.path.join(tmp, "tadv%d.fa" % seed)
+    with open(tp, "wb") as f:
+        f.write(b"ACGTACGTACGTACGT\n@77\n")  # before any header: ignored / applies to record 0
+        for i in range(len(t)):
+            s = t.seq(i).tobytes()
+            f.write(b">ctg%d\r\n" % i if i == 2 else b">ctg%d\n" % i)
+            for k in range(0, len(s), 80):
+                f.write(s[k:k + 80] + b"\n")
+            if i == 1:
+                f.write(b"@%d\n" % 4242)  # after the sequence: belongs to this record
+        f.write(b">\nACGTACGTACGTACGTACGTACGTACGTACGT\n")  # empty header: dropped
+    long_read = synth.make_reads(rng, t, 1, length=7000)
+    qs = [os.path.join(tmp, "qadv%d_%d.fa" % (seed, k)) for k in range(3)]
+    fs = [open(p, "wb") for p in qs]
+    try:
+        for i in range(len(q)):
+            f = fs[min(2, i * 3 // len(q))]
+            s = q.seq(i).tobytes()
+            f.write(b">read%d\n" % i)
+            if i % 17 == 5:  # a blank line inside the record: only the first half counts
+                f.write(s[:80] + b"\n\n" + s[80:] + b"\n")
+            else:
+                f.write(s[:75] + b"\n" + s[75:] + b"\n")
+            if i == len(q) // 2:
+                f.write(b">long\n" + long_read.seq(0).tobytes() + b"\n")
+    finally:
+        for f in fs:
+            f.close()
+    return tp, qs

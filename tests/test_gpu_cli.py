@@ -7,7 +7,7 @@ import pytest
 
 import oracle as O
 from clast_b200 import api
-from _fasta import write_pair, write_quirky
+from _fasta import write_adversarial, write_pair, write_quirky
 
 pytestmark = pytest.mark.gpu
 
@@ -41,5 +41,13 @@ def test_cli_matches_oracle(tmp_path, extra):
 def test_cli_quirky_fasta(tmp_path):
     tp, qps = write_quirky(str(tmp_path), 7)
     a, b = run_both(str(tmp_path), ["-t", tp, "-q"] + qps + ["-qRAM", "0.01"])
+    assert b.count(b"\n") > 20
+    assert a == b
+
+
+@pytest.mark.parametrize("budgets", [[], ["-tRAM", "0.02", "-qRAM", "0.012"]])
+def test_cli_adversarial_fasta(tmp_path, budgets):
+    tp, qps = write_adversarial(str(tmp_path), 11)
+    a, b = run_both(str(tmp_path), ["-t", tp, "-q"] + qps + budgets)
     assert b.count(b"\n") > 20
     assert a == b
