@@ -129,7 +129,9 @@ __device__ __forceinline__ int64_t record_home16(uint32_t code, int l, uint32_t 
 }
 // Filter hash of a code: an xorshift then a multiply by an odd constant
 // (Fibonacci hashing).  The top bits select the 32-bit filter word, bits
-// 16..30 the three filter bits.
+// 16..30 the three filter bits.  (Filter words taken from the code's own top
+// bits, which would let the sorted codes fill the filter without atomics,
+// measured slower at lookup time.)
 __host__ __device__ __forceinline__ uint64_t key_hash(uint64_t code) {
   return (code ^ (code >> 31)) * 0x9E3779B97F4A7C15ull;
 }

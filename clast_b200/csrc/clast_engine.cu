@@ -243,25 +243,27 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix, un
   int32_t* pos2 = pbits ? nullptr : ws.get<int32_t>("ix_pos2", ns);
   sample_keys(packed, nmask, ns, p->stride, l, pbits, items, pos, st);
   const int in_alt = radix_sort_u64(ws, items, pos, items2, pos2, ns, pbits, pbits + 2 * l + 1, st);
+  // key heads (first sample of every valid code) come with the split
+  const uint64_t bound = 1ull << (2 * l);  // the code of l-mers with a non-ACGT base
   uint64_t* keys;
   int32_t* vals;
+  int32_t* head = ws.get<int32_t>("ix_head", ns);
   if (pbits) {
     keys = ws.get<uint64_t>("ix_keys", ns);
     vals = ws.get<int32_t>("ix_vals", ns);
-    split_items(in_alt ? items2 : items, ns, pbits, keys, vals, st);
+    split_items(in_alt ? items2 : items, ns, pbits, bound, keys, vals, head, st);
   } else {
     keys = in_alt ? items2 : items;
     vals = in_alt ? pos2 : pos;
+    index_heads(keys, ns, bound, head, st);
   }
   // From here on no host synchronisation: every array is sized for the ns
   // samples (an upper bound of the valid samples nv, the unique keys nu and
   // the entries); nv = *nv_dev and nu = hpos[ns] stay on the device.
   int64_t* nv_dev = ws.get<int64_t>("ix_nv", 1);
-  if (ns > 0) count_below(keys, ns, 1ull << (2 * l), nv_dev, st);
+  if (ns > 0) count_below(keys, ns, bound, nv_dev, st);
   else CLAST_CK(cudaMemsetAsync(nv_dev, 0, sizeof(int64_t), st));
-  int32_t* head = ws.get<int32_t>("ix_head", ns);
   int64_t* hpos = ws.get<int64_t>("ix_hpos", ns + 1);
-  index_heads(keys, ns, nv_dev, head, st);
   scan_i32(ws, head, ns, hpos, st);
   const int64_t* nu_dev = hpos + ns;
   uint64_t* ukeys = ws.get<uint64_t>("ix_ukeys", ns);
@@ -284,16 +286,10 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix, un
   const int64_t nb = std::max<int64_t>(1, ns);
   if (nb >= (int64_t)UINT32_MAX) throw std::invalid_argument("window has too many sampled l-mers");
   ix->nbuckets = (uint32_t)nb;
-  int32_t* kept = ws.get<int32_t>("ix_kept", ns);
   int64_t* rank = ws.get<int64_t>("ix_rank", ns + 1);
-  table_kept(ucnt, ns, kept, st);
-  scan_i32(ws, kept, ns, rank, st);
-  int64_t* slack = ws.get<int64_t>("ix_slack", ns);
+  scan_positive(ws, ucnt, ns, rank, st);
   int64_t* run_max = ws.get<int64_t>("ix_runmax", ns);
-  // past the kept codes the slack stays far below any home record (0x80... bytes)
-  CLAST_CK(cudaMemsetAsync(slack, 0x80, (size_t)std::max<int64_t>(ns, 1) * sizeof(int64_t), st));
-  table_slack(ukeys, ucnt, rank, ns, l, ix->nbuckets, slack, st);
-  maxscan_i64(ws, slack, ns, run_max, st);
+  table_runmax(ws, ukeys, ucnt, rank, ns, l, ix->nbuckets, run_max, st);
   ix->n_records = 2 * nb + (1 << 16);
   ix->table.alloc((size_t)ix->n_records);
   CLAST_CK(cudaMemsetAsync(ix->table.p, 0xff, (size_t)ix->n_records * sizeof(ulonglong2), st));
@@ -951,6 +947,28 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     S.map_launches = S.query_bases = S.query_kmers = S.seeds = S.hits = S.results = S.dp_cells = 0;
     ctx->timer.reset();
     const int64_t nreads = reads->n_seqs;
+    const int64_t nb = reads->offsets[nreads] - reads->offsets[0];
+    // The reads' bases go up first, on the copy stream (allocated there, so
+    // nothing waits for the compute stream, which may still be building the
+    // target indexes), so that the host preparation below overlaps the
+    // transfer; the compute stream waits for the uploads further down and
+    // frees the buffers in its order.
+    cudaStream_t cs = ctx->st_copy;
+    CLAST_CK(cudaEventRecord(ctx->ev0, cs));
+    DevArray<char> draw;
+    const char* rsrc = reads->bases + reads->offsets[0];
+    if (!reads->bases_on_device) {
+      g_alloc_stream = cs;
+      draw.alloc((size_t)nb + 64);
+      g_alloc_stream = st;
+      draw.st = st;
+      if (nb) CLAST_CK(cudaMemcpyAsync(draw.p, rsrc, nb, cudaMemcpyHostToDevice, cs));
+      rsrc = draw.p;
+      // the compute stream, which frees draw (also when a check below
+      // throws), comes after the copy
+      CLAST_CK(cudaEventRecord(ctx->ev3, cs));
+      CLAST_CK(cudaStreamWaitEvent(st, ctx->ev3, 0));
+    }
     // query windows of every load, in read order
     std::vector<int64_t> wfirst;
     std::vector<int64_t> load_first(n_loads + 1, 0);
@@ -961,7 +979,6 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     std::vector<int32_t> wstart(wfirst.size());
     for (size_t i = 0; i < wfirst.size(); ++i) wstart[i] = (int32_t)(2 * wfirst[i]);
     // every read uploaded once; strands are built on the device
-    const int64_t nb = reads->offsets[nreads] - reads->offsets[0];
     std::vector<int64_t> off0;
     const int64_t* offs_rel = reads->offsets;  // offsets relative to the first read
     if (reads->offsets[0] != 0) {
@@ -969,18 +986,13 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
       for (int64_t i = 0; i <= nreads; ++i) off0[i] = reads->offsets[i] - reads->offsets[0];
       offs_rel = off0.data();
     }
-    // uploads go on the copy stream (allocated there, so nothing waits for the
-    // compute stream, which may still be building the target indexes); the
-    // compute stream waits for them below and frees the buffers in its order
-    DevArray<char> draw;
     DevArray<int64_t> doff;
-    g_alloc_stream = ctx->st_copy;
-    if (!reads->bases_on_device) draw.alloc((size_t)nb + 64);
+    g_alloc_stream = cs;
     doff.alloc((size_t)nreads + 1);
     QueryBatch qb;
     qb.wstart.alloc(wstart.size());
     g_alloc_stream = st;
-    draw.st = doff.st = qb.wstart.st = st;
+    doff.st = qb.wstart.st = st;
     qb.n = 2 * nb;
     qb.nstrands = (int32_t)(2 * nreads);
     qb.min_len = nreads ? INT32_MAX : 0;
@@ -995,13 +1007,6 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     qb.len.alloc(2 * nreads);
     qb.nwin = (int32_t)wfirst.size() - 1;
     S.map_prep_ms = wall_ms() - w0;
-    cudaStream_t cs = ctx->st_copy;
-    CLAST_CK(cudaEventRecord(ctx->ev0, cs));
-    const char* rsrc = reads->bases + reads->offsets[0];
-    if (!reads->bases_on_device) {
-      if (nb) CLAST_CK(cudaMemcpyAsync(draw.p, rsrc, nb, cudaMemcpyHostToDevice, cs));
-      rsrc = draw.p;
-    }
     CLAST_CK(cudaMemcpyAsync(doff.p, offs_rel, (nreads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, cs));
     CLAST_CK(cudaMemcpyAsync(qb.wstart.p, wstart.data(), wstart.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
                              cs));

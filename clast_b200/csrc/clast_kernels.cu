@@ -44,9 +44,20 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 // ------------------------------------------------------------------------
 constexpr int kScanThreads = 256, kScanItems = 8, kScanTile = kScanThreads * kScanItems;
 
+// Element loaders of the scans: an array, or a flag computed from one.
 template <class T>
-__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const T* __restrict__ in, int64_t n_in,
-                                                             int64_t n_out, int64_t* __restrict__ out,
+struct ArrayLoad {
+  const T* __restrict__ p;
+  __device__ __forceinline__ int64_t operator()(int64_t i) const { return (int64_t)p[i]; }
+};
+struct PositiveLoad {  // 1 where p[i] > 0
+  const int32_t* __restrict__ p;
+  __device__ __forceinline__ int64_t operator()(int64_t i) const { return p[i] > 0 ? 1 : 0; }
+};
+
+template <class Load>
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(Load in, int64_t n_in, int64_t n_out,
+                                                             int64_t* __restrict__ out,
                                                              int64_t* __restrict__ tile_sums) {
   __shared__ int64_t warp_tot[kScanThreads / 32];
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
@@ -55,7 +66,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const T* __restrict
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     const int64_t idx = base + i;
-    v[i] = (idx < n_in) ? (int64_t)in[idx] : 0;
+    v[i] = (idx < n_in) ? in(idx) : 0;
     s += v[i];
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -89,17 +100,143 @@ __global__ void k_scan_add(int64_t* __restrict__ out, int64_t n_out, const int64
   if (i < n_out) out[i] += tile_pre[i / kScanTile];
 }
 
-template <class T>
-void scan_impl(Workspace& ws, const T* in, int64_t n, int64_t* out, cudaStream_t st, int level) {
+// ---- single-pass exclusive scan (decoupled look-back) ----
+// Tiles take their index from a counter in launch order, so a tile only waits
+// for tiles that have already started.  Each tile publishes its aggregate,
+// then its first warp walks back over the predecessors' words, 32 at a time
+// (flag in the top two bits: aggregate or inclusive prefix), until it meets an
+// inclusive prefix.  The walk waits at most kScanSpinLimit polls per step;
+// past that the tile sums the inputs before it directly, so no tile can wait
+// for ever.  For non-negative inputs (counts and flags) with sums below 2^62.
+constexpr uint64_t kScanAgg = 1ull << 62, kScanInc = 2ull << 62, kScanValue = (1ull << 62) - 1;
+constexpr int kScanSpinLimit = 1 << 16;
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <class Load>
+__global__ void __launch_bounds__(kScanThreads) k_scan_1pass(Load in, int64_t n_in, int64_t n_out,
+                                                             int64_t* __restrict__ out,
+                                                             unsigned long long* __restrict__ state) {
+  __shared__ int64_t warp_tot[kScanThreads / 32];
+  __shared__ int64_t s_prefix;
+  __shared__ unsigned long long s_tile;
+  __shared__ int s_fallback;
+  unsigned long long* status = state + 1;  // state[0]: the tile counter
+  if (threadIdx.x == 0) s_tile = atomicAdd(state, 1ull);
+  __syncthreads();
+  const int64_t t = (int64_t)s_tile;
+  const int64_t base = t * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int64_t v[kScanItems];
+  int64_t sum = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int64_t idx = base + i;
+    v[i] = (idx < n_in) ? in(idx) : 0;
+    sum += v[i];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  int64_t wpre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < kScanThreads / 32; ++w) {
+    const int64_t x = warp_tot[w];
+    if (w < warp) wpre += x;
+    tot += x;
+  }
+  if (warp == 0) {
+    int64_t run = 0;
+    int fallback = 0;
+    if (t == 0) {
+      if (lane == 0) st_relaxed_u64(status, kScanInc | (unsigned long long)tot);
+    } else {
+      if (lane == 0) st_relaxed_u64(status + t, kScanAgg | (unsigned long long)tot);
+      for (int64_t j = t - 1;; j -= 32) {
+        // lane L reads tile j - L; tiles before 0 read as an inclusive 0
+        const int64_t jj = j - lane;
+        unsigned long long w = jj >= 0 ? ld_relaxed_u64(status + jj) : kScanInc;
+        for (int spin = 0; __any_sync(kFull, (w >> 62) == 0) && spin < kScanSpinLimit; ++spin)
+          if ((w >> 62) == 0) w = ld_relaxed_u64(status + jj);
+        if (__any_sync(kFull, (w >> 62) == 0)) {
+          fallback = 1;
+          break;
+        }
+        const unsigned inc = __ballot_sync(kFull, (w & kScanInc) != 0);
+        const int last = inc ? __ffs(inc) - 1 : 31;  // nearest inclusive prefix, else the whole step
+        int64_t x = lane <= last ? (int64_t)(w & kScanValue) : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+        run += x;
+        if (inc) break;
+      }
+    }
+    if (lane == 0) {
+      s_prefix = run;
+      s_fallback = fallback;
+    }
+  }
+  __syncthreads();
+  if (s_fallback) {  // a predecessor never published: sum the inputs before this tile
+    int64_t part = 0;
+    for (int64_t i = threadIdx.x; i < t * kScanTile && i < n_in; i += kScanThreads) part += in(i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+    __syncthreads();
+    if (lane == 0) warp_tot[warp] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int64_t run = 0;
+      for (int w = 0; w < kScanThreads / 32; ++w) run += warp_tot[w];
+      s_prefix = run;
+      st_relaxed_u64(status + t, kScanInc | (unsigned long long)(run + tot));
+    }
+    __syncthreads();
+  } else if (threadIdx.x == 0 && t > 0) {
+    st_relaxed_u64(status + t, kScanInc | (unsigned long long)(s_prefix + tot));
+  }
+  int64_t run = s_prefix + wpre + incl - sum;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int64_t idx = base + i;
+    if (idx < n_out) out[idx] = run;
+    run += v[i];
+  }
+}
+
+template <class Load>
+void scan_1pass(Workspace& ws, Load in, int64_t n, int64_t* out, cudaStream_t st) {
+  const int64_t n_out = n + 1;
+  const int64_t tiles = (n_out + kScanTile - 1) / kScanTile;
+  unsigned long long* state = ws.get<unsigned long long>("scan1_state", tiles + 1);
+  CLAST_CK(cudaMemsetAsync(state, 0, (tiles + 1) * sizeof(unsigned long long), st));
+  k_scan_1pass<Load><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, n_out, out, state);
+  CLAST_LAUNCHED();
+}
+
+template <class Load>
+void scan_impl(Workspace& ws, Load in, int64_t n, int64_t* out, cudaStream_t st, int level) {
   const int64_t n_out = n + 1;
   const int64_t tiles = (n_out + kScanTile - 1) / kScanTile;
   const std::string tag = "scan" + std::to_string(level);
   int64_t* sums = ws.get<int64_t>(tag + "s", tiles);
-  k_scan_tiles<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, n_out, out, sums);
+  k_scan_tiles<Load><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, n_out, out, sums);
   CLAST_LAUNCHED();
   if (tiles > 1) {
     int64_t* pre = ws.get<int64_t>(tag + "p", tiles + 1);
-    scan_impl<int64_t>(ws, sums, tiles, pre, st, level + 1);
+    scan_impl(ws, ArrayLoad<int64_t>{sums}, tiles, pre, st, level + 1);
     k_scan_add<<<blocks_for(n_out, 256), 256, 0, st>>>(out, n_out, pre);
     CLAST_LAUNCHED();
   }
@@ -196,16 +333,31 @@ __global__ void k_strand_meta(const int64_t* __restrict__ off, int64_t n_reads, 
 
 // One warp per read: the '+' strand copy and the reverse complement are both
 // coalesced (the reversed writes of a warp still cover one contiguous run).
+// The read goes in chunks of 8 x 32 bytes whose loads are all issued before
+// the first store, so a short read waits for memory once.
 __global__ void k_strands(const char* __restrict__ reads, const int64_t* __restrict__ off, int64_t n_reads,
                           char* __restrict__ out) {
   const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (r >= n_reads) return;
   const int64_t a = off[r], len = off[r + 1] - a;
-  for (int64_t j = lane; j < len; j += 32) {
-    const char c = reads[a + j];
-    out[2 * a + j] = c;
-    out[2 * a + len + (len - 1 - j)] = complement(c);
+  char* const fwd = out + 2 * a;
+  char* const rev = out + 2 * a + 2 * len - 1;  // base j of the read -> rev[-j]
+  for (int64_t j0 = 0; j0 < len; j0 += 8 * 32) {
+    char c[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t j = j0 + u * 32 + lane;
+      c[u] = j < len ? reads[a + j] : 'N';
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t j = j0 + u * 32 + lane;
+      if (j < len) {
+        fwd[j] = c[u];
+        rev[-j] = complement(c[u]);
+      }
+    }
   }
 }
 
@@ -233,18 +385,26 @@ __global__ void k_build_window(const char* __restrict__ src, const int64_t* __re
   int lo = first_seq;
   while (lo + 1 < nseqs && (int64_t)gw[lo + 1] <= b0) ++lo;
   unsigned char c[16];
+  const int64_t j0 = b0 - gw[lo];
+  if (b0 + 16 <= n && j0 + 16 <= (int64_t)len[lo]) {
+    // inside one sequence's bases: independent loads
+    const char* p = src + src_off[lo] + j0;
 #pragma unroll
-  for (int k = 0; k < 16; ++k) {
-    const int64_t i = b0 + k;
-    while (lo + 1 < nseqs && (int64_t)gw[lo + 1] <= i) ++lo;
-    const int64_t j = i - gw[lo];
-    const int64_t L = len[lo];
-    char v = 'N';
-    if (i < n) {
-      if (j < L) v = src[src_off[lo] + j];
-      else if (j - L < L) v = src[src_off[lo] + (j - L)];
+    for (int k = 0; k < 16; ++k) c[k] = (unsigned char)p[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int64_t i = b0 + k;
+      while (lo + 1 < nseqs && (int64_t)gw[lo + 1] <= i) ++lo;
+      const int64_t j = i - gw[lo];
+      const int64_t L = len[lo];
+      char v = 'N';
+      if (i < n) {
+        if (j < L) v = src[src_off[lo] + j];
+        else if (j - L < L) v = src[src_off[lo] + (j - L)];
+      }
+      c[k] = (unsigned char)v;
     }
-    c[k] = (unsigned char)v;
   }
   if (b0 + 16 <= n) {
     uint4 q;
@@ -279,22 +439,29 @@ __global__ void k_sample_keys(const uint64_t* __restrict__ packed, const uint64_
   }
 }
 
-__global__ void k_split_items(const uint64_t* __restrict__ items, int64_t n, int pbits, uint64_t* __restrict__ keys,
-                              int32_t* __restrict__ vals) {
+// keys / vals of the sorted words, and head[i] = whether key i is valid
+// (< bound) and differs from key i - 1.
+__global__ void k_split_items(const uint64_t* __restrict__ items, int64_t n, int pbits, uint64_t bound,
+                              uint64_t* __restrict__ keys, int32_t* __restrict__ vals, int32_t* __restrict__ head) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint64_t v = items[i];
-  keys[i] = v >> pbits;
+  const uint64_t k = v >> pbits;
+  keys[i] = k;
   vals[i] = (int32_t)(v & ((1ull << pbits) - 1));
+  head[i] = (k < bound && (i == 0 || (items[i - 1] >> pbits) != k)) ? 1 : 0;
 }
 
 // ---- LSD radix sort of 64-bit words by a bit range, 8 bits per pass ----
 // A block takes a tile of kRsTile consecutive words; warp w owns words
 // [w * kRsWarpItems, (w + 1) * kRsWarpItems) of it.  Each pass: per-block digit
 // counts (k_rs_hist), one scan of the counts laid out digit-major, then
-// k_rs_scatter ranks the tile stably in shared memory (warp-private digit
-// counters, ranks inside 32-word steps by match_any) and writes every digit's
-// run out contiguously.
+// k_rs_scatter ranks the tile stably in shared memory and writes every
+// digit's run out contiguously.  Ranking takes one step per 32 words: the
+// lanes holding the same digit are found with eight ballots (one per digit
+// bit), the lowest of them adds the group's size to the warp's counter of that
+// digit, and each lane's rank is the counter's old value plus the lanes of its
+// group below it.
 constexpr int kRsThreads = 256, kRsItems = 16, kRsTile = kRsThreads * kRsItems;
 constexpr int kRsWarps = kRsThreads / 32, kRsWarpItems = 32 * kRsItems;
 
@@ -313,15 +480,27 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint64_t* __restri
   hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
+// Lanes of the warp whose 8-bit digit equals this lane's, among the lanes in `among`.
+__device__ __forceinline__ unsigned digit_peers(unsigned d, unsigned among) {
+  unsigned peers = among;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const unsigned bit = (d >> b) & 1u;
+    const unsigned bb = __ballot_sync(kFull, bit);
+    peers &= bit ? bb : ~bb;
+  }
+  return peers;
+}
+
 // PAY: a 32-bit value travels with every word (vin -> vout).  Dynamic shared
 // memory: the staged tile, kRsTile words (+ kRsTile values).
 template <bool PAY>
-__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __restrict__ kin,
+__global__ void __launch_bounds__(kRsThreads, 3) k_rs_scatter(const uint64_t* __restrict__ kin,
                                                            const int32_t* __restrict__ vin,
                                                            uint64_t* __restrict__ kout, int32_t* __restrict__ vout,
                                                            int64_t n, int shift, const int64_t* __restrict__ offs,
                                                            int nblocks) {
-  __shared__ uint32_t wc[kRsWarps][256];  // per-warp digit counters, then running positions
+  __shared__ uint32_t wc[kRsWarps][256];  // per-warp digit counters, then the warps' run starts
   __shared__ uint32_t tile_start[256];
   __shared__ uint32_t wsum[kRsWarps];
   __shared__ int64_t goff[256];
@@ -331,21 +510,31 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
   goff[tid] = offs[(int64_t)tid * nblocks + blockIdx.x];
 #pragma unroll
   for (int w = 0; w < kRsWarps; ++w) wc[w][tid] = 0;
-  __syncthreads();
   const int64_t base = (int64_t)blockIdx.x * kRsTile + (int64_t)warp * kRsWarpItems;
   const unsigned lt = lanemask_lt();
   uint64_t k[kRsItems];
   int32_t v[PAY ? kRsItems : 1];
-  // warp-private digit counts, in word order
 #pragma unroll
   for (int r = 0; r < kRsItems; ++r) {
     const int64_t idx = base + r * 32 + lane;
     k[r] = idx < n ? kin[idx] : 0ull;
     if (PAY) v[r] = idx < n ? vin[idx] : 0;
-    const unsigned d = idx < n ? (unsigned)((k[r] >> shift) & 255) : 256u;
-    const unsigned peers = __match_any_sync(kFull, d);
-    if (d < 256u && lane == __ffs(peers) - 1) wc[warp][d] += __popc(peers);
-    __syncwarp();
+  }
+  __syncthreads();
+  // stable ranks within the warp's runs, two 16-bit ranks per register
+  uint32_t rk[kRsItems / 2];
+#pragma unroll
+  for (int r = 0; r < kRsItems; ++r) {
+    const bool ok = base + r * 32 + lane < n;
+    const unsigned d = (unsigned)(k[r] >> shift) & 255u;
+    const unsigned peers = digit_peers(d, __ballot_sync(kFull, ok));
+    const int leader = __ffs(peers) - 1;  // -1 only for a lane past n
+    uint32_t old = 0;
+    if (ok && lane == leader) old = atomicAdd(&wc[warp][d], (uint32_t)__popc(peers));
+    old = __shfl_sync(kFull, old, leader & 31);
+    const uint32_t rank = old + (uint32_t)__popc(peers & lt);
+    if (r & 1) rk[r >> 1] |= rank << 16;
+    else rk[r >> 1] = rank;
   }
   __syncthreads();
   // digit d = tid: tile-wide start (exclusive scan over digits), then the
@@ -371,20 +560,15 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
     start += c;
   }
   __syncthreads();
-  // stable positions inside the tile
+  // stage the tile in sorted order
 #pragma unroll
   for (int r = 0; r < kRsItems; ++r) {
-    const int64_t idx = base + r * 32 + lane;
-    const unsigned d = idx < n ? (unsigned)((k[r] >> shift) & 255) : 256u;
-    const unsigned peers = __match_any_sync(kFull, d);
-    if (d < 256u) {
-      const uint32_t at = wc[warp][d] + __popc(peers & lt);
+    if (base + r * 32 + lane < n) {
+      const unsigned d = (unsigned)(k[r] >> shift) & 255u;
+      const uint32_t at = wc[warp][d] + ((rk[r >> 1] >> (16 * (r & 1))) & 0xffffu);
       stage[at] = k[r];
       if (PAY) stage_v[at] = v[r];
     }
-    __syncwarp();
-    if (d < 256u && lane == __ffs(peers) - 1) wc[warp][d] += __popc(peers);
-    __syncwarp();
   }
   __syncthreads();
   // digit runs out, contiguous
@@ -414,10 +598,10 @@ __global__ void k_count_below(const uint64_t* __restrict__ keys, int64_t n, uint
 // samples (an upper bound) and read the counts that matter from the device
 // (*nv valid samples; *nu = hpos[n] unique keys, as the scans end with the
 // total and every flag past the valid range is 0).
-__global__ void k_index_heads(const uint64_t* __restrict__ k, int64_t n, const int64_t* __restrict__ nv_dev,
+__global__ void k_index_heads(const uint64_t* __restrict__ k, int64_t n, uint64_t bound,
                               int32_t* __restrict__ head) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) head[i] = (i < *nv_dev && (i == 0 || k[i] != k[i - 1])) ? 1 : 0;
+  if (i < n) head[i] = (k[i] < bound && (i == 0 || k[i] != k[i - 1])) ? 1 : 0;
 }
 
 __global__ void k_index_unique(const uint64_t* __restrict__ k, const int32_t* __restrict__ head,
@@ -484,18 +668,20 @@ __global__ void k_index_buckets(const int64_t* __restrict__ ufirst, const int64_
 // r = rank among the kept codes, linear probing puts code r at
 // max(home_r, pos_{r-1} + 1) = r + max_{j <= r}(home_j - j).
 
-__global__ void k_table_kept(const int32_t* __restrict__ ucnt, int64_t n, int32_t* __restrict__ kept) {
-  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) kept[k] = ucnt[k] > 0 ? 1 : 0;  // 0: removed by the repeat cut, joints only, or past the keys
-}
-
-__global__ void k_table_slack(const uint64_t* __restrict__ ucode, const int32_t* __restrict__ ucnt,
-                              const int64_t* __restrict__ rank, int64_t n, int l, uint32_t nbuckets,
-                              int64_t* __restrict__ slack) {
-  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n || ucnt[k] <= 0) return;
-  slack[rank[k]] = record_home(ucode[k], l, nbuckets) - rank[k];
-}
+// The running maximum is taken over the unique codes k (not over the ranks):
+// for kept code k it equals max over kept j <= k of home_j - rank_j.  Codes
+// without entries (repeat cut, joints only, past the keys: ucnt 0) count as
+// INT64_MIN.
+struct SlackLoad {
+  const uint64_t* __restrict__ ucode;
+  const int32_t* __restrict__ ucnt;
+  const int64_t* __restrict__ rank;
+  int l;
+  uint32_t nbuckets;
+  __device__ __forceinline__ int64_t operator()(int64_t k) const {
+    return ucnt[k] > 0 ? record_home(ucode[k], l, nbuckets) - rank[k] : INT64_MIN;
+  }
+};
 
 __global__ void k_table_place(const uint64_t* __restrict__ ucode, const int32_t* __restrict__ ustart,
                               const int32_t* __restrict__ ucnt, const int2* __restrict__ entries,
@@ -516,15 +702,14 @@ __global__ void k_table_place(const uint64_t* __restrict__ ucode, const int32_t*
   } else {
     payload = kMulti | ((uint64_t)(uint32_t)ustart[k] << 32) | (uint32_t)c;
   }
-  const int64_t r = rank[k];
-  const int64_t pos = r + run_max[r];
+  const int64_t pos = rank[k] + run_max[k];
   if (pos >= 0 && pos < n_records) table[pos] = make_ulonglong2(code, payload);
   else atomicAdd(failed, 1ull);  // unreachable: positions rise to the last one, which the table holds
 }
 
 // ---- inclusive running maximum (int64) ----
-__global__ void __launch_bounds__(kScanThreads) k_maxscan_tiles(const int64_t* __restrict__ in, int64_t n,
-                                                                int64_t* __restrict__ out,
+template <class Load>
+__global__ void __launch_bounds__(kScanThreads) k_maxscan_tiles(Load in, int64_t n, int64_t* __restrict__ out,
                                                                 int64_t* __restrict__ tile_max) {
   __shared__ int64_t warp_max[kScanThreads / 32];
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
@@ -533,7 +718,7 @@ __global__ void __launch_bounds__(kScanThreads) k_maxscan_tiles(const int64_t* _
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     const int64_t idx = base + i;
-    v[i] = (idx < n) ? in[idx] : INT64_MIN;
+    v[i] = (idx < n) ? in(idx) : INT64_MIN;
     m = v[i] > m ? v[i] : m;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -576,12 +761,13 @@ __global__ void k_maxscan_apply(int64_t* __restrict__ out, int64_t n, const int6
 // ------------------------------------------------------------------------
 // Seeding in one pass, one warp per strand.  The strand's l-mers go in rounds
 // of 32 * kSeedPerLane; in a round lane L takes the kSeedPerLane consecutive
-// l-mers from L * kSeedPerLane, so it reads their 2-bit words once and shifts
-// each key out of them.  The lookups of a round are issued together, level by
-// level (2-bit words → filter words → home records → second records), so a
-// strand waits about one latency per level.  Round 0's results stay in
-// registers for the write pass (one round covers 160 l-mers: a 164 bp strand);
-// later rounds are looked up again when written.  The strand's seeds get one
+// l-mers from L * kSeedPerLane, so it reads their 2-bit words and N flags once
+// and shifts each key out of them.  The lookups of a round are issued
+// together, level by level (2-bit words and N flags → filter words → home
+// buckets), so a strand waits about one latency per level.  Round 0's results
+// are staged for the write pass while the range reservation is in flight (one
+// round covers 160 l-mers: a 164 bp strand); later rounds are looked up again
+// when written.  The strand's seeds get one
 // contiguous range from an atomic cursor; if the range would pass `cap`,
 // nothing is written and the host reruns with a larger buffer (the cursor then
 // holds the exact total).  Seeds are written in l-mer order, so the seeds of a
@@ -592,9 +778,21 @@ constexpr int kSeedParts = 32;
 
 // Payloads of the l-mers qi = r0 + lane * P + i (i < P) of a strand; invalid or
 // absent ones get kNoPayload.  Returns the number of valid l-mers.
+// Both records of a home bucket: one 256-bit streaming load (sm_100), the
+// address 32-byte aligned (home records are even, the table 256-byte aligned).
+__device__ __forceinline__ void ld_bucket(const ulonglong2* a, uint64_t& c0, uint64_t& p0, uint64_t& c1,
+                                          uint64_t& p1) {
+  asm volatile("ld.global.cs.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(c0), "=l"(p0), "=l"(c1), "=l"(p1) : "l"(a));
+}
+
+// (hi << s) | (lo >> (64 - s)) for s in [0, 63]: the 64 bits from bit s of hi:lo
+__device__ __forceinline__ uint64_t funnel64(uint64_t hi, uint64_t lo, int s) {
+  return (hi << s) | ((lo >> 1) >> (63 - s));
+}
+
 template <bool SMALL>
 __device__ __forceinline__ int round_lookup(const QueryView& q, const IndexView& ix, int64_t st, int nk, int r0,
-                                            int lane, bool any_n, uint64_t (&pl)[kSeedPerLane]) {
+                                            int lane, uint64_t (&pl)[kSeedPerLane]) {
   constexpr int P = kSeedPerLane;
   const int q0 = r0 + lane * P;
   const int nv = max(0, min(P, nk - q0));  // valid l-mer slots of this lane
@@ -602,12 +800,20 @@ __device__ __forceinline__ int round_lookup(const QueryView& q, const IndexView&
   uint32_t vmask = 0;
   if (nv > 0) {
     const int64_t f = st + q0;
+    // The lane's P l-mers span P - 1 + l <= 35 bases from f: their 2-bit words
+    // and non-ACGT flags are read in one batch.  An l-mer with a non-ACGT base
+    // is not looked up (SRepelHasOddBase).
+    vmask = (1u << nv) - 1;
     if (SMALL) {
-      // the P keys lie in 16-base units j0 .. j0 + 2 (unit j = 32-bit element j ^ 1)
+      // 16-base units j0 .. j0 + 2 of the codes, 32-base units k0, k0 + 1 of
+      // the flags (unit j = 32-bit element j ^ 1)
       const uint32_t* p32 = reinterpret_cast<const uint32_t*>(q.packed);
-      const int64_t j0 = f >> 4;
+      const uint32_t* n32 = reinterpret_cast<const uint32_t*>(q.nmask);
+      const int64_t j0 = f >> 4, k0 = f >> 5;
       const uint32_t u0 = __ldcs(p32 + (j0 ^ 1)), u1 = __ldcs(p32 + ((j0 + 1) ^ 1)),
                      u2 = __ldcs(p32 + ((j0 + 2) ^ 1));
+      const uint32_t m0 = __ldcs(n32 + (k0 ^ 1)), m1 = __ldcs(n32 + ((k0 + 1) ^ 1));
+      const uint32_t nflag = __funnelshift_l(m1, m0, (int)(f & 31));  // base f in the top bit
       const int o = 2 * (int)(f & 15);
       const uint32_t mask = (2 * ix.l == 32) ? ~0u : ((1u << (2 * ix.l)) - 1);
 #pragma unroll
@@ -616,20 +822,22 @@ __device__ __forceinline__ int round_lookup(const QueryView& q, const IndexView&
         const uint32_t x = bo < 32 ? __funnelshift_l(u1, u0, bo) : __funnelshift_l(u2, u1, bo - 32);
         const uint32_t key = x >> (32 - 2 * ix.l);
         code[i] = (uint32_t)(key * (uint32_t)0x6659FD93u) & mask;  // order_code for l <= 16
+        if ((nflag << i) >> (32 - ix.l)) vmask &= ~(1u << i);
       }
     } else {
+      // 32-base words w0 .. w0 + 2 of the codes, 64-base words k0, k0 + 1 of the flags
+      const int64_t w0 = f >> 5, k0 = f >> 6;
+      const uint64_t u0 = ld_stream(q.packed + w0), u1 = ld_stream(q.packed + w0 + 1),
+                     u2 = ld_stream(q.packed + w0 + 2);
+      const uint64_t nflag = funnel64(ld_stream(q.nmask + k0), ld_stream(q.nmask + k0 + 1), (int)(f & 63));
+      const int o = 2 * (int)(f & 31);
 #pragma unroll
-      for (int i = 0; i < P; ++i) code[i] = i < nv ? order_code(kmer_key(q.packed, f + i, ix.l), ix.l) : 0ull;
-    }
-    vmask = (1u << nv) - 1;
-    // l-mers with a non-ACGT base are not looked up (SRepelHasOddBase)
-    if (any_n) {
-#pragma unroll
-      for (int i = 0; i < P; ++i)
-        if (((vmask >> i) & 1u) &&
-            (SMALL ? kmer_has_n16(reinterpret_cast<const uint32_t*>(q.nmask), f + i, ix.l)
-                   : kmer_has_n(q.nmask, f + i, ix.l)))
-          vmask &= ~(1u << i);
+      for (int i = 0; i < P; ++i) {
+        const int bo = o + 2 * i;  // < 2 * (31 + P)
+        const uint64_t x = bo < 64 ? funnel64(u0, u1, bo) : funnel64(u1, u2, bo - 64);
+        code[i] = order_code(x >> (64 - 2 * ix.l), ix.l);
+        if ((nflag << i) >> (64 - ix.l)) vmask &= ~(1u << i);
+      }
     }
   }
   uint32_t fw[P], fm[P];
@@ -639,42 +847,41 @@ __device__ __forceinline__ int round_lookup(const QueryView& q, const IndexView&
     fm[i] = filter_mask(h);
     fw[i] = ((vmask >> i) & 1u) ? __ldg(ix.filter + filter_word(h, ix.fshift)) : 0u;
   }
-  ulonglong2 rec[P];
-  uint32_t pmask = 0;
+  // The home bucket (records home and home + 1, one aligned 32-byte sector)
+  // in one load; only keys displaced past it probe further.
+  uint64_t c0[P], p0[P], c1[P], p1[P];
 #pragma unroll
   for (int i = 0; i < P; ++i) {
     const bool pass = ((vmask >> i) & 1u) && (fw[i] & fm[i]) == fm[i];
-    pmask |= (uint32_t)pass << i;
-    rec[i] = make_ulonglong2(0ull, kNoPayload);
+    c0[i] = 0ull;
+    p0[i] = kNoPayload;
+    c1[i] = 0ull;
+    p1[i] = kNoPayload;
     if (pass)
-      rec[i] = __ldcs(ix.table + (SMALL ? record_home16((uint32_t)code[i], ix.l, ix.nbuckets)
-                                        : record_home(code[i], ix.l, ix.nbuckets)));
+      ld_bucket(ix.table + (SMALL ? record_home16((uint32_t)code[i], ix.l, ix.nbuckets)
+                                  : record_home(code[i], ix.l, ix.nbuckets)),
+                c0[i], p0[i], c1[i], p1[i]);
   }
-  // resolve from the home records; the keys displaced further read the next
-  // record (the home bucket's second, same 32-byte sector) together
-  uint32_t more = 0;
 #pragma unroll
   for (int i = 0; i < P; ++i) {
-    pl[i] = kNoPayload;
-    if ((pmask >> i) & 1u) {
-      if (rec[i].x == code[i]) pl[i] = rec[i].y;
-      else if (rec[i].y != kNoPayload) more |= 1u << i;
-    }
-  }
-  if (__any_sync(kFull, more != 0)) {
-#pragma unroll
-    for (int i = 0; i < P; ++i)
-      if ((more >> i) & 1u)
-        rec[i] = __ldcs(ix.table + 1 + (SMALL ? record_home16((uint32_t)code[i], ix.l, ix.nbuckets)
-                                              : record_home(code[i], ix.l, ix.nbuckets)));
-#pragma unroll
-    for (int i = 0; i < P; ++i)
-      if ((more >> i) & 1u) {
-        if (rec[i].x == code[i] || rec[i].y == kNoPayload) pl[i] = rec[i].y;
-        else pl[i] = table_probe(ix, code[i], record_home(code[i], ix.l, ix.nbuckets) + 2);
-      }
+    if (c0[i] == code[i] || p0[i] == kNoPayload) pl[i] = p0[i];
+    else if (c1[i] == code[i] || p1[i] == kNoPayload) pl[i] = p1[i];
+    else pl[i] = table_probe(ix, code[i], record_home(code[i], ix.l, ix.nbuckets) + 2);
   }
   return __popc(vmask);
+}
+
+// Writes the seed of entry e (sequence within window, index within sequence)
+// for l-mer qi at w; tlen = length of sequence e.x (global mode only).
+__device__ __forceinline__ void seed_store(int2 e, int qi, int tlen, int gap, int local, int qlen, int64_t w,
+                                           int& valid, uint64_t* __restrict__ skey, uint32_t* __restrict__ sq) {
+  const int s0 = e.y - qi;  // tHitStartIdx, is_onCorner
+  const bool drop = !local && ((s0 + gap < 0) || (s0 + qlen - gap > tlen));
+  // streaming stores: the seeds must not evict the filter from L2
+  __stcs(reinterpret_cast<unsigned long long*>(skey + w),
+         drop ? kDroppedSeed : (((uint64_t)(uint32_t)e.x << 32) | ((uint32_t)s0 ^ 0x80000000u)));
+  __stcs(sq + w, (uint32_t)qi);
+  valid += drop ? 0 : 1;
 }
 
 // Writes the c = payload_count(pl) seeds of l-mer qi at w onwards.
@@ -686,13 +893,7 @@ __device__ __forceinline__ void seed_put(const IndexView& ix, const TargetView& 
   const int us = (int)(pl >> 32) & 0x7fffffff;
   for (int i = 0; i < c; ++i) {
     const int2 e = multi ? __ldcs(ix.entries + us + i) : make_int2((int)(pl >> 32), (int)(uint32_t)pl);
-    const int s0 = e.y - qi;  // tHitStartIdx, is_onCorner
-    const bool drop = !local && ((s0 + gap < 0) || (s0 + qlen - gap > t.lengths[e.x]));
-    // streaming stores: the seeds must not evict the filter from L2
-    __stcs(reinterpret_cast<unsigned long long*>(skey + w + i),
-           drop ? kDroppedSeed : (((uint64_t)(uint32_t)e.x << 32) | ((uint32_t)s0 ^ 0x80000000u)));
-    __stcs(sq + w + i, (uint32_t)qi);
-    valid += drop ? 0 : 1;
+    seed_store(e, qi, local ? 0 : t.lengths[e.x], gap, local, qlen, w + i, valid, skey, sq);
   }
 }
 
@@ -776,26 +977,49 @@ __global__ void __launch_bounds__(kSeedFusedThreads, SMALL ? 8 : 6) k_seed_fused
   const int64_t st = q.start[s];
   const int qlen = q.len[s];
   const int nk = qlen - ix.l + 1;
-  // does the strand hold a non-ACGT base?  (one vote over its mask words)
-  bool any_n = false;
-  if (qlen > 0) {
-    const int64_t w0 = st >> 6, w1 = (st + qlen - 1) >> 6;
-    for (int64_t w = w0 + lane; w <= w1; w += 32) {
-      uint64_t m = ld_stream(q.nmask + w);
-      if (w == w0) m &= ~0ull >> (st & 63);
-      if (w == w1) m &= ~0ull << (63 - ((st + qlen - 1) & 63));
-      any_n |= m != 0;
-    }
-  }
-  any_n = __any_sync(kFull, any_n);
   uint64_t pl0[P];
-  int valid_kmers = round_lookup<SMALL>(q, ix, st, nk, 0, lane, any_n, pl0);
+  int valid_kmers = round_lookup<SMALL>(q, ix, st, nk, 0, lane, pl0);
   int lane_cnt = 0;
+  bool multi0 = false;
 #pragma unroll
-  for (int i = 0; i < P; ++i) lane_cnt += payload_count(pl0[i]);
+  for (int i = 0; i < P; ++i) {
+    const int c = payload_count(pl0[i]);
+    lane_cnt += c;
+    multi0 |= c > 1;
+  }
+  // Round 0 is staged before its range is known: in the single-entry case
+  // lane j takes seed j of the round and reads its sequence length now, so
+  // that the load overlaps the range reservation below.
+  int rt0;
+  const int excl0 = warp_excl_scan(lane_cnt, lane, &rt0);
+  const bool simple0 = !__any_sync(kFull, multi0);
+  uint64_t* const spl = stage_pl[wib];
+  int32_t* const sqi = stage_qi[wib];
+  uint64_t pl_j = kNoPayload;
+  int qi_j = 0, tl_j = 0;
+  if (simple0) {
+    int k = excl0;
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+      if (pl0[i] != kNoPayload) {
+        spl[k] = pl0[i];
+        sqi[k] = lane * P + i;
+        ++k;
+      }
+    __syncwarp();
+    if (lane < rt0) {
+      pl_j = spl[lane];
+      qi_j = sqi[lane];
+      if (!local) tl_j = t.lengths[(int)(pl_j >> 32)];
+    }
+  } else {
+    // the payloads wait in the lane's own stage slots
+#pragma unroll
+    for (int i = 0; i < P; ++i) spl[lane * P + i] = pl0[i];
+  }
   for (int r0 = kSeedRound; r0 < nk; r0 += kSeedRound) {
     uint64_t pl[P];
-    valid_kmers += round_lookup<SMALL>(q, ix, st, nk, r0, lane, any_n, pl);
+    valid_kmers += round_lookup<SMALL>(q, ix, st, nk, r0, lane, pl);
 #pragma unroll
     for (int i = 0; i < P; ++i) lane_cnt += payload_count(pl[i]);
   }
@@ -820,11 +1044,28 @@ __global__ void __launch_bounds__(kSeedFusedThreads, SMALL ? 8 : 6) k_seed_fused
   }
   int valid = 0;
   int64_t w = (int64_t)base;
-  round_emit(ix, t, gap, local, qlen, 0, lane, pl0, w, valid, skey, sq, stage_pl[wib], stage_qi[wib]);
+  if (simple0) {
+    if (lane < rt0)
+      seed_store(make_int2((int)(pl_j >> 32), (int)(uint32_t)pl_j), qi_j, tl_j, gap, local, qlen, w + lane, valid,
+                 skey, sq);
+    for (int j = lane + 32; j < rt0; j += 32) seed_put(ix, t, gap, local, qlen, sqi[j], spl[j], w + j, valid, skey, sq);
+  } else {
+    int64_t wl = w + excl0;
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      const uint64_t pl = spl[lane * P + i];
+      if (pl != kNoPayload) {
+        seed_put(ix, t, gap, local, qlen, lane * P + i, pl, wl, valid, skey, sq);
+        wl += payload_count(pl);
+      }
+    }
+  }
+  __syncwarp();
+  w += rt0;
   for (int r0 = kSeedRound; r0 < nk; r0 += kSeedRound) {
     uint64_t pl[P];
-    round_lookup<SMALL>(q, ix, st, nk, r0, lane, any_n, pl);
-    round_emit(ix, t, gap, local, qlen, r0, lane, pl, w, valid, skey, sq, stage_pl[wib], stage_qi[wib]);
+    round_lookup<SMALL>(q, ix, st, nk, r0, lane, pl);
+    round_emit(ix, t, gap, local, qlen, r0, lane, pl, w, valid, skey, sq, spl, sqi);
   }
   valid = (int)__reduce_add_sync(kFull, (unsigned)valid);
   if (lane == 0) nvalid[s] = valid;
@@ -1470,9 +1711,11 @@ __device__ __forceinline__ void banded_hit(const int2* __restrict__ tab, const c
       const int nH = max(hA, hB);
       const int2 w = tab[bd.tc[c] | qc];  // (POINT + 7, match increment)
       const int pt = bd.A[c] + w.x;
-      bool h_wins, not_diag;
-      const int mx = __vibmax_s32(nH, nV, &h_wins);   // h_wins = nH >= nV
-      const int nS = __vibmax_s32(mx, pt, &not_diag);  // not_diag = mx >= pt
+      // (plain compares and maxima: fewer instructions than __vibmax_s32 here)
+      const bool h_wins = nH >= nV;
+      const int mx = max(nH, nV);
+      const bool not_diag = mx >= pt;
+      const int nS = max(mx, pt);
       const int side_m = h_wins ? hM : vM;
       const int nM = not_diag ? side_m : (bd.M[c] + w.y);
       const int nA = nS + kGapSO;
@@ -1730,10 +1973,14 @@ __global__ void k_gather_i64(const int64_t* __restrict__ src, const int64_t* __r
 // launch wrappers
 // ------------------------------------------------------------------------
 void scan_i32(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st, int level) {
-  scan_impl<int32_t>(ws, in, n, out, st, level);
+  (void)level;
+  scan_1pass(ws, ArrayLoad<int32_t>{in}, n, out, st);
 }
 void scan_i64(Workspace& ws, const int64_t* in, int64_t n, int64_t* out, cudaStream_t st, int level) {
-  scan_impl<int64_t>(ws, in, n, out, st, level);
+  scan_impl(ws, ArrayLoad<int64_t>{in}, n, out, st, level);
+}
+void scan_positive(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st) {
+  scan_1pass(ws, PositiveLoad{in}, n, out, st);
 }
 
 void pack_bases(const char* bases, int64_t n, uint64_t* packed, uint64_t* nmask, cudaStream_t st) {
@@ -1768,9 +2015,10 @@ void sample_keys(const uint64_t* packed, const uint64_t* nmask, int64_t n_sample
   CLAST_LAUNCHED();
 }
 
-void split_items(const uint64_t* items, int64_t n, int pbits, uint64_t* keys, int32_t* vals, cudaStream_t st) {
+void split_items(const uint64_t* items, int64_t n, int pbits, uint64_t bound, uint64_t* keys, int32_t* vals,
+                 int32_t* head, cudaStream_t st) {
   if (n <= 0) return;
-  k_split_items<<<blocks_for(n, 256), 256, 0, st>>>(items, n, pbits, keys, vals);
+  k_split_items<<<blocks_for(n, 256), 256, 0, st>>>(items, n, pbits, bound, keys, vals, head);
   CLAST_LAUNCHED();
 }
 
@@ -1793,7 +2041,7 @@ int radix_sort_u64(Workspace& ws, uint64_t* keys, int32_t* vals, uint64_t* keys_
   for (int shift = lo_bit; shift < hi_bit; shift += 8) {
     k_rs_hist<<<nblocks, kRsThreads, 0, st>>>(a, n, shift, hist, nblocks);
     CLAST_LAUNCHED();
-    scan_impl<uint32_t>(ws, hist, (int64_t)256 * nblocks, offs, st, 0);
+    scan_1pass(ws, ArrayLoad<uint32_t>{hist}, (int64_t)256 * nblocks, offs, st);
     if (pay) k_rs_scatter<true><<<nblocks, kRsThreads, smem, st>>>(a, va, b, vb, n, shift, offs, nblocks);
     else k_rs_scatter<false><<<nblocks, kRsThreads, smem, st>>>(a, nullptr, b, nullptr, n, shift, offs, nblocks);
     CLAST_LAUNCHED();
@@ -1809,9 +2057,9 @@ void count_below(const uint64_t* keys, int64_t n, uint64_t bound, int64_t* out, 
   CLAST_LAUNCHED();
 }
 
-void index_heads(const uint64_t* keys, int64_t n, const int64_t* nv_dev, int32_t* head, cudaStream_t st) {
+void index_heads(const uint64_t* keys, int64_t n, uint64_t bound, int32_t* head, cudaStream_t st) {
   if (n <= 0) return;
-  k_index_heads<<<blocks_for(n, 256), 256, 0, st>>>(keys, n, nv_dev, head);
+  k_index_heads<<<blocks_for(n, 256), 256, 0, st>>>(keys, n, bound, head);
   CLAST_LAUNCHED();
 }
 void index_unique(const uint64_t* keys, const int32_t* head, const int64_t* hpos, int64_t n, const int64_t* nv_dev,
@@ -1858,32 +2106,25 @@ void seed_fused(const QueryView& q, const IndexView& ix, const TargetView& t, in
   CLAST_LAUNCHED();
 }
 
-void maxscan_i64(Workspace& ws, const int64_t* in, int64_t n, int64_t* out, cudaStream_t st, int level) {
+template <class Load>
+void maxscan_impl(Workspace& ws, Load in, int64_t n, int64_t* out, cudaStream_t st, int level) {
   if (n <= 0) return;
   const int64_t tiles = (n + kScanTile - 1) / kScanTile;
   const std::string tag = "maxscan" + std::to_string(level);
   int64_t* tmax = ws.get<int64_t>(tag + "m", tiles);
-  k_maxscan_tiles<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, out, tmax);
+  k_maxscan_tiles<Load><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, out, tmax);
   CLAST_LAUNCHED();
   if (tiles > 1) {
     int64_t* trun = ws.get<int64_t>(tag + "r", tiles);
-    maxscan_i64(ws, tmax, tiles, trun, st, level + 1);
+    maxscan_impl(ws, ArrayLoad<int64_t>{tmax}, tiles, trun, st, level + 1);
     k_maxscan_apply<<<blocks_for(n, 256), 256, 0, st>>>(out, n, trun);
     CLAST_LAUNCHED();
   }
 }
 
-void table_kept(const int32_t* ucnt, int64_t n_unique, int32_t* kept, cudaStream_t st) {
-  if (n_unique <= 0) return;
-  k_table_kept<<<blocks_for(n_unique, 256), 256, 0, st>>>(ucnt, n_unique, kept);
-  CLAST_LAUNCHED();
-}
-
-void table_slack(const uint64_t* ucode, const int32_t* ucnt, const int64_t* rank, int64_t n_unique, int l,
-                 uint32_t nbuckets, int64_t* slack, cudaStream_t st) {
-  if (n_unique <= 0) return;
-  k_table_slack<<<blocks_for(n_unique, 256), 256, 0, st>>>(ucode, ucnt, rank, n_unique, l, nbuckets, slack);
-  CLAST_LAUNCHED();
+void table_runmax(Workspace& ws, const uint64_t* ucode, const int32_t* ucnt, const int64_t* rank, int64_t n_unique,
+                  int l, uint32_t nbuckets, int64_t* run_max, cudaStream_t st) {
+  maxscan_impl(ws, SlackLoad{ucode, ucnt, rank, l, nbuckets}, n_unique, run_max, st, 0);
 }
 
 void table_place(const uint64_t* ucode, const int32_t* ustart, const int32_t* ucnt, const int2* entries,

@@ -14,6 +14,8 @@ struct Workspace;  // device scratch pool (clast_engine.cu)
 // out[0..n] = exclusive prefix sums of in[0..n) (out[n] = total).
 void scan_i32(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st, int level = 0);
 void scan_i64(Workspace& ws, const int64_t* in, int64_t n, int64_t* out, cudaStream_t st, int level = 0);
+// exclusive scan of (in[i] > 0)
+void scan_positive(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st);
 
 // 2-bit codes (32 bases per word) and non-ACGT mask (64 per word) of bases[0..n);
 // positions >= n count as 'N'.  packed needs ceil(n/32)+2 words, nmask ceil(n/64)+2.
@@ -34,8 +36,10 @@ void build_window(const char* src, const int64_t* src_off, const int32_t* gatewa
 // items[j] = code, vals[j] = j.
 void sample_keys(const uint64_t* packed, const uint64_t* nmask, int64_t n_samples, int stride, int l, int pbits,
                  uint64_t* items, int32_t* vals, cudaStream_t st);
-// keys[i] = items[i] >> pbits, vals[i] = the low pbits bits.
-void split_items(const uint64_t* items, int64_t n, int pbits, uint64_t* keys, int32_t* vals, cudaStream_t st);
+// keys[i] = items[i] >> pbits, vals[i] = the low pbits bits, head[i] =
+// whether keys[i] < bound and differs from keys[i - 1].
+void split_items(const uint64_t* items, int64_t n, int pbits, uint64_t bound, uint64_t* keys, int32_t* vals,
+                 int32_t* head, cudaStream_t st);
 // Stable LSD radix sort of 64-bit words by bits [lo_bit, hi_bit), carrying
 // vals along unless vals is null.  Returns 0 when the result is in (keys,
 // vals), 1 when it is in (keys_alt, vals_alt).
@@ -44,8 +48,9 @@ int radix_sort_u64(Workspace& ws, uint64_t* keys, int32_t* vals, uint64_t* keys_
 // *out = number of keys < bound in the sorted array keys[0..n)
 void count_below(const uint64_t* keys, int64_t n, uint64_t bound, int64_t* out, cudaStream_t st);
 // Index build over n samples with the valid count *nv_dev and the unique
-// count *nu_dev on the device (no host synchronisation).
-void index_heads(const uint64_t* keys, int64_t n, const int64_t* nv_dev, int32_t* head, cudaStream_t st);
+// count *nu_dev on the device (no host synchronisation).  head[i] = whether
+// keys[i] < bound and differs from keys[i - 1].
+void index_heads(const uint64_t* keys, int64_t n, uint64_t bound, int32_t* head, cudaStream_t st);
 void index_unique(const uint64_t* keys, const int32_t* head, const int64_t* hpos, int64_t n, const int64_t* nv_dev,
                   uint64_t* ukeys, int64_t* ufirst, cudaStream_t st);
 void index_keep(const int32_t* vals, const int64_t* hpos, const int64_t* ufirst, int64_t n, const int64_t* nv_dev,
@@ -55,16 +60,14 @@ void index_entries(const int32_t* keep, const int64_t* kpos, const int2* resolve
                    int2* entries, cudaStream_t st);
 void index_buckets(const int64_t* ufirst, const int64_t* kpos, int64_t n, const int64_t* nu_dev, int32_t* ustart,
                    int32_t* ucnt, cudaStream_t st);
-// Hash table of the index without atomics (layout: IndexView).  kept[k] =
-// whether unique code k keeps entries; rank = exclusive scan of kept;
-// slack[rank] = home - rank of every kept code; run_max = running maximum of
-// slack; table_place writes every kept code's record at rank + run_max[rank]
-// and sets its filter bits (filter zeroed, table records set to ~0 by the
-// caller); *failed counts records that would fall outside the table (none).
-void table_kept(const int32_t* ucnt, int64_t n_unique, int32_t* kept, cudaStream_t st);
-void table_slack(const uint64_t* ucode, const int32_t* ucnt, const int64_t* rank, int64_t n_unique, int l,
-                 uint32_t nbuckets, int64_t* slack, cudaStream_t st);
-void maxscan_i64(Workspace& ws, const int64_t* in, int64_t n, int64_t* out, cudaStream_t st, int level = 0);
+// Hash table of the index without atomics (layout: IndexView).  rank =
+// exclusive scan of (ucnt > 0), the codes that keep entries; table_runmax:
+// run_max[k] = max over kept j <= k of home_j - rank_j; table_place writes
+// every kept code's record at rank[k] + run_max[k] and sets its filter bits
+// (filter zeroed, table records set to ~0 by the caller); *failed counts
+// records that would fall outside the table (none).
+void table_runmax(Workspace& ws, const uint64_t* ucode, const int32_t* ucnt, const int64_t* rank, int64_t n_unique,
+                  int l, uint32_t nbuckets, int64_t* run_max, cudaStream_t st);
 void table_place(const uint64_t* ucode, const int32_t* ustart, const int32_t* ucnt, const int2* entries,
                  const int64_t* rank, const int64_t* run_max, int64_t n_unique, ulonglong2* table, int64_t n_records,
                  uint32_t* filter, int fshift, unsigned long long* failed, cudaStream_t st);
