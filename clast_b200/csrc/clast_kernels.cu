@@ -953,14 +953,15 @@ __device__ __forceinline__ void round_emit(const IndexView& ix, const TargetView
   w += round_total;
 }
 
-constexpr int kSeedFusedThreads = 128;
+constexpr int kSeedFusedThreads = 64;  // two strands per block: blocks retire at a finer grain than with four
+constexpr int kSeedPrefetchBlocks = 2048;
 
 // The seed buffer is split into kSeedParts partitions of part_cap seeds, each
 // with its own cursor; strand s takes its range in partition s % kSeedParts, so
 // the range reservations of neighbouring warps hit different counters.
 // SMALL: l <= 16, keys read with 32-bit funnel shifts.
 template <bool SMALL>
-__global__ void __launch_bounds__(kSeedFusedThreads, SMALL ? 8 : 6) k_seed_fused(QueryView q, IndexView ix, TargetView t, int gap,
+__global__ void __launch_bounds__(kSeedFusedThreads, SMALL ? 16 : 12) k_seed_fused(QueryView q, IndexView ix, TargetView t, int gap,
                                                                    int local, unsigned long long* __restrict__ cursor,
                                                                    unsigned long long* __restrict__ n_kmers,
                                                                    int64_t* __restrict__ off, int32_t* __restrict__ cnt,
@@ -977,6 +978,21 @@ __global__ void __launch_bounds__(kSeedFusedThreads, SMALL ? 8 : 6) k_seed_fused
   const int64_t st = q.start[s];
   const int qlen = q.len[s];
   const int nk = qlen - ix.l + 1;
+  // L2 prefetch for the block kSeedPrefetchBlocks later: its strand table
+  // entries and, estimated from this strand's start and the mean strand
+  // length, its 2-bit words and N flags, so that its first loads hit L2.
+  // Every address stays inside its array.
+  if (wib == 0 && lane < 5) {
+    const int64_t sp = ((int64_t)blockIdx.x + kSeedPrefetchBlocks) * (kSeedFusedThreads / 32);
+    if (sp < q.nstrands && q.n > 0) {
+      const int64_t f = min(q.n - 1, st + (sp - s) * (q.n / q.nstrands));
+      const void* a = lane == 0 ? (const void*)(q.start + sp)
+                    : lane == 1 ? (const void*)(q.len + sp)
+                    : lane == 4 ? (const void*)(q.nmask + (f >> 6))
+                                : (const void*)(q.packed + min((f >> 5) + 16 * (lane - 2), q.n / 32 + 3));
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+    }
+  }
   uint64_t pl0[P];
   int valid_kmers = round_lookup<SMALL>(q, ix, st, nk, 0, lane, pl0);
   int lane_cnt = 0;
