@@ -43,7 +43,7 @@ from clast_b200 import api, synth  # noqa: E402
 METRIC = "query Mbp/s (bit-exact hits)"
 # DRAM bytes (read + write) per looked-up l-mer of k_seed_fused, from an ncu
 # capture on the half-size medium workload (profiles/k_seed_fused_medium_half.md)
-SEED_DRAM_BYTES_PER_KMER = 12.1
+SEED_DRAM_BYTES_PER_KMER = 12.2
 T_RAM, Q_RAM, T_VRAM, Q_VRAM = 64e6, 64e6, 64e6, 2e6  # common.hpp:12-15, x 1e6 (CHostSetting.cu:133-136)
 
 
