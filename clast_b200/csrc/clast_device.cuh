@@ -88,22 +88,6 @@ __device__ __forceinline__ uint64_t kmer_key(const uint64_t* packed, int64_t f, 
   return b >> (64 - 2 * l);
 }
 
-// The same for l <= 16 from the 32-bit halves of the words: a 64-bit word
-// keeps its first base in its top bits, so the 16-base unit j of the packed
-// array (and the 32-base unit j of the N mask) is 32-bit element j ^ 1.
-__device__ __forceinline__ uint32_t kmer_key16(const uint32_t* packed32, int64_t f, int l) {
-  const int64_t j = f >> 4;
-  const uint32_t hi = __ldcs(packed32 + (j ^ 1));
-  const uint32_t lo = __ldcs(packed32 + ((j + 1) ^ 1));
-  return __funnelshift_l(lo, hi, 2 * (int)(f & 15)) >> (32 - 2 * l);
-}
-__device__ __forceinline__ bool kmer_has_n16(const uint32_t* nmask32, int64_t f, int l) {
-  const int64_t j = f >> 5;
-  const uint32_t hi = __ldcs(nmask32 + (j ^ 1));
-  const uint32_t lo = __ldcs(nmask32 + ((j + 1) ^ 1));
-  return (__funnelshift_l(lo, hi, (int)(f & 31)) >> (32 - l)) != 0;
-}
-
 __device__ __forceinline__ bool kmer_at(const uint64_t* packed, const uint64_t* nmask, int64_t f,
                                         int l, uint64_t& key) {
   if (kmer_has_n(nmask, f, l)) return false;
@@ -143,10 +127,6 @@ __host__ __device__ __forceinline__ uint32_t filter_mask(uint64_t h) {
   const uint32_t v = (uint32_t)(h >> 16);
   return (1u << (v & 31)) | (1u << ((v >> 5) & 31)) | (1u << ((v >> 10) & 31));
 }
-__device__ __forceinline__ bool filter_pass(uint32_t word, uint64_t h) {
-  const uint32_t m = filter_mask(h);
-  return (word & m) == m;
-}
 // Entries of a payload (0 for none).
 __host__ __device__ __forceinline__ int payload_count(uint64_t p) {
   return p == kNoPayload ? 0 : ((p & kMulti) ? (int)(uint32_t)p : 1);
@@ -162,15 +142,6 @@ __device__ __forceinline__ uint64_t table_probe(const IndexView& ix, uint64_t c,
     if (rec.x == c || rec.y == kNoPayload) return rec.y;
   }
   return kNoPayload;
-}
-
-// Payload of key, or kNoPayload (krnlBinarySearch.cu:3-33 followed by the
-// bucket lookup of writeSeedList).
-__device__ __forceinline__ uint64_t index_find(const IndexView& ix, uint64_t key) {
-  const uint64_t c = order_code(key, ix.l);
-  const uint64_t h = key_hash(c);
-  if (!filter_pass(__ldg(ix.filter + filter_word(h, ix.fshift)), h)) return kNoPayload;
-  return table_probe(ix, c, record_home(c, ix.l, ix.nbuckets));
 }
 
 }  // namespace clast

@@ -55,51 +55,6 @@ struct PositiveLoad {  // 1 where p[i] > 0
   __device__ __forceinline__ int64_t operator()(int64_t i) const { return p[i] > 0 ? 1 : 0; }
 };
 
-template <class Load>
-__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(Load in, int64_t n_in, int64_t n_out,
-                                                             int64_t* __restrict__ out,
-                                                             int64_t* __restrict__ tile_sums) {
-  __shared__ int64_t warp_tot[kScanThreads / 32];
-  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
-  int64_t v[kScanItems];
-  int64_t s = 0;
-#pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
-    const int64_t idx = base + i;
-    v[i] = (idx < n_in) ? in(idx) : 0;
-    s += v[i];
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int64_t incl = s;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int64_t y = __shfl_up_sync(kFull, incl, o);
-    if (lane >= o) incl += y;
-  }
-  if (lane == 31) warp_tot[warp] = incl;
-  __syncthreads();
-  int64_t wpre = 0, tot = 0;
-#pragma unroll
-  for (int w = 0; w < kScanThreads / 32; ++w) {
-    const int64_t t = warp_tot[w];
-    if (w < warp) wpre += t;
-    tot += t;
-  }
-  int64_t run = wpre + incl - s;
-#pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
-    const int64_t idx = base + i;
-    if (idx < n_out) out[idx] = run;
-    run += v[i];
-  }
-  if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
-}
-
-__global__ void k_scan_add(int64_t* __restrict__ out, int64_t n_out, const int64_t* __restrict__ tile_pre) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n_out) out[i] += tile_pre[i / kScanTile];
-}
-
 // ---- single-pass exclusive scan (decoupled look-back) ----
 // Tiles take their index from a counter in launch order, so a tile only waits
 // for tiles that have already started.  Each tile publishes its aggregate,
@@ -226,21 +181,6 @@ void scan_1pass(Workspace& ws, Load in, int64_t n, int64_t* out, cudaStream_t st
   CLAST_LAUNCHED();
 }
 
-template <class Load>
-void scan_impl(Workspace& ws, Load in, int64_t n, int64_t* out, cudaStream_t st, int level) {
-  const int64_t n_out = n + 1;
-  const int64_t tiles = (n_out + kScanTile - 1) / kScanTile;
-  const std::string tag = "scan" + std::to_string(level);
-  int64_t* sums = ws.get<int64_t>(tag + "s", tiles);
-  k_scan_tiles<Load><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, n_out, out, sums);
-  CLAST_LAUNCHED();
-  if (tiles > 1) {
-    int64_t* pre = ws.get<int64_t>(tag + "p", tiles + 1);
-    scan_impl(ws, ArrayLoad<int64_t>{sums}, tiles, pre, st, level + 1);
-    k_scan_add<<<blocks_for(n_out, 256), 256, 0, st>>>(out, n_out, pre);
-    CLAST_LAUNCHED();
-  }
-}
 
 // ------------------------------------------------------------------------
 // packing and query strands
@@ -776,8 +716,6 @@ constexpr int kSeedPerLane = 5;
 constexpr int kSeedRound = 32 * kSeedPerLane;
 constexpr int kSeedParts = 32;
 
-// Payloads of the l-mers qi = r0 + lane * P + i (i < P) of a strand; invalid or
-// absent ones get kNoPayload.  Returns the number of valid l-mers.
 // Both records of a home bucket: one 256-bit streaming load (sm_100), the
 // address 32-byte aligned (home records are even, the table 256-byte aligned).
 __device__ __forceinline__ void ld_bucket(const ulonglong2* a, uint64_t& c0, uint64_t& p0, uint64_t& c1,
@@ -790,6 +728,9 @@ __device__ __forceinline__ uint64_t funnel64(uint64_t hi, uint64_t lo, int s) {
   return (hi << s) | ((lo >> 1) >> (63 - s));
 }
 
+// Payloads of the l-mers qi = r0 + lane * P + i (i < P) of a strand; invalid or
+// absent ones get kNoPayload (the key search of krnlBinarySearch.cu:3-33 and
+// the bucket read of writeSeedList).  Returns the number of valid l-mers.
 template <bool SMALL>
 __device__ __forceinline__ int round_lookup(const QueryView& q, const IndexView& ix, int64_t st, int nk, int r0,
                                             int lane, uint64_t (&pl)[kSeedPerLane]) {
@@ -1988,12 +1929,8 @@ __global__ void k_gather_i64(const int64_t* __restrict__ src, const int64_t* __r
 // ------------------------------------------------------------------------
 // launch wrappers
 // ------------------------------------------------------------------------
-void scan_i32(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st, int level) {
-  (void)level;
+void scan_i32(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st) {
   scan_1pass(ws, ArrayLoad<int32_t>{in}, n, out, st);
-}
-void scan_i64(Workspace& ws, const int64_t* in, int64_t n, int64_t* out, cudaStream_t st, int level) {
-  scan_impl(ws, ArrayLoad<int64_t>{in}, n, out, st, level);
 }
 void scan_positive(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st) {
   scan_1pass(ws, PositiveLoad{in}, n, out, st);

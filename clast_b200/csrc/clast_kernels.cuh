@@ -12,8 +12,7 @@ namespace clast {
 struct Workspace;  // device scratch pool (clast_engine.cu)
 
 // out[0..n] = exclusive prefix sums of in[0..n) (out[n] = total).
-void scan_i32(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st, int level = 0);
-void scan_i64(Workspace& ws, const int64_t* in, int64_t n, int64_t* out, cudaStream_t st, int level = 0);
+void scan_i32(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st);
 // exclusive scan of (in[i] > 0)
 void scan_positive(Workspace& ws, const int32_t* in, int64_t n, int64_t* out, cudaStream_t st);
 
