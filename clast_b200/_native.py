@@ -38,6 +38,25 @@ class clast_map_result(C.Structure):
                [("evalue", C.POINTER(C.c_double)), ("owner", C.c_void_p)]
 
 
+class clast_labels(C.Structure):
+    _fields_ = [("n", C.c_int64), ("chars", C.c_void_p), ("offsets", C.POINTER(C.c_int64))]
+
+
+class clast_tsv(C.Structure):
+    _fields_ = [("n_bytes", C.c_int64), ("text", C.c_void_p), ("load_offsets", C.POINTER(C.c_int64)),
+                ("owner", C.c_void_p)]
+
+
+class clast_server_config(C.Structure):
+    _fields_ = [("lanes", C.c_int32), ("q_vram", C.c_int32), ("q_ram", C.c_int32), ("reserved0", C.c_int32),
+                ("max_batch_bases", C.c_int64), ("hbm_budget", C.c_int64), ("hbm_reserve", C.c_int64)]
+
+
+class clast_server_stats(C.Structure):
+    _fields_ = [(f, C.c_int64) for f in ("batches", "requests", "bases", "max_batch_requests", "queued", "running",
+                                         "hbm_budget", "hbm_in_flight_max")]
+
+
 class clast_stats(C.Structure):
     _fields_ = [("index_ms", C.c_double), ("index_upload_ms", C.c_double), ("map_ms", C.c_double),
                 ("map_upload_ms", C.c_double), ("index_launches", C.c_int64), ("map_launches", C.c_int64),
@@ -45,7 +64,8 @@ class clast_stats(C.Structure):
                 ("results", C.c_int64), ("dp_cells", C.c_int64), ("seed_ms", C.c_double),
                 ("seed_launches", C.c_int64), ("dp_ms", C.c_double), ("dp_launches", C.c_int64),
                 ("sort_ms", C.c_double), ("final_ms", C.c_double), ("index_wall_ms", C.c_double),
-                ("map_wall_ms", C.c_double), ("map_prep_ms", C.c_double), ("map_call_ms", C.c_double)]
+                ("map_wall_ms", C.c_double), ("map_prep_ms", C.c_double), ("map_call_ms", C.c_double),
+                ("index_bases", C.c_int64), ("index_keys", C.c_int64)]
 
 
 # symbol name -> (restype, argtypes); the full export list of include/clast_gpu.h
@@ -68,12 +88,28 @@ SIGNATURES = {
     "clast_targets_free": (None, [C.c_void_p]),
     "clast_targets_save": (C.c_int, [C.c_void_p, C.c_void_p, C.c_char_p]),
     "clast_targets_load": (C.c_int, [C.c_void_p, C.POINTER(clast_params), C.c_char_p, C.POINTER(C.c_void_p)]),
+    "clast_targets_verify": (C.c_int, [C.POINTER(clast_params), C.c_char_p, C.c_char_p, C.c_int]),
     "clast_map": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(clast_params), C.c_int32, C.POINTER(clast_seqs),
                             C.c_int32, C.c_void_p, C.POINTER(clast_map_result)]),
     "clast_map_result_free": (None, [C.POINTER(clast_map_result)]),
+    "clast_format_tsv": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(clast_map_result), C.c_int32,
+                                   C.POINTER(clast_labels), C.POINTER(clast_labels), C.c_void_p, C.c_int32,
+                                   C.POINTER(clast_tsv)]),
+    "clast_tsv_free": (None, [C.POINTER(clast_tsv)]),
     "clast_last_map_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "clast_get_stats": (C.c_int, [C.c_void_p, C.POINTER(clast_stats)]),
     "clast_int32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "clast_server_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(clast_params),
+                                      C.POINTER(clast_server_config), C.POINTER(C.c_void_p)]),
+    "clast_server_submit": (C.c_int, [C.c_void_p, C.POINTER(clast_seqs), C.POINTER(C.c_int64)]),
+    "clast_server_poll": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(clast_map_result)]),
+    "clast_server_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
+    "clast_server_release": (C.c_int, [C.c_void_p, C.c_int64]),
+    "clast_server_times": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                     C.POINTER(C.c_int64)]),
+    "clast_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(clast_server_stats)]),
+    "clast_server_last_error": (C.c_char_p, [C.c_void_p]),
+    "clast_server_destroy": (None, [C.c_void_p]),
     "clast_cli_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), C.c_char_p, C.c_int]),
 }
 

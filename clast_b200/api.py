@@ -90,6 +90,44 @@ def _comp(seq: bytes) -> bytes:
     return bytes(c if c in b"ACGT" else ord("N") for c in out) if any(c not in b"ACGT" for c in out) else out
 
 
+_COMP_TABLE = np.full(256, ord("N"), dtype=np.uint8)
+for _a, _b in zip(b"ACGT", b"TGCA"):
+    _COMP_TABLE[_a] = _b
+
+
+def joint_layout(bases, offsets, lmer: int, first: int, end: int, both_strands: bool):
+    """The base array CHostSeqList::getBaseArray builds for records
+    [first, end) of a one-strand set (utilAddSequence.cu:6-47): every
+    sequence followed by its first l-1 bases ('N' past its end); with
+    ``both_strands`` every record gives its '+' strand then its reverse
+    complement (non-ACGT -> N, utilReverseSeq.cpp:3-19), as
+    CHostSeqList_query::add does.  Returns (uint8 bases, int64 window-relative
+    gateway, int32 lengths), vectorised."""
+    offsets = np.asarray(offsets, dtype=np.int64)
+    lens = np.diff(offsets[first:end + 1])
+    k = 2 if both_strands else 1
+    L = np.repeat(lens, k)
+    src0 = np.repeat(offsets[first:end], k)
+    rev = np.tile(np.array([False, True]), len(lens)) if both_strands else np.zeros(len(L), bool)
+    per = L + lmer - 1
+    gw = np.zeros(len(per), dtype=np.int64)
+    if len(per) > 1:
+        np.cumsum(per[:-1], out=gw[1:])
+    total = int(per.sum()) if len(per) else 0
+    sid = np.repeat(np.arange(len(per)), per)
+    pos = np.arange(total, dtype=np.int64) - gw[sid]
+    Ls = L[sid]
+    kk = np.where(pos < Ls, pos, pos - Ls)           # index within the sequence (joint: its first bases)
+    ok = kk < Ls
+    r = rev[sid]
+    src = src0[sid] + np.where(r, Ls - 1 - kk, kk)
+    src = np.where(ok, src, 0)
+    b = np.asarray(bases)[src] if total else np.zeros(0, np.uint8)
+    b = np.where(r, _COMP_TABLE[b], b)
+    out = np.where(ok, b, np.uint8(ord("N"))).astype(np.uint8)
+    return out, gw, L.astype(np.int32)
+
+
 class SeqList:
     """CHostSeqList: concatenated sequences, each followed by its first l-1
     bases (the joint, utilAddSequence.cu:6-47), with gateway prefix sums."""
@@ -143,6 +181,14 @@ class SeqList:
         return bases, gw, ln
 
 
+def _ptr(b):
+    """Pointer argument for bytes or a contiguous numpy array (no copy)."""
+    if isinstance(b, np.ndarray):
+        assert b.flags.c_contiguous
+        return b.ctypes.data
+    return b
+
+
 def _hits_to_numpy(h: N.clast_hits) -> dict:
     n = int(h.n)
     out = {}
@@ -167,11 +213,28 @@ class _MapResultOwner:
         self.r = None
 
 
+class MapResult(dict):
+    """Fields of a clast_map result (numpy views of the library's pinned
+    arrays); ``owner`` keeps the library result alive."""
+    owner = None
+
+
+def flat_labels(labels):
+    """(chars, offsets) of a list of str / bytes labels (clast_labels)."""
+    enc = [x.encode() if isinstance(x, str) else bytes(x) for x in labels]
+    offsets = np.zeros(len(enc) + 1, dtype=np.int64)
+    if enc:
+        np.cumsum([len(x) for x in enc], out=offsets[1:])
+    return b"".join(enc), offsets
+
+
 def _map_result_arrays(engine, r, n_loads) -> dict:
     """Zero-copy numpy views of a clast_map result."""
     owner = _MapResultOwner(engine, r)
     n = int(r.n)
-    out = {}
+    out = MapResult()
+    out.owner = owner
+    out.n_loads = n_loads
     for f in MAP_FIELDS:
         ct = C.c_double if f == "evalue" else C.c_int32
         buf = (ct * max(n, 1)).from_address(C.cast(getattr(r, f), C.c_void_p).value)
@@ -238,12 +301,13 @@ class Engine:
             raise ClastError(rc, self._lib.clast_last_error(self.ctx).decode(errors="replace"))
 
     # -- the reference seam ------------------------------------------------
-    def hash_table_window(self, s: Setting, bases: bytes, gateway, lengths, t_begin: int) -> HashTable:
+    def hash_table_window(self, s: Setting, bases, gateway, lengths, t_begin: int) -> HashTable:
+        """``bases``: bytes or a contiguous uint8 numpy array (no copy)."""
         gw = np.ascontiguousarray(gateway, dtype=np.int32)
         ln = np.ascontiguousarray(lengths, dtype=np.int32)
         out = C.c_void_p()
         p = s.c()
-        self._check(self._lib.clast_index_build(self.ctx, C.byref(p), bases, len(bases), gw.ctypes.data,
+        self._check(self._lib.clast_index_build(self.ctx, C.byref(p), _ptr(bases), len(bases), gw.ctypes.data,
                                                 ln.ctypes.data, len(gw), t_begin, C.byref(out)))
         return HashTable(self, out.value, t_begin)
 
@@ -258,7 +322,7 @@ class Engine:
         ln = np.ascontiguousarray(q_lengths, dtype=np.int32)
         h = N.clast_hits()
         p = s.c()
-        self._check(self._lib.clast_search(self.ctx, ix.handle, C.byref(p), q_bases, len(q_bases),
+        self._check(self._lib.clast_search(self.ctx, ix.handle, C.byref(p), _ptr(q_bases), len(q_bases),
                                            gw.ctypes.data, ln.ctypes.data, len(gw), q_begin, C.byref(h)))
         try:
             return _hits_to_numpy(h)
@@ -354,6 +418,39 @@ class Engine:
         self.last_map_py_ms = ((t1 - t0) * 1e3, (t2 - t1) * 1e3, (time.perf_counter() - t2) * 1e3)
         return out
 
+    def format_tsv(self, targets: Targets, result: dict, read_labels, target_labels, start_idx=None,
+                   num_out: int = -1, out=None):
+        """clast_format_tsv: the reference's 10-column text of a map result
+        (every query load in order).  ``read_labels`` / ``target_labels``:
+        every read / target record given to map() / targets(), or their
+        flat_labels() (chars, offsets).  Returns the text as bytes, or, with
+        ``out`` (a binary file), writes it there straight from the library's
+        buffer and returns its length.  The byte offset of every load's text
+        is left in ``last_tsv_load_offsets``."""
+        rl = read_labels if isinstance(read_labels, tuple) else flat_labels(read_labels)
+        tl = target_labels if isinstance(target_labels, tuple) else flat_labels(target_labels)
+        roff = np.ascontiguousarray(rl[1], dtype=np.int64)
+        toff = np.ascontiguousarray(tl[1], dtype=np.int64)
+        rlab = N.clast_labels(len(roff) - 1, C.cast(C.c_char_p(rl[0]), C.c_void_p),
+                              roff.ctypes.data_as(C.POINTER(C.c_int64)))
+        tlab = N.clast_labels(len(toff) - 1, C.cast(C.c_char_p(tl[0]), C.c_void_p),
+                              toff.ctypes.data_as(C.POINTER(C.c_int64)))
+        si = None if start_idx is None else np.ascontiguousarray(start_idx, dtype=np.int32)
+        t = N.clast_tsv()
+        self._check(self._lib.clast_format_tsv(self.ctx, targets.handle, C.byref(result.owner.r), result.n_loads,
+                                               C.byref(rlab), C.byref(tlab), None if si is None else si.ctypes.data,
+                                               int(num_out), C.byref(t)))
+        try:
+            n = int(t.n_bytes)
+            self.last_tsv_load_offsets = np.ctypeslib.as_array(t.load_offsets, shape=(result.n_loads + 1,)).copy()
+            if out is None:
+                return C.string_at(t.text, n) if n else b""
+            if n:
+                out.write(memoryview((C.c_char * n).from_address(t.text)))
+            return n
+        finally:
+            self._lib.clast_tsv_free(C.byref(t))
+
     def stats(self) -> dict:
         """clast_get_stats: CUDA-event timings and counts of the last
         targets()/map() calls."""
@@ -372,6 +469,95 @@ class Engine:
         k = C.c_int64()
         self._check(self._lib.clast_last_map_stats(self.ctx, C.byref(ms), C.byref(k)))
         return ms.value, k.value
+
+
+PENDING = 1
+ERR_CANCELLED = -5
+
+
+class Server:
+    """The served form (clast_server_*): resident targets, requests batched
+    as they arrive, ``lanes`` batches on the GPU at once.  Results are dicts
+    of MAP_FIELDS (read = record index within the request) plus
+    ``load_offsets``, copied out of the library."""
+
+    def __init__(self, engine: "Engine", targets: Targets, s: Setting, lanes: int = 2, q_vram: int = 2_000_000,
+                 q_ram: int = 32_000_000, max_batch_bases: int = 8_000_000, hbm_budget: int = 0,
+                 hbm_reserve: int = 0):
+        self._lib = N.load()
+        self.engine, self.targets = engine, targets
+        self.q_ram = q_ram
+        self._nloads = {}
+        cfg = N.clast_server_config(lanes, q_vram, q_ram, 0, max_batch_bases, hbm_budget, hbm_reserve)
+        p = s.c()
+        h = C.c_void_p()
+        engine._check(self._lib.clast_server_create(engine.ctx, targets.handle, C.byref(p), C.byref(cfg),
+                                                    C.byref(h)))
+        self.handle = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise ClastError(rc, self._lib.clast_server_last_error(self.handle).decode(errors="replace"))
+
+    def submit(self, bases, offsets) -> int:
+        o = np.ascontiguousarray(offsets, dtype=np.int64)
+        b = np.ascontiguousarray(bases, dtype=np.uint8)
+        seqs = N.clast_seqs(len(o) - 1, b.ctypes.data, o.ctypes.data_as(C.POINTER(C.c_int64)), 0)
+        rid = C.c_int64()
+        self._check(self._lib.clast_server_submit(self.handle, C.byref(seqs), C.byref(rid)))
+        # the request's RAM loads (the same rule the server applies)
+        self._nloads[rid.value] = len(ram_loads(np.diff(o), self.q_ram)[1])
+        return rid.value
+
+    def poll(self, rid: int, timeout_ms: int = -1):
+        """The request's hits when done, None while it is pending; raises
+        ClastError when it failed or was cancelled."""
+        r = N.clast_map_result()
+        rc = self._lib.clast_server_poll(self.handle, int(rid), int(timeout_ms), C.byref(r))
+        if rc == PENDING:
+            return None
+        self._check(rc)
+        n = int(r.n)
+        out = {}
+        for f in MAP_FIELDS:
+            dt = np.float64 if f == "evalue" else np.int32
+            out[f] = np.ctypeslib.as_array(getattr(r, f), shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+        nl = self._nloads.get(int(rid), 0)
+        out["load_offsets"] = np.ctypeslib.as_array(r.load_offsets, shape=(nl + 1,)).copy()
+        return out
+
+    def cancel(self, rid: int) -> None:
+        self._check(self._lib.clast_server_cancel(self.handle, int(rid)))
+
+    def release(self, rid: int) -> None:
+        self._check(self._lib.clast_server_release(self.handle, int(rid)))
+        self._nloads.pop(int(rid), None)
+
+    def times(self, rid: int):
+        """(queued, started, finished) steady-clock ns (time.monotonic_ns)."""
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        self._check(self._lib.clast_server_times(self.handle, int(rid), C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def stats(self) -> dict:
+        st = N.clast_server_stats()
+        self._check(self._lib.clast_server_get_stats(self.handle, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in N.clast_server_stats._fields_}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.clast_server_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+
+def verify_targets_file(s: Setting, path: str):
+    """clast_targets_verify: (ok, reason) for an index file, on the host."""
+    err = C.create_string_buffer(512)
+    p = s.c()
+    rc = N.load().clast_targets_verify(C.byref(p), os.fsencode(path), err, len(err))
+    return rc == 0, err.value.decode(errors="replace")
 
 
 def run_clast(argv) -> tuple:

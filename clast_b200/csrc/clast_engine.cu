@@ -26,146 +26,19 @@
 #include "clast_device.cuh"
 #include "clast_kernels.cuh"
 #include "clast_workspace.h"
+#include "clast_engine.h"
 
 using namespace clast;
 
-// CUDA-event timing of device stages on one stream: begin()/end() bracket
-// launches, flush() (after a stream synchronisation) adds up the intervals.
-struct StageTimer {
-  enum Stage { SEED = 0, DP = 1, SORT = 2, FINAL = 3, N_STAGES = 4 };
-  std::vector<cudaEvent_t> pool;
-  struct Pending { int stage; cudaEvent_t a, b; };
-  std::vector<Pending> pending;
-  double ms[N_STAGES] = {0, 0, 0, 0};
-  int64_t n[N_STAGES] = {0, 0, 0, 0};
-  cudaEvent_t cur_a = nullptr;
+namespace clast {
+thread_local cudaStream_t g_alloc_stream = nullptr;
+}  // namespace clast
 
-  cudaEvent_t take() {
-    if (pool.empty()) {
-      cudaEvent_t e;
-      CLAST_CK(cudaEventCreate(&e));
-      return e;
-    }
-    cudaEvent_t e = pool.back();
-    pool.pop_back();
-    return e;
-  }
-  void begin(cudaStream_t st) {
-    cur_a = take();
-    CLAST_CK(cudaEventRecord(cur_a, st));
-  }
-  void end(int stage, cudaStream_t st, int launches = 1) {
-    cudaEvent_t b = take();
-    CLAST_CK(cudaEventRecord(b, st));
-    pending.push_back({stage, cur_a, b});
-    n[stage] += launches;
-  }
-  void flush() {
-    for (auto& p : pending) {
-      float t = 0;
-      CLAST_CK(cudaEventElapsedTime(&t, p.a, p.b));
-      ms[p.stage] += t;
-      pool.push_back(p.a);
-      pool.push_back(p.b);
-    }
-    pending.clear();
-  }
-  void reset() {
-    flush();
-    for (int i = 0; i < N_STAGES; ++i) { ms[i] = 0; n[i] = 0; }
-  }
-  ~StageTimer() {
-    for (auto e : pool) cudaEventDestroy(e);
-    for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
-  }
-};
 
-// Pinned host buffer that holds one clast_map result; reused once released.
-struct PinnedArena {
-  void* p = nullptr;
-  size_t bytes = 0;
-  bool in_use = false;
-};
 
-struct clast_ctx {
-  std::vector<std::unique_ptr<PinnedArena>> arenas;
-  int device = 0;
-  cudaStream_t st = nullptr;
-  cudaStream_t st_copy = nullptr;  // query uploads, overlapping index builds still running on st
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
-  Workspace ws;
-  std::string err;
-  double last_ms = 0;
-  int64_t last_launches = 0;
-  clast_stats stats{};
-  StageTimer timer;
-  int64_t seed_hint = 0;  // seed buffer capacity that sufficed before
-};
+
 
 namespace {
-
-double wall_ms() {
-  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
-}
-
-// Stream used for the stream-ordered allocations of the current API call.
-thread_local cudaStream_t g_alloc_stream = nullptr;
-
-// Owning device allocation from the device's stream-ordered memory pool
-// (cudaMallocAsync / cudaFreeAsync on the owning context's stream), so
-// steady-state calls reuse pool memory instead of calling cudaMalloc.
-template <class T>
-struct DevArray {
-  T* p = nullptr;
-  size_t n = 0;
-  cudaStream_t st = nullptr;
-  DevArray() = default;
-  DevArray(const DevArray&) = delete;
-  DevArray& operator=(const DevArray&) = delete;
-  DevArray(DevArray&& o) noexcept : p(o.p), n(o.n), st(o.st) { o.p = nullptr; o.n = 0; }
-  DevArray& operator=(DevArray&& o) noexcept {
-    if (this != &o) {
-      release();
-      p = o.p;
-      n = o.n;
-      st = o.st;
-      o.p = nullptr;
-      o.n = 0;
-    }
-    return *this;
-  }
-  void alloc(size_t count) {
-    release();
-    n = count;
-    st = g_alloc_stream;
-    if (cudaMallocAsync(reinterpret_cast<void**>(&p), (count ? count : 1) * sizeof(T), st) != cudaSuccess) {
-      (void)cudaGetLastError();
-      p = nullptr;
-      n = 0;
-      throw std::bad_alloc();
-    }
-  }
-  void release() {
-    if (p) cudaFreeAsync(p, st);
-    p = nullptr;
-    n = 0;
-  }
-  ~DevArray() { release(); }
-};
-
-void check_params(const clast_params* p) {
-  if (!p) throw std::invalid_argument("params is null");
-  if (p->lmer < 1 || p->lmer > 31) throw std::invalid_argument("lmer must be in 1..31");
-  if (p->stride < 1) throw std::invalid_argument("stride must be >= 1");
-  if (p->gap < 2 || p->gap > 16) throw std::invalid_argument("gap must be in 2..16");
-}
-
-// Device copy of a base array with kPad 'N' bytes on both sides.
-void upload_padded(const char* host, int64_t n, DevArray<char>& dev, cudaStream_t st) {
-  dev.alloc((size_t)n + 2 * kPad);
-  CLAST_CK(cudaMemsetAsync(dev.p, 'N', (size_t)n + 2 * kPad, st));
-  if (n > 0) CLAST_CK(cudaMemcpyAsync(dev.p + kPad, host, (size_t)n, cudaMemcpyHostToDevice, st));
-}
 
 template <class T>
 T read_scalar(const T* dev, cudaStream_t st) {
@@ -177,43 +50,6 @@ T read_scalar(const T* dev, cudaStream_t st) {
 
 }  // namespace
 
-struct clast_index {
-  int l = 0, stride = 0, cut = 0;
-  int32_t t_begin = 0;
-  int64_t n = 0;
-  int32_t nseqs = 0;
-  DevArray<char> bases;  // padded
-  DevArray<int32_t> gateway, lengths;
-  DevArray<uint32_t> filter;     // blocked Bloom filter, 2^(64 - fshift) words
-  DevArray<ulonglong2> table;    // 2 * nbuckets records {key, payload}
-  DevArray<int2> entries;
-  int64_t n_unique = 0, n_keys = 0, n_entries = 0;
-  uint32_t nbuckets = 1;
-  int64_t n_records = 2;
-  int fshift = 63;
-
-  IndexView view() const {
-    IndexView v;
-    v.l = l;
-    v.fshift = fshift;
-    v.filter = filter.p;
-    v.table = table.p;
-    v.nbuckets = nbuckets;
-    v.n_records = n_records;
-    v.entries = entries.p;
-    v.n_keys = n_keys;
-    return v;
-  }
-  TargetView tview() const {
-    TargetView t;
-    t.bases = bases.p + kPad;
-    t.n = n;
-    t.gateway = gateway.p;
-    t.lengths = lengths.p;
-    t.nseqs = nseqs;
-    return t;
-  }
-};
 
 namespace {
 
@@ -288,6 +124,8 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix, un
   ix->nbuckets = (uint32_t)nb;
   int64_t* rank = ws.get<int64_t>("ix_rank", ns + 1);
   scan_positive(ws, ucnt, ns, rank, st);
+  ix->kept.alloc(1);
+  CLAST_CK(cudaMemcpyAsync(ix->kept.p, rank + ns, sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
   int64_t* run_max = ws.get<int64_t>("ix_runmax", ns);
   table_runmax(ws, ukeys, ucnt, rank, ns, l, ix->nbuckets, run_max, st);
   ix->n_records = 2 * nb + (1 << 16);
@@ -542,55 +380,14 @@ T* host_copy(const std::vector<T>& v) {
   return p;
 }
 
-int fail(clast_ctx* c, int code, const std::string& msg) {
-  if (c) c->err = msg;
-  return code;
-}
-
-// Runs f() and turns every exception into a status code plus message.
-template <class F>
-int guarded(clast_ctx* ctx, F&& f) {
-  try {
-    return f();
-  } catch (const CudaError& e) {
-    return fail(ctx, CLAST_ERR_CUDA, e.what());
-  } catch (const std::bad_alloc&) {
-    return fail(ctx, CLAST_ERR_NOMEM, "out of memory");
-  } catch (const std::invalid_argument& e) {
-    return fail(ctx, CLAST_ERR_ARG, e.what());
-  } catch (const std::exception& e) {
-    return fail(ctx, CLAST_ERR_INTERNAL, e.what());
-  }
-}
 
 }  // namespace
 
 // ----------------------------------------------------------------------------
 // targets / map: whole job with resident indexes
 // ----------------------------------------------------------------------------
-struct clast_targets {
-  clast_ctx* ctx = nullptr;
-  struct Win {
-    int32_t load, first;  // target load, first record within the load
-    std::unique_ptr<clast_index> ix;
-  };
-  std::vector<Win> wins;
-  int32_t n_loads = 0;
-  // The index builds run on the context's stream after clast_targets_create
-  // returns; the first clast_map waits for them, reads the overflow count and
-  // the build time (events) and reports either.
-  DevArray<unsigned long long> failed;
-  cudaEvent_t ev_start = nullptr, ev_up = nullptr, ev_done = nullptr;  // from the context's event pool
-  mutable bool settled = false;
-  int64_t launches = 0;
-  ~clast_targets() {
-    if (ev_done) cudaEventSynchronize(ev_done);
-    for (cudaEvent_t e : {ev_start, ev_up, ev_done})
-      if (e) ctx->timer.pool.push_back(e);
-  }
-};
 
-namespace {
+namespace clast {
 
 // Waits for the index builds of clast_targets_create (once), records their
 // time in the context's stats and reports a table overflow.
@@ -606,7 +403,16 @@ void settle_targets(clast_ctx* ctx, const clast_targets* T) {
   ctx->stats.index_launches = T->launches;
   if (read_scalar(reinterpret_cast<const int64_t*>(T->failed.p), ctx->st) != 0)
     throw std::runtime_error("index table overflow");
+  ctx->stats.index_bases = ctx->stats.index_keys = 0;
+  for (const auto& w : T->wins) {
+    ctx->stats.index_bases += w.ix->n;
+    if (w.ix->kept.p) ctx->stats.index_keys += read_scalar(w.ix->kept.p, ctx->st);
+  }
 }
+
+}  // namespace clast
+
+namespace {
 
 
 // One read window list per query load (moveQueryWindow, CHostSchedular.cu:12-23):
@@ -667,9 +473,16 @@ int clast_ctx_create(int device, clast_ctx** out) {
 void clast_ctx_destroy(clast_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
+  for (auto& a : ctx->arenas) {  // device copies of results, freed on the stream before it goes
+    for (auto& f : a->dev.f) f.release();
+    a->dev.evalue.release();
+    a->dev.load_offsets.release();
+  }
   if (ctx->st) cudaStreamSynchronize(ctx->st);
   ctx->ws.release_all();
   for (auto& a : ctx->arenas)
+    if (a->p) cudaFreeHost(a->p);
+  for (auto& a : ctx->tsv_arenas)
     if (a->p) cudaFreeHost(a->p);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -797,6 +610,7 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
     std::unique_ptr<clast_targets> T(new clast_targets());
     T->ctx = ctx;
     T->n_loads = n_loads;
+    for (int32_t k = 0; k < n_loads; ++k) T->load_first.push_back(T->load_first.back() + load_sizes[k]);
     cudaStream_t st = ctx->st;
     T->ev_start = ctx->timer.take();
     T->ev_up = ctx->timer.take();
@@ -1054,6 +868,7 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     dlo.alloc(lf.size());
     CLAST_CK(cudaMemcpyAsync(dlf.p, lf.data(), lf.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
     if (nreads > 0) gather_i64(moff, dlf.p, (int)lf.size(), dlo.p, st);
+    else CLAST_CK(cudaMemsetAsync(dlo.p, 0, lf.size() * sizeof(int64_t), st));
     clast_map_result res;
     std::memset(&res, 0, sizeof(res));
     res.n = F;
@@ -1097,6 +912,16 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     d2h32(res.match, m_match); d2h32(res.score, m_score);
     res.evalue = reinterpret_cast<double*>(take((F ? F : 1) * sizeof(double)));
     if (F) CLAST_CK(cudaMemcpyAsync(res.evalue, m_e.p, F * sizeof(double), cudaMemcpyDeviceToHost, st));
+    {  // the device copy stays with the arena for clast_format_tsv
+      PinnedArena::Device& d = arena->dev;
+      DevArray<int32_t>* src[10] = {&m_read, &m_strand, &m_load, &m_seq, &m_tidx, &m_qidx, &m_tlen, &m_qlen,
+                                    &m_match, &m_score};
+      for (int k = 0; k < 10; ++k) d.f[k] = std::move(*src[k]);
+      d.evalue = std::move(m_e);
+      d.load_offsets = std::move(dlo);
+      d.n = F;
+      d.n_loads = n_loads;
+    }
     CLAST_CK(cudaEventRecord(ctx->ev2, st));
     CLAST_CK(cudaEventSynchronize(ctx->ev2));
     float up = 0, ms = 0;
@@ -1378,163 +1203,3 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
   });
 }
 
-// ----------------------------------------------------------------------------
-// Index persistence: every window of a clast_targets in one file.
-// ----------------------------------------------------------------------------
-namespace {
-
-constexpr char kIndexMagic[8] = {'C', 'L', 'A', 'S', 'T', 'I', 'X', '1'};
-
-struct FileCloser {
-  FILE* f;
-  ~FileCloser() {
-    if (f) std::fclose(f);
-  }
-};
-
-template <class T>
-void put(FILE* f, const T& v) {
-  if (std::fwrite(&v, sizeof(T), 1, f) != 1) throw std::runtime_error("index file write failed");
-}
-template <class T>
-T get(FILE* f) {
-  T v;
-  if (std::fread(&v, sizeof(T), 1, f) != 1) throw std::invalid_argument("index file truncated");
-  return v;
-}
-
-// Device array -> file, through a host bounce buffer.
-template <class T>
-void put_array(FILE* f, const T* dev, int64_t count, std::vector<char>& buf, cudaStream_t st) {
-  const int64_t bytes = count * (int64_t)sizeof(T);
-  for (int64_t off = 0; off < bytes; off += (int64_t)buf.size()) {
-    const size_t len = (size_t)std::min<int64_t>((int64_t)buf.size(), bytes - off);
-    CLAST_CK(cudaMemcpyAsync(buf.data(), reinterpret_cast<const char*>(dev) + off, len, cudaMemcpyDeviceToHost, st));
-    CLAST_CK(cudaStreamSynchronize(st));
-    if (std::fwrite(buf.data(), 1, len, f) != len) throw std::runtime_error("index file write failed");
-  }
-}
-template <class T>
-void get_array(FILE* f, DevArray<T>& dev, int64_t count, std::vector<char>& buf, cudaStream_t st) {
-  if (count < 0 || count > ((int64_t)1 << 40)) throw std::invalid_argument("index file holds a bad array size");
-  dev.alloc((size_t)count);
-  const int64_t bytes = count * (int64_t)sizeof(T);
-  for (int64_t off = 0; off < bytes; off += (int64_t)buf.size()) {
-    const size_t len = (size_t)std::min<int64_t>((int64_t)buf.size(), bytes - off);
-    if (std::fread(buf.data(), 1, len, f) != len) throw std::invalid_argument("index file truncated");
-    CLAST_CK(cudaMemcpyAsync(reinterpret_cast<char*>(dev.p) + off, buf.data(), len, cudaMemcpyHostToDevice, st));
-    CLAST_CK(cudaStreamSynchronize(st));  // the bounce buffer is reused
-  }
-}
-
-}  // namespace
-
-extern "C" int clast_targets_save(clast_ctx* ctx, const clast_targets* T, const char* path) {
-  if (!ctx || !T || !path) return CLAST_ERR_ARG;
-  return guarded(ctx, [&]() -> int {
-    CLAST_CK(cudaSetDevice(ctx->device));
-    settle_targets(ctx, T);
-    FileCloser fc{std::fopen(path, "wb")};
-    if (!fc.f) throw std::invalid_argument(std::string("cannot open ") + path + " for writing");
-    FILE* f = fc.f;
-    cudaStream_t st = ctx->st;
-    std::vector<char> buf((size_t)64 << 20);
-    std::fwrite(kIndexMagic, 1, sizeof(kIndexMagic), f);
-    const clast_index* first = T->wins.empty() ? nullptr : T->wins[0].ix.get();
-    put<int32_t>(f, first ? first->l : 0);
-    put<int32_t>(f, first ? first->stride : 0);
-    put<int32_t>(f, first ? first->cut : 0);
-    put<int32_t>(f, T->n_loads);
-    put<int64_t>(f, (int64_t)T->wins.size());
-    for (const auto& w : T->wins) {
-      const clast_index& ix = *w.ix;
-      put<int32_t>(f, w.load);
-      put<int32_t>(f, w.first);
-      put<int32_t>(f, ix.t_begin);
-      put<int32_t>(f, ix.nseqs);
-      put<int64_t>(f, ix.n);
-      put<uint32_t>(f, ix.nbuckets);
-      put<int32_t>(f, ix.fshift);
-      put<int64_t>(f, ix.n_records);
-      put<int64_t>(f, (int64_t)ix.filter.n);
-      put<int64_t>(f, (int64_t)ix.entries.n);
-      put<int64_t>(f, ix.n_keys);
-      put_array(f, ix.bases.p, ix.n + 2 * kPad, buf, st);
-      put_array(f, ix.gateway.p, ix.nseqs, buf, st);
-      put_array(f, ix.lengths.p, ix.nseqs, buf, st);
-      put_array(f, ix.entries.p, (int64_t)ix.entries.n, buf, st);
-      put_array(f, ix.table.p, ix.n_records, buf, st);
-      put_array(f, ix.filter.p, (int64_t)ix.filter.n, buf, st);
-    }
-    if (std::fflush(f) != 0) throw std::runtime_error("index file write failed");
-    return CLAST_OK;
-  });
-}
-
-extern "C" int clast_targets_load(clast_ctx* ctx, const clast_params* p, const char* path, clast_targets** out) {
-  if (!ctx || !out || !path) return CLAST_ERR_ARG;
-  *out = nullptr;
-  return guarded(ctx, [&]() -> int {
-    check_params(p);
-    CLAST_CK(cudaSetDevice(ctx->device));
-    g_alloc_stream = ctx->st;
-    FileCloser fc{std::fopen(path, "rb")};
-    if (!fc.f) throw std::invalid_argument(std::string("cannot open ") + path);
-    FILE* f = fc.f;
-    char magic[sizeof(kIndexMagic)];
-    if (std::fread(magic, 1, sizeof(magic), f) != sizeof(magic) || std::memcmp(magic, kIndexMagic, sizeof(magic)))
-      throw std::invalid_argument(std::string(path) + " is not a clast index file");
-    const int32_t l = get<int32_t>(f), stride = get<int32_t>(f), cut = get<int32_t>(f);
-    const int32_t n_loads = get<int32_t>(f);
-    const int64_t n_wins = get<int64_t>(f);
-    if (n_wins > 0 && (l != p->lmer || stride != p->stride || cut != p->cut_repeat))
-      throw std::invalid_argument("the index was built with other lMer / stride / repeat settings");
-    if (n_loads < 0 || n_wins < 0 || n_wins > (int64_t)1 << 24) throw std::invalid_argument("bad index file header");
-    cudaStream_t st = ctx->st;
-    std::vector<char> buf((size_t)64 << 20);
-    std::unique_ptr<clast_targets> T(new clast_targets());
-    T->ctx = ctx;
-    T->n_loads = n_loads;
-    for (int64_t k = 0; k < n_wins; ++k) {
-      clast_targets::Win w;
-      w.load = get<int32_t>(f);
-      w.first = get<int32_t>(f);
-      std::unique_ptr<clast_index> ix(new clast_index());
-      ix->l = l;
-      ix->stride = stride;
-      ix->cut = cut;
-      ix->t_begin = get<int32_t>(f);
-      ix->nseqs = get<int32_t>(f);
-      ix->n = get<int64_t>(f);
-      ix->nbuckets = get<uint32_t>(f);
-      ix->fshift = get<int32_t>(f);
-      ix->n_records = get<int64_t>(f);
-      const int64_t n_filter = get<int64_t>(f), n_entries = get<int64_t>(f);
-      ix->n_keys = get<int64_t>(f);
-      if (ix->n < 0 || ix->nseqs < 0 || ix->nbuckets == 0 || ix->fshift < 32 || ix->fshift > 63 ||
-          ix->n_records < 2 * (int64_t)ix->nbuckets || n_filter != ((int64_t)1 << (64 - ix->fshift)))
-        throw std::invalid_argument("bad index file window header");
-      get_array(f, ix->bases, ix->n + 2 * kPad, buf, st);
-      get_array(f, ix->gateway, ix->nseqs, buf, st);
-      get_array(f, ix->lengths, ix->nseqs, buf, st);
-      get_array(f, ix->entries, n_entries, buf, st);
-      get_array(f, ix->table, ix->n_records, buf, st);
-      get_array(f, ix->filter, n_filter, buf, st);
-      w.ix = std::move(ix);
-      T->wins.push_back(std::move(w));
-    }
-    // nothing left to wait for: the targets are settled
-    T->failed.alloc(1);
-    CLAST_CK(cudaMemsetAsync(T->failed.p, 0, sizeof(unsigned long long), st));
-    T->ev_start = ctx->timer.take();
-    T->ev_up = ctx->timer.take();
-    T->ev_done = ctx->timer.take();
-    CLAST_CK(cudaEventRecord(T->ev_start, st));
-    CLAST_CK(cudaEventRecord(T->ev_up, st));
-    CLAST_CK(cudaEventRecord(T->ev_done, st));
-    CLAST_CK(cudaStreamSynchronize(st));
-    T->settled = true;
-    *out = T.release();
-    return CLAST_OK;
-  });
-}

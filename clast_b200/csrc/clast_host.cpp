@@ -399,81 +399,21 @@ class Loader {
   ParsedFasta cache_;
 };
 
-// ---------------------------------------------------------------------------
-// TSV (CHostResultHolder::printResult)
-// ---------------------------------------------------------------------------
-struct TargetMeta {
-  std::vector<std::vector<std::string>> labels;  // per load
-  std::vector<std::vector<int32_t>> start_idx;
-};
-
-void write_tsv(FILE* f, const Load& q, int64_t read0, const TargetMeta& tm, const clast_map_result& r, int64_t a,
-               int64_t b, int num_out) {
-  // which hits print: consecutive identical records are skipped and at most
-  // num_out per query label (the first is always printed)
-  const int64_t n = b - a;
-  std::vector<char> print(n, 0);
-  const std::string* pre_label = nullptr;
-  const std::string* pre_tlabel = nullptr;
-  int pre_qidx = 0, pre_tidx = 0, pre_tlen = 0, pre_qlen = 0, pre_match = 0, pre_score = 0;
-  char pre_strand = 0;
-  double pre_e = 0;
-  int count = 0;
-  static const std::string kEmpty;
-  for (int64_t j = 0; j < n; ++j) {
-    const int64_t i = a + j;
-    const std::string& ql = q.labels[r.read[i] - read0];
-    const bool new_label = !pre_label || *pre_label != ql;
-    if (new_label) count = 0;
-    if (num_out == -1 || new_label || count < num_out) {
-      const std::string& tl = tm.labels[r.t_load[i]][r.t_seq[i]];
-      const int tidx = r.t_idx[i] + tm.start_idx[r.t_load[i]][r.t_seq[i]];
-      const char strand = r.strand[i] ? '-' : '+';
-      if (new_label || pre_qidx != r.q_idx[i] || pre_strand != strand || *pre_tlabel != tl || pre_tidx != tidx ||
-          pre_tlen != r.t_len[i] || pre_qlen != r.q_len[i] || pre_match != r.match[i] ||
-          pre_score != r.score[i] || pre_e != r.evalue[i]) {
-        print[j] = 1;
-        ++count;
-        pre_label = &ql;
-        pre_qidx = r.q_idx[i];
-        pre_strand = strand;
-        pre_tlabel = &tl;
-        pre_tidx = tidx;
-        pre_tlen = r.t_len[i];
-        pre_qlen = r.q_len[i];
-        pre_match = r.match[i];
-        pre_score = r.score[i];
-        pre_e = r.evalue[i];
+// Labels of every record of a list of loads, flat (clast_labels).
+struct FlatLabels {
+  std::string chars;
+  std::vector<int64_t> offsets{0};
+  std::vector<int32_t> start_idx;
+  void add(const std::vector<Load>& loads) {
+    for (const Load& L : loads)
+      for (size_t i = 0; i < L.size(); ++i) {
+        chars += L.labels[i];
+        offsets.push_back((int64_t)chars.size());
+        start_idx.push_back(L.start_idx[i]);
       }
-    }
   }
-  // format in parallel chunks, write in order
-  const int64_t chunk = 1 << 14;
-  const int64_t nchunks = (n + chunk - 1) / chunk;
-  std::vector<std::string> bufs(nchunks);
-#pragma omp parallel for schedule(dynamic, 1)
-  for (int64_t c = 0; c < nchunks; ++c) {
-    std::string& o = bufs[c];
-    char line[512];
-    for (int64_t j = c * chunk; j < std::min(n, (c + 1) * chunk); ++j) {
-      if (!print[j]) continue;
-      const int64_t i = a + j;
-      const std::string& ql = q.labels[r.read[i] - read0];
-      const std::string& tl = tm.labels[r.t_load[i]][r.t_seq[i]];
-      const int tidx = r.t_idx[i] + tm.start_idx[r.t_load[i]][r.t_seq[i]];
-      // std::ostream's default double format is %g with precision 6
-      const int k = std::snprintf(line, sizeof(line), "\t%d\t%d\t%c\t", r.q_idx[i], r.q_len[i],
-                                  r.strand[i] ? '-' : '+');
-      o += ql;
-      o.append(line, k);
-      o += tl;
-      const int k2 = std::snprintf(line, sizeof(line), "\t%d\t%d\t%d(%g%%)\t%d\t%g\n", tidx, r.t_len[i], r.match[i],
-                                   (double)(r.match[i] * 100) / r.q_len[i], r.score[i], r.evalue[i]);
-      o.append(line, k2);
-    }
-  }
-  for (const auto& o : bufs) std::fwrite(o.data(), 1, o.size(), f);
-}
+  clast_labels view() const { return clast_labels{(int64_t)offsets.size() - 1, chars.data(), offsets.data()}; }
+};
 
 // Wall-clock phases of one command-line run, printed to stderr when the
 // environment variable CLAST_CLI_TIMING is set.
@@ -551,7 +491,6 @@ int run(int argc, const char* const* argv, std::string& err) {
   // concatenated targets and reads (a load's bases are contiguous already)
   std::string tb, qb;
   std::vector<int64_t> toff{0}, qoff{0}, tsizes, qsizes;
-  TargetMeta tm;
   auto concat = [](const std::vector<Load>& loads, std::string& b, std::vector<int64_t>& off,
                    std::vector<int64_t>& sizes) {
     size_t total = 0, recs = 0;
@@ -570,10 +509,9 @@ int run(int argc, const char* const* argv, std::string& err) {
   };
   concat(tloads, tb, toff, tsizes);
   concat(qloads, qb, qoff, qsizes);
-  for (const Load& L : tloads) {
-    tm.labels.push_back(L.labels);
-    tm.start_idx.push_back(L.start_idx);
-  }
+  FlatLabels tlabels, qlabels;
+  tlabels.add(tloads);
+  qlabels.add(qloads);
   clock.mark("concatenate");
   ctx_thread.join();
   clock.mark("CUDA context (wait)");
@@ -601,15 +539,22 @@ int run(int argc, const char* const* argv, std::string& err) {
   }
   std::unique_ptr<clast_map_result, void (*)(clast_map_result*)> r_guard(&res, clast_map_result_free);
   clock.mark("GPU search");
+  const clast_labels ql = qlabels.view(), tl = tlabels.view();
+  clast_tsv text;
+  rc = clast_format_tsv(ctx, targets, &res, (int32_t)qsizes.size(), &ql, &tl, tlabels.start_idx.data(), s.numOut,
+                        &text);
+  if (rc != CLAST_OK) {
+    err = clast_last_error(ctx);
+    return 6;
+  }
+  std::unique_ptr<clast_tsv, void (*)(clast_tsv*)> text_guard(&text, clast_tsv_free);
+  clock.mark("TSV text");
   FILE* f = std::fopen(s.out.c_str(), "ab");
   if (!f) throw UsageError(3, "cannot open output file " + s.out);
-  int64_t read0 = 0;
-  for (size_t k = 0; k < qloads.size(); ++k) {
-    write_tsv(f, qloads[k], read0, tm, res, res.load_offsets[k], res.load_offsets[k + 1], s.numOut);
-    read0 += (int64_t)qloads[k].size();
-  }
+  const bool ok = text.n_bytes == 0 || std::fwrite(text.text, 1, (size_t)text.n_bytes, f) == (size_t)text.n_bytes;
   std::fclose(f);
-  clock.mark("TSV");
+  if (!ok) throw UsageError(3, "cannot write output file " + s.out);
+  clock.mark("TSV write");
   return 0;
 }
 

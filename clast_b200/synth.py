@@ -202,7 +202,9 @@ def make_reads_fixed(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, in
     w /= w.sum()
     out = np.empty((n_reads, length), dtype=np.uint8)
     for b0 in range(0, n_reads, batch):
-        B = min(batch, n_reads - b0)
+        # every batch draws `batch` reads, so a smaller n_reads gives a prefix
+        # of a larger one
+        B = batch
         c = ok[rng.choice(len(ok), size=B, p=w)]
         start = target.offsets[c] + (rng.random(B) * (tl[c] - M + 1)).astype(np.int64)
         src = target.bases[start[:, None] + np.arange(M)[None, :]]
@@ -243,25 +245,79 @@ def make_reads_fixed(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, in
         r[rev] = _COMP[r[rev, ::-1]]
         dec = rng.random(B) < decoy_frac
         r[dec] = ACGT[rng.integers(0, 4, size=(int(dec.sum()), length))]
-        out[b0:b0 + B] = r
+        out[b0:b0 + B] = r[:min(B, n_reads - b0)]
     offsets = np.arange(n_reads + 1, dtype=np.int64) * length
     return SeqSet(["r%d" % i for i in range(n_reads)], out.ravel(), offsets)
 
 
-def workload(name: str, seed: int = 0xC1A57, scale: float = 1.0):
-    """(target, reads) for a named shape; ``scale`` shrinks sizes for tests."""
+def make_reads_var(rng, target: SeqSet, n_reads: int, len_range=(100, 5000), sub=0.02, rev_frac=0.5,
+                   decoy_frac=0.0) -> SeqSet:
+    """Vectorised reads of log-uniform length in ``len_range`` sampled
+    uniformly (by base) from the target, with substitutions at rate ``sub``
+    (no indels), reverse-complemented with probability ``rev_frac``, random
+    decoys with probability ``decoy_frac``."""
+    lo, hi = len_range
+    L = np.exp(rng.uniform(np.log(lo), np.log(hi), size=n_reads)).astype(np.int64)
+    tl = target.lengths
+    ok = np.flatnonzero(tl > hi + 1)
+    if ok.size == 0:
+        raise ValueError("target contigs shorter than the longest read")
+    w = tl[ok].astype(np.float64)
+    w /= w.sum()
+    c = ok[rng.choice(len(ok), size=n_reads, p=w)]
+    start = target.offsets[c] + (rng.random(n_reads) * (tl[c] - L)).astype(np.int64)
+    offsets = np.concatenate([[0], np.cumsum(L)]).astype(np.int64)
+    total = int(offsets[-1])
+    rid = np.repeat(np.arange(n_reads), L)
+    k = np.arange(total, dtype=np.int64) - offsets[rid]
+    rev = rng.random(n_reads) < rev_frac
+    pos = np.where(rev[rid], start[rid] + L[rid] - 1 - k, start[rid] + k)
+    b = target.bases[pos]
+    b = np.where(rev[rid], _COMP[b], b)
+    m = rng.random(total) < sub
+    idx = np.searchsorted(ACGT, b)
+    valid = (idx < 4) & (ACGT[np.minimum(idx, 3)] == b)
+    newb = ACGT[(np.where(valid, idx, 0) + rng.integers(1, 4, size=total)) % 4]
+    b = np.where(m & valid, newb, b).astype(np.uint8)
+    dec = rng.random(n_reads) < decoy_frac
+    if dec.any():
+        dmask = dec[rid]
+        b[dmask] = ACGT[rng.integers(0, 4, size=int(dmask.sum()))]
+    return SeqSet(["r%d" % i for i in range(n_reads)], b, offsets)
+
+
+def served_requests(rng, n_requests: int, pool: SeqSet, count_range=(1, 10_000)):
+    """Read ranges of ``n_requests`` requests with log-uniform read counts in
+    ``count_range``, taken one after another from ``pool`` (wrapping
+    around): a list of (first read, end read)."""
+    lo, hi = count_range
+    counts = np.exp(rng.uniform(np.log(lo), np.log(hi + 1), size=n_requests)).astype(np.int64)
+    counts = np.clip(counts, lo, min(hi, len(pool)))
+    out, at = [], 0
+    for c in counts:
+        if at + c > len(pool):
+            at = 0
+        out.append((at, at + int(c)))
+        at += int(c)
+    return out
+
+
+def workload(name: str, seed: int = 0xC1A57, scale: float = 1.0, n_reads: int | None = None):
+    """(target, reads) for a named shape; ``scale`` shrinks sizes for tests,
+    ``n_reads`` sets the read count (for ``medium``, the first n_reads of
+    the full read set)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     if name == "small":
         t = make_target(rng, int(1_000_000 * scale))
-        q = make_reads(rng, t, max(1, int(1000 * scale)))
+        q = make_reads(rng, t, n_reads or max(1, int(1000 * scale)))
     elif name == "medium":
         t = make_target(rng, int(100_000_000 * scale), n_contigs=max(1, int(200 * min(1.0, scale * 10))),
                         median=300_000 * scale, repeat_frac=0.10, n_families=max(1, int(500 * scale)))
-        q = make_reads_fixed(rng, t, max(1, int(1_000_000 * scale)))
+        q = make_reads_fixed(rng, t, n_reads or max(1, int(1_000_000 * scale)))
     elif name == "uneven":
         t = make_target(rng, int(100_000_000 * scale), n_contigs=max(1, int(200 * min(1.0, scale * 10))),
                         median=300_000 * scale, repeat_frac=0.10, n_families=max(1, int(500 * scale)))
-        q = make_reads(rng, t, max(1, int(200_000 * scale)), log_uniform=(50, 10_000),
+        q = make_reads(rng, t, n_reads or max(1, int(200_000 * scale)), log_uniform=(50, 10_000),
                        err_range=(0.01, 0.12), decoy_frac=0.0)
     else:
         raise ValueError("unknown workload %r" % name)

@@ -36,7 +36,9 @@ typedef enum clast_status {
   CLAST_ERR_ARG = -1,      /* invalid argument (sizes, parameter ranges) */
   CLAST_ERR_CUDA = -2,     /* a CUDA runtime call failed */
   CLAST_ERR_NOMEM = -3,    /* device or host allocation failed */
-  CLAST_ERR_INTERNAL = -4  /* internal consistency check failed */
+  CLAST_ERR_INTERNAL = -4, /* internal consistency check failed */
+  CLAST_ERR_CANCELLED = -5, /* a served request was cancelled */
+  CLAST_PENDING = 1         /* a served request is still queued or running */
 } clast_status;
 
 typedef struct clast_ctx clast_ctx;
@@ -161,6 +163,12 @@ void clast_targets_free(clast_targets* t);
  * other lmer / stride / cut_repeat settings or is not an index file. */
 int clast_targets_save(clast_ctx* ctx, const clast_targets* t, const char* path);
 int clast_targets_load(clast_ctx* ctx, const clast_params* p, const char* path, clast_targets** out);
+/* The checks clast_targets_load makes, on the host only (no device needed):
+ * the file's layout version, its settings, and every sequence range, entry
+ * range and table payload of every window against its arrays, so that a
+ * stale or corrupt file is rejected before any of it is uploaded.  0 when
+ * the file would load; otherwise CLAST_ERR_ARG and the reason in err. */
+int clast_targets_verify(const clast_params* p, const char* path, char* err, int err_len);
 
 /* Result of clast_map: hits of every query load in the order
  * CHostResultHolder::fixResult leaves them (load by load).  read = record
@@ -194,6 +202,42 @@ int clast_map(clast_ctx* ctx, const clast_targets* t, const clast_params* p, int
               clast_map_result* out);
 void clast_map_result_free(clast_map_result* r);
 
+/* ---- result text: CHostResultHolder::printResult (CHostResultHolder.cu:131-243) ---- */
+
+/* Labels of a set of records: label i = chars[offsets[i] .. offsets[i+1]). */
+typedef struct clast_labels {
+  int64_t n;
+  const char* chars;
+  const int64_t* offsets; /* n + 1 values */
+} clast_labels;
+
+/* The 10-column tab-separated text of a map result, every query load in
+ * order (load k's lines are text[load_offsets[k] .. load_offsets[k+1])).
+ * Owned by the library; release with clast_tsv_free. */
+typedef struct clast_tsv {
+  int64_t n_bytes;
+  const char* text;
+  int64_t* load_offsets; /* n_loads + 1 values */
+  void* owner;           /* library-internal */
+} clast_tsv;
+
+/* Formats the hits of a clast_map result as the reference's command line
+ * prints them, load by load (printResult is called once per query RAM load):
+ *   qLabel qIdx qHitLen strand tLabel tIdx+startIdx tHitLen match(pct%) score E
+ * with std::ostream's default number format (%g, 6 significant digits); a
+ * hit identical to the last printed line is skipped, and at most num_out
+ * lines are printed per run of equal query labels (-1: all).
+ *   t:            the targets r was mapped against;
+ *   reads:        the labels of every read given to clast_map (same order);
+ *   targets:      the labels of every target record given to
+ *                 clast_targets_create (all loads, in order);
+ *   t_start_idx:  per target record, the '@' start index (null: all 0).
+ * r must not have been released yet. */
+int clast_format_tsv(clast_ctx* ctx, const clast_targets* t, const clast_map_result* r, int32_t n_loads,
+                     const clast_labels* reads, const clast_labels* targets, const int32_t* t_start_idx,
+                     int32_t num_out, clast_tsv* out);
+void clast_tsv_free(clast_tsv* t);
+
 /* Device-side timing of the last clast_map call in milliseconds (kernels and
  * copies on the context's stream), and how many kernels it launched. */
 int clast_last_map_stats(const clast_ctx* ctx, double* device_ms, int64_t* kernel_launches);
@@ -224,8 +268,68 @@ typedef struct clast_stats {
   double map_wall_ms;        /* host wall time of the last clast_map          */
   double map_prep_ms;        /* ... of which host preparation before the first copy */
   double map_call_ms;        /* host wall time of the whole clast_map call, buffers released */
+  int64_t index_bases;       /* bases of every target window (joints included) of the last targets */
+  int64_t index_keys;        /* distinct l-mers kept in those windows' indexes after the repeat cut */
 } clast_stats;
 int clast_get_stats(const clast_ctx* ctx, clast_stats* out);
+
+/* ---- served form: resident targets, requests batched as they arrive ----
+ *
+ * No counterpart in the reference, whose only mode is the one-shot loop of
+ * main.cu:44-89.  A server keeps one clast_targets resident and runs
+ * `lanes` batches on the GPU at once, each on its own context (stream,
+ * scratch, pinned result buffers) on the targets' device.  A request is a
+ * set of reads; it is split into RAM loads of q_ram bases per strand and
+ * each load into query windows of q_vram bases, exactly as clast_map does
+ * for a query file of those reads, so a request's hits do not depend on the
+ * other requests it is batched with.  Admission: a free lane takes the
+ * queued requests in arrival order while their bases fit max_batch_bases
+ * and the device bytes estimated for every batch in flight fit hbm_budget;
+ * requests that arrive while batches run are taken by the next lane that
+ * frees up, so their work overlaps the batches already on the GPU. */
+typedef struct clast_server clast_server;
+typedef struct clast_server_config {
+  int32_t lanes;           /* batches in flight at once; 0: 2                         */
+  int32_t q_vram;          /* query window budget (bases, moveQueryWindow); 0: 2 MBase */
+  int32_t q_ram;           /* RAM load budget per strand (bases); 0: 32 MBase         */
+  int32_t reserved0;
+  int64_t max_batch_bases; /* read bases of one batch; 0: 8 MBase                     */
+  int64_t hbm_budget;      /* device bytes for the batches in flight; 0: free HBM at
+                              creation minus hbm_reserve                              */
+  int64_t hbm_reserve;     /* device bytes left free when hbm_budget is 0; 0: 2 GiB   */
+} clast_server_config;
+
+/* Starts the lanes.  t must have been created on ctx and outlive the server;
+ * the server does not use ctx after this call returns. */
+int clast_server_create(clast_ctx* ctx, const clast_targets* t, const clast_params* p,
+                        const clast_server_config* cfg, clast_server** out);
+/* Queues a request (the reads are copied; bases must be host memory) and
+ * returns its id at once.  CLAST_ERR_NOMEM when the request alone cannot fit
+ * the device budget. */
+int clast_server_submit(clast_server* s, const clast_seqs* reads, int64_t* request_id);
+/* Waits up to timeout_ms (0: no wait, -1: no limit) for a request.  CLAST_OK
+ * and its hits (read = record index within the request, loads = the
+ * request's RAM loads) when done; CLAST_PENDING while queued or running;
+ * CLAST_ERR_CANCELLED, or the failure's code, otherwise.  The result stays
+ * valid until clast_server_release(request_id). */
+int clast_server_poll(clast_server* s, int64_t request_id, int32_t timeout_ms, clast_map_result* out);
+/* Cancels a request that no lane has taken yet (CLAST_ERR_ARG otherwise). */
+int clast_server_cancel(clast_server* s, int64_t request_id);
+/* Forgets a finished (done, failed or cancelled) request and frees its result. */
+int clast_server_release(clast_server* s, int64_t request_id);
+/* Steady-clock nanoseconds (CLOCK_MONOTONIC) at which a request was queued,
+ * taken by a lane, and finished (its hits in host memory); 0 = not yet. */
+int clast_server_times(clast_server* s, int64_t request_id, int64_t* submit_ns, int64_t* start_ns, int64_t* done_ns);
+/* Counters since creation: batches run, requests finished, read bases
+ * mapped, and the largest number of requests in one batch. */
+typedef struct clast_server_stats {
+  int64_t batches, requests, bases, max_batch_requests, queued, running;
+  int64_t hbm_budget, hbm_in_flight_max;
+} clast_server_stats;
+int clast_server_get_stats(clast_server* s, clast_server_stats* out);
+const char* clast_server_last_error(const clast_server* s);
+/* Cancels every queued request, waits for the batches on the GPU, stops. */
+void clast_server_destroy(clast_server* s);
 
 /* Measurement helper, not part of the reference's seam: INT32 throughput of
  * the context's GPU (tera-ops/s) on the banded DP's operation mix (integer

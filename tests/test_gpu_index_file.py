@@ -1,10 +1,12 @@
 """Index persistence: clast_targets_save / clast_targets_load round trip
-through the C ABI gives the same clast_map result as the freshly built
-indexes, and a mismatched or foreign file is rejected."""
+through the C ABI gives the oracle's whole-job result (and the freshly built
+indexes' one), a saved file passes the host-side checks, and a mismatched or
+foreign file is rejected."""
 import numpy as np
 import pytest
 
 from clast_b200 import api, synth
+from _oracle_map import oracle_map
 
 pytestmark = pytest.mark.gpu
 
@@ -29,12 +31,20 @@ def test_saved_index_maps_identically(engine, tmp_path):
     path = str(tmp_path / "targets.clastix")
     engine.save_targets(T, path)
     T.close()
+    ok, why = api.verify_targets_file(s, path)
+    assert ok, why
     T2 = engine.load_targets(s, path)
+    ref = oracle_map(s, [t.seq(i).tobytes() for i in range(len(t))], [len(t)], 150_000,
+                     [q.seq(i).tobytes() for i in range(len(q))], [len(q)], 2_000_000)
     for _ in range(2):
         got = run_map(engine, s, T2, q)
         assert set(got) == set(want)
         for f in want:
             np.testing.assert_array_equal(got[f], want[f], err_msg=f)
+            if f == "evalue":
+                np.testing.assert_allclose(got[f], ref[f], rtol=1e-12, atol=0)
+            else:
+                np.testing.assert_array_equal(got[f], ref[f], err_msg=f)
     T2.close()
 
 

@@ -1,0 +1,40 @@
+"""Query sharding on the device path: the reads split by shard.shard_reads,
+each shard mapped by Engine.map (clast_map), the shards merged by
+shard.merge_shards, give the oracle's whole-job result.  The shards run one
+after another on one GPU; on several GPUs each would be one rank's work."""
+import numpy as np
+import pytest
+
+from clast_b200 import api, shard, synth
+from _oracle_map import oracle_map
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_map_merges_to_oracle(engine, world):
+    rng = np.random.Generator(np.random.PCG64(404))
+    t = synth.make_target(rng, 200_000, n_contigs=5, median=30_000)
+    q = synth.make_reads(rng, t, 900, log_uniform=(60, 600))
+    s = api.Setting(total_db=float(t.offsets[-1]))
+    q_loads, q_vram, t_vram = [300, 600], 20_000, 90_000
+    T = engine.targets(s, t.bases, t.offsets, [len(t)], t_vram)
+    lengths = np.diff(q.offsets)
+    shards = shard.shard_reads(lengths, q_loads, s.lmer, q_vram, world)
+    results = []
+    for (a, b, sizes, _ids) in shards:
+        sub_off = q.offsets[a:b + 1] - q.offsets[a]
+        res = engine.map(s, T, q.bases[q.offsets[a]:q.offsets[b]], sub_off, sizes, q_vram)
+        results.append({f: np.array(res[f]) for f in list(api.MAP_FIELDS) + ["load_offsets"]})
+        del res
+    merged = shard.merge_shards(results, shards, len(q_loads))
+    T.close()
+    want = oracle_map(s, [t.seq(i).tobytes() for i in range(len(t))], [len(t)], t_vram,
+                      [q.seq(i).tobytes() for i in range(len(q))], q_loads, q_vram)
+    assert len(want["read"]) > 200
+    np.testing.assert_array_equal(merged["load_offsets"], want["load_offsets"])
+    for f in api.MAP_FIELDS:
+        if f == "evalue":
+            np.testing.assert_allclose(merged[f], want[f], rtol=1e-12, atol=0)
+        else:
+            np.testing.assert_array_equal(merged[f], want[f], err_msg=f)
