@@ -236,54 +236,105 @@ struct DevHits {
   DevArray<int64_t> foff;
 };
 
-// CDeviceHitList for every query window of `qb` against one index.
-void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, const QueryBatch& qb,
-                  int32_t q_first, DevHits& out) {
+// Seeds of one target window for a query batch (createRawSeedList +
+// deleteSeedsOnSequenceBoundary), in the workspace slots of `slot`.
+struct SeedSet {
+  const clast_index* ix = nullptr;
+  int64_t* off = nullptr;
+  int32_t* len32 = nullptr;
+  int32_t* nvalid = nullptr;
+  unsigned long long* counters = nullptr;  // [1] DP cells, then seed_parts() cursors and l-mer counters
+  uint64_t* skey = nullptr;
+  uint32_t* sq = nullptr;
+  int64_t part_cap = 0;
+  int64_t S = 0;
+};
+
+// Seeds of up to kMaxSeedWins windows (all of `sets`) in one pass over the
+// query: the 2-bit words are read once and every l-mer's lookups in all the
+// windows are issued together.  A window whose seed partition overflowed is
+// seeded again (alone with the others that overflowed) with partitions sized
+// from the exact counts.
+void seed_windows(clast_ctx* c, const clast_params* p, const QueryBatch& qb, std::vector<SeedSet>& sets) {
   cudaStream_t st = c->st;
   Workspace& ws = c->ws;
   const QueryView q = qb.view();
-  const IndexView iv = ix->view();
+  const int64_t ns = qb.nstrands;
+  const int parts = seed_parts();
+  StageTimer& tm = c->timer;
+  std::vector<int> todo;
+  for (size_t k = 0; k < sets.size(); ++k) {
+    SeedSet& z = sets[k];
+    const std::string tag = "#" + std::to_string(k);
+    z.off = ws.get<int64_t>("s_off" + tag, ns + 1);
+    z.len32 = ws.get<int32_t>("s_len32" + tag, ns);
+    z.nvalid = ws.get<int32_t>("s_nvalid" + tag, ns);
+    z.counters = ws.get<unsigned long long>("s_counters" + tag, 2 + 2 * parts);
+    z.part_cap = std::max<int64_t>(c->seed_hint, qb.n / 16 + (1 << 20)) / parts + 1;
+    todo.push_back((int)k);
+  }
+  for (int attempt = 0; attempt < 2 && !todo.empty(); ++attempt) {
+    SeedWins W{};
+    for (size_t j = 0; j < todo.size(); ++j) {
+      SeedSet& z = sets[todo[j]];
+      const std::string tag = "#" + std::to_string(todo[j]);
+      z.skey = ws.get<uint64_t>("s_key" + tag, (size_t)z.part_cap * parts);
+      z.sq = ws.get<uint32_t>("s_q" + tag, (size_t)z.part_cap * parts);
+      CLAST_CK(cudaMemsetAsync(z.counters, 0, (2 + 2 * parts) * sizeof(unsigned long long), st));
+      W.w[j] = SeedWin{z.ix->view(), z.ix->tview(), z.counters + 2, z.counters + 2 + parts, z.off, z.len32,
+                       z.nvalid, z.skey, z.sq, z.part_cap};
+    }
+    tm.begin(st);
+    seed_multi(q, W, (int)todo.size(), p->gap, p->local, st);
+    tm.end(StageTimer::SEED, st);
+    std::vector<unsigned long long> cur(todo.size() * 2 * parts);
+    for (size_t j = 0; j < todo.size(); ++j)
+      CLAST_CK(cudaMemcpyAsync(cur.data() + j * 2 * parts, sets[todo[j]].counters + 2,
+                               2 * parts * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CLAST_CK(cudaStreamSynchronize(st));
+    std::vector<int> again;
+    for (size_t j = 0; j < todo.size(); ++j) {
+      SeedSet& z = sets[todo[j]];
+      const unsigned long long* cj = cur.data() + j * 2 * parts;
+      int64_t S = 0, most = 0, kmers = 0;
+      for (int i = 0; i < parts; ++i) {
+        S += (int64_t)cj[i];
+        most = std::max<int64_t>(most, (int64_t)cj[i]);
+        kmers += (int64_t)cj[parts + i];
+      }
+      z.S = S;
+      if (most <= z.part_cap) {
+        c->stats.query_kmers += kmers;
+        c->seed_hint = std::max<int64_t>(c->seed_hint, S + S / 4);
+      } else {
+        z.part_cap = most;  // strands past a full partition wrote nothing: run again
+        again.push_back(todo[j]);
+      }
+    }
+    todo.swap(again);
+  }
+  if (!todo.empty()) throw std::runtime_error("seed partitions overflowed twice");
+}
+
+// CDeviceHitList for every query window of `qb` against the window whose
+// seeds are in z: seed filters, DP, result order.
+void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, int32_t q_first, SeedSet& z,
+                   DevHits& out) {
+  cudaStream_t st = c->st;
+  Workspace& ws = c->ws;
+  const clast_index* ix = z.ix;
+  const QueryView q = qb.view();
   const TargetView tv = ix->tview();
   const int64_t ns = qb.nstrands, nr = ns / 2;
   out = DevHits();
-  if (ns == 0 || ix->n_keys == 0) return;
-  // createRawSeedList + deleteSeedsOnSequenceBoundary, one pass
-  int64_t* off = ws.get<int64_t>("s_off", ns + 1);
-  int32_t* len32 = ws.get<int32_t>("s_len32", ns);
-  int32_t* nvalid = ws.get<int32_t>("s_nvalid", ns);
-  const int parts = seed_parts();
-  // [1] DP cells, then one seed cursor and one l-mer count per partition
-  unsigned long long* counters = ws.get<unsigned long long>("s_counters", 2 + 2 * parts);
   StageTimer& tm = c->timer;
-  int64_t part_cap = std::max<int64_t>(c->seed_hint, qb.n / 16 + (1 << 20)) / parts + 1;
-  int64_t S = 0;
-  uint64_t* skey = nullptr;
-  uint32_t* sq = nullptr;
-  for (int attempt = 0; attempt < 2; ++attempt) {
-    skey = ws.get<uint64_t>("s_key", (size_t)part_cap * parts);
-    sq = ws.get<uint32_t>("s_q", (size_t)part_cap * parts);
-    CLAST_CK(cudaMemsetAsync(counters, 0, (2 + 2 * parts) * sizeof(unsigned long long), st));
-    tm.begin(st);
-    seed_fused(q, iv, tv, p->gap, p->local, counters + 2, counters + 2 + parts, off, len32, nvalid, skey, sq,
-               part_cap, st);
-    tm.end(StageTimer::SEED, st);
-    unsigned long long cur[128];
-    CLAST_CK(cudaMemcpyAsync(cur, counters + 2, 2 * parts * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-    CLAST_CK(cudaStreamSynchronize(st));
-    S = 0;
-    int64_t most = 0, kmers = 0;
-    for (int i = 0; i < parts; ++i) {
-      S += (int64_t)cur[i];
-      most = std::max<int64_t>(most, (int64_t)cur[i]);
-      kmers += (int64_t)cur[parts + i];
-    }
-    if (most <= part_cap) {
-      c->stats.query_kmers += kmers;
-      break;
-    }
-    part_cap = most;  // strands past a full partition wrote nothing: run again
-  }
-  c->seed_hint = std::max<int64_t>(c->seed_hint, S + S / 4);
+  const int64_t S = z.S;
+  int64_t* off = z.off;
+  int32_t* len32 = z.len32;
+  int32_t* nvalid = z.nvalid;
+  unsigned long long* counters = z.counters;
+  uint64_t* skey = z.skey;
+  uint32_t* sq = z.sq;
   auto add_counters = [&]() {
     unsigned long long cells = 0;
     CLAST_CK(cudaMemcpyAsync(&cells, counters + 1, sizeof(cells), cudaMemcpyDeviceToHost, st));
@@ -370,6 +421,17 @@ void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, co
   FinalOut fo{out.t_id.p, out.t_idx.p, out.q_id.p, out.q_idx.p, out.t_len.p, out.q_len.p, out.match.p,
               out.score.p, out.evalue.p};
   final_compact(fsel, roff, fcnt, foff, nr, hk, hs, o, ix->t_begin, q_first, fo, st);
+}
+
+// CDeviceHitList for every query window of `qb` against one index.
+void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, const QueryBatch& qb,
+                  int32_t q_first, DevHits& out) {
+  out = DevHits();
+  if (qb.nstrands == 0 || ix->n_keys == 0) return;
+  std::vector<SeedSet> sets(1);
+  sets[0].ix = ix;
+  seed_windows(c, p, qb, sets);
+  search_seeded(c, p, qb, q_first, sets[0], out);
 }
 
 template <class T>
@@ -835,7 +897,23 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     settle_targets(ctx, T);
     // every target window, in holder order (target load, window)
     std::vector<DevHits> per_win(T->wins.size());
-    for (size_t w = 0; w < T->wins.size(); ++w) search_batch(ctx, T->wins[w].ix.get(), p, qb, 0, per_win[w]);
+    // seeding several windows per pass over the query (CLAST_SEED_WINDOWS, 1..4)
+    int group = 2;
+    if (const char* e = std::getenv("CLAST_SEED_WINDOWS")) group = std::max(1, std::min(kMaxSeedWins, std::atoi(e)));
+    for (size_t g0 = 0; g0 < T->wins.size(); g0 += (size_t)group) {
+      std::vector<SeedSet> sets;
+      std::vector<size_t> idx;
+      for (size_t w = g0; w < std::min(T->wins.size(), g0 + (size_t)group); ++w) {
+        const clast_index* ix = T->wins[w].ix.get();
+        if (qb.nstrands == 0 || ix->n_keys == 0) continue;
+        sets.emplace_back();
+        sets.back().ix = ix;
+        idx.push_back(w);
+      }
+      if (sets.empty()) continue;
+      seed_windows(ctx, p, qb, sets);
+      for (size_t j = 0; j < sets.size(); ++j) search_seeded(ctx, p, qb, 0, sets[j], per_win[idx[j]]);
+    }
     // fixResult: stable merge by (read, score desc) over the windows, on the device
     std::vector<WinHits> wh;
     int64_t n_items = 0;

@@ -1028,6 +1028,265 @@ __global__ void __launch_bounds__(kSeedFusedThreads, SMALL ? 16 : 12) k_seed_fus
   if (lane == 0) nvalid[s] = valid;
 }
 
+// ------------------------------------------------------------------------
+// Seeding of several target windows in one pass over the query
+// ------------------------------------------------------------------------
+// One warp per strand as in k_seed_fused, but every round's l-mers are looked
+// up in NW target windows at once: the 2-bit words and N flags are read once
+// for all windows, the NW filter words of every l-mer are loaded together, and
+// the l-mers that pass a filter are listed in the warp's shared memory (code,
+// window, l-mer) so that the 32 lanes share the bucket reads evenly (about one
+// per lane and window in a round of 160 l-mers) instead of each lane reading
+// the buckets of its own l-mers.  Payloads land in shared memory, one slot per
+// (window, l-mer); the emission of each window's seeds is round_emit's.
+// A strand reserves its range in every window with one atomic per window,
+// issued by lanes 0..NW-1 together.
+template <int NW>
+struct SeedSmem {
+  uint64_t pl[NW][kSeedRound];  // payload of (window, l-mer) of the current round
+  union {
+    struct {
+      uint64_t code[NW * kSeedRound];
+      uint16_t tag[NW * kSeedRound];  // window << 8 | l-mer within the round
+    } list;                           // the l-mers that passed a window's filter
+    struct {
+      uint64_t pl[kSeedRound];
+      int32_t qi[kSeedRound];
+    } stage;  // round_emit's staging
+  } u;
+};
+
+// Payload of the key of code c in the table of one window (home bucket in one
+// 32-byte read, then linear probing).
+template <bool SMALL>
+__device__ __forceinline__ uint64_t bucket_payload(const IndexView& ix, uint64_t c) {
+  const int64_t home = SMALL ? record_home16((uint32_t)c, ix.l, ix.nbuckets) : record_home(c, ix.l, ix.nbuckets);
+  uint64_t c0, p0, c1, p1;
+  ld_bucket(ix.table + home, c0, p0, c1, p1);
+  if (c0 == c || p0 == kNoPayload) return p0;
+  if (c1 == c || p1 == kNoPayload) return p1;
+  return table_probe(ix, c, home + 2);
+}
+
+// Looks up the l-mers r0 + lane * P + i (i < P) of a strand in the NW windows.
+// When `keep`, their payloads go to sm.pl (kNoPayload for invalid or absent
+// l-mers); cnt[w] adds the entries of the l-mers this lane resolved in window
+// w.  Returns the number of valid l-mers of this lane.
+template <bool SMALL, int NW>
+__device__ __forceinline__ int round_lookup_multi(const QueryView& q, const SeedWins& W, int64_t st, int nk, int r0,
+                                                  int lane, SeedSmem<NW>& sm, bool keep, int (&cnt)[NW]) {
+  constexpr int P = kSeedPerLane;
+  const int l = W.w[0].ix.l;
+  const int q0 = r0 + lane * P;
+  const int nv = max(0, min(P, nk - q0));
+  uint64_t code[P];
+  uint32_t vmask = 0;
+#pragma unroll
+  for (int i = 0; i < P; ++i) code[i] = 0;
+  if (nv > 0) {
+    const int64_t f = st + q0;
+    vmask = (1u << nv) - 1;
+    if (SMALL) {
+      const uint32_t* p32 = reinterpret_cast<const uint32_t*>(q.packed);
+      const uint32_t* n32 = reinterpret_cast<const uint32_t*>(q.nmask);
+      const int64_t j0 = f >> 4, k0 = f >> 5;
+      const uint32_t u0 = __ldcs(p32 + (j0 ^ 1)), u1 = __ldcs(p32 + ((j0 + 1) ^ 1)),
+                     u2 = __ldcs(p32 + ((j0 + 2) ^ 1));
+      const uint32_t m0 = __ldcs(n32 + (k0 ^ 1)), m1 = __ldcs(n32 + ((k0 + 1) ^ 1));
+      const uint32_t nflag = __funnelshift_l(m1, m0, (int)(f & 31));
+      const int o = 2 * (int)(f & 15);
+      const uint32_t mask = (2 * l == 32) ? ~0u : ((1u << (2 * l)) - 1);
+#pragma unroll
+      for (int i = 0; i < P; ++i) {
+        const int bo = o + 2 * i;
+        const uint32_t x = bo < 32 ? __funnelshift_l(u1, u0, bo) : __funnelshift_l(u2, u1, bo - 32);
+        const uint32_t key = x >> (32 - 2 * l);
+        code[i] = (uint32_t)(key * (uint32_t)0x6659FD93u) & mask;  // order_code for l <= 16
+        if ((nflag << i) >> (32 - l)) vmask &= ~(1u << i);
+      }
+    } else {
+      const int64_t w0 = f >> 5, k0 = f >> 6;
+      const uint64_t u0 = ld_stream(q.packed + w0), u1 = ld_stream(q.packed + w0 + 1),
+                     u2 = ld_stream(q.packed + w0 + 2);
+      const uint64_t nflag = funnel64(ld_stream(q.nmask + k0), ld_stream(q.nmask + k0 + 1), (int)(f & 63));
+      const int o = 2 * (int)(f & 31);
+#pragma unroll
+      for (int i = 0; i < P; ++i) {
+        const int bo = o + 2 * i;
+        const uint64_t x = bo < 64 ? funnel64(u0, u1, bo) : funnel64(u1, u2, bo - 64);
+        code[i] = order_code(x >> (64 - 2 * l), l);
+        if ((nflag << i) >> (64 - l)) vmask &= ~(1u << i);
+      }
+    }
+  }
+  // the filter words of every window, all in flight together
+  uint32_t pass = 0;  // bit w * P + i
+  {
+    uint32_t fm[P], fw[NW][P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      const uint64_t h = key_hash(code[i]);
+      fm[i] = filter_mask(h);
+#pragma unroll
+      for (int w = 0; w < NW; ++w)
+        fw[w][i] = ((vmask >> i) & 1u) ? __ldg(W.w[w].ix.filter + filter_word(h, W.w[w].ix.fshift)) : 0u;
+    }
+#pragma unroll
+    for (int w = 0; w < NW; ++w)
+#pragma unroll
+      for (int i = 0; i < P; ++i)
+        if (((vmask >> i) & 1u) && (fw[w][i] & fm[i]) == fm[i]) pass |= 1u << (w * P + i);
+  }
+  if (keep) {
+#pragma unroll
+    for (int w = 0; w < NW; ++w)
+#pragma unroll
+      for (int i = 0; i < P; ++i) sm.pl[w][lane * P + i] = kNoPayload;
+  }
+  int total;
+  int k = warp_excl_scan(__popc(pass), lane, &total);
+#pragma unroll
+  for (int w = 0; w < NW; ++w)
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+      if ((pass >> (w * P + i)) & 1u) {
+        sm.u.list.code[k] = code[i];
+        sm.u.list.tag[k] = (uint16_t)((w << 8) | (lane * P + i));
+        ++k;
+      }
+  __syncwarp();
+  // the bucket reads, shared by the lanes: two in flight per lane
+  for (int j = lane; j < total; j += 64) {
+    const bool two = j + 32 < total;
+    const uint64_t ca = sm.u.list.code[j];
+    const int ta = sm.u.list.tag[j];
+    const uint64_t cb = two ? sm.u.list.code[j + 32] : 0ull;
+    const int tb = two ? sm.u.list.tag[j + 32] : 0;
+    const int wa = ta >> 8, wb = tb >> 8;
+    const IndexView& ia = W.w[wa].ix;
+    const int64_t ha = SMALL ? record_home16((uint32_t)ca, l, ia.nbuckets) : record_home(ca, l, ia.nbuckets);
+    uint64_t a0, a1, a2, a3, b0 = 0, b1 = kNoPayload, b2 = 0, b3 = kNoPayload;
+    ld_bucket(ia.table + ha, a0, a1, a2, a3);
+    int64_t hb = 0;
+    if (two) {
+      const IndexView& ib = W.w[wb].ix;
+      hb = SMALL ? record_home16((uint32_t)cb, l, ib.nbuckets) : record_home(cb, l, ib.nbuckets);
+      ld_bucket(ib.table + hb, b0, b1, b2, b3);
+    }
+    uint64_t pa;
+    if (a0 == ca || a1 == kNoPayload) pa = a1;
+    else if (a2 == ca || a3 == kNoPayload) pa = a3;
+    else pa = table_probe(ia, ca, ha + 2);
+    if (keep) sm.pl[wa][ta & 0xff] = pa;
+    const int na = payload_count(pa);
+#pragma unroll
+    for (int w = 0; w < NW; ++w) cnt[w] += (w == wa) ? na : 0;
+    if (two) {
+      uint64_t pb;
+      if (b0 == cb || b1 == kNoPayload) pb = b1;
+      else if (b2 == cb || b3 == kNoPayload) pb = b3;
+      else pb = table_probe(W.w[wb].ix, cb, hb + 2);
+      if (keep) sm.pl[wb][tb & 0xff] = pb;
+      const int nb = payload_count(pb);
+#pragma unroll
+      for (int w = 0; w < NW; ++w) cnt[w] += (w == wb) ? nb : 0;
+    }
+  }
+  __syncwarp();
+  return __popc(vmask);
+}
+
+template <bool SMALL, int NW>
+__global__ void __launch_bounds__(kSeedFusedThreads, NW <= 2 ? 16 : 8) k_seed_multi(QueryView q, SeedWins W, int gap,
+                                                                                    int local) {
+  constexpr int P = kSeedPerLane;
+  __shared__ SeedSmem<NW> smem[kSeedFusedThreads / 32];
+  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  if (s >= q.nstrands) return;
+  SeedSmem<NW>& sm = smem[wib];
+  const int64_t st = q.start[s];
+  const int qlen = q.len[s];
+  const int nk = qlen - W.w[0].ix.l + 1;
+  // L2 prefetch for the block kSeedPrefetchBlocks later (as in k_seed_fused);
+  // every address stays inside its array
+  if (wib == 0 && lane < 5) {
+    const int64_t sp = ((int64_t)blockIdx.x + kSeedPrefetchBlocks) * (kSeedFusedThreads / 32);
+    if (sp < q.nstrands && q.n > 0) {
+      const int64_t f = min(q.n - 1, st + (sp - s) * (q.n / q.nstrands));
+      const void* a = lane == 0 ? (const void*)(q.start + sp)
+                    : lane == 1 ? (const void*)(q.len + sp)
+                    : lane == 4 ? (const void*)(q.nmask + (f >> 6))
+                                : (const void*)(q.packed + min((f >> 5) + 16 * (lane - 2), q.n / 32 + 3));
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+    }
+  }
+  // pass 1: counts of every window; round 0's payloads stay in shared memory
+  int cnt[NW];
+#pragma unroll
+  for (int w = 0; w < NW; ++w) cnt[w] = 0;
+  int valid_kmers = 0;
+  if (nk > 0) {
+    for (int r0 = 0; r0 < nk; r0 += kSeedRound)
+      valid_kmers += round_lookup_multi<SMALL, NW>(q, W, st, nk, r0, lane, sm, r0 == 0, cnt);
+  }
+  valid_kmers = (int)__reduce_add_sync(kFull, (unsigned)valid_kmers);
+  int tot[NW];
+#pragma unroll
+  for (int w = 0; w < NW; ++w) tot[w] = (int)__reduce_add_sync(kFull, (unsigned)cnt[w]);
+  const int part = (int)(s % kSeedParts);
+  // the range reservations: lane w reserves window w's
+  unsigned long long rel = 0;
+  if (lane < NW) {
+    int my = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) my = (w == lane) ? tot[w] : my;
+    const SeedWin& sw = W.w[lane];
+    if (valid_kmers) atomicAdd(sw.n_kmers + part, (unsigned long long)valid_kmers);
+    rel = my ? atomicAdd(&sw.cursor[part], (unsigned long long)my) : 0ull;
+  }
+  int64_t wpos[NW];
+  bool ok[NW];
+  bool any = false;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) {
+    const unsigned long long r = __shfl_sync(kFull, rel, w);
+    const int64_t base = (int64_t)part * W.w[w].part_cap + (int64_t)r;
+    wpos[w] = base;
+    ok[w] = tot[w] > 0 && base + tot[w] <= (int64_t)(part + 1) * W.w[w].part_cap;
+    any |= ok[w];
+    if (lane == 0) {
+      W.w[w].off[s] = base;
+      W.w[w].cnt[s] = tot[w];
+      if (!ok[w]) W.w[w].nvalid[s] = 0;
+    }
+  }
+  if (!any) return;
+  // pass 2: the seeds of every window, round by round
+  int valid[NW];
+  int dummy[NW];
+#pragma unroll
+  for (int w = 0; w < NW; ++w) valid[w] = dummy[w] = 0;
+  for (int r0 = 0; r0 < nk; r0 += kSeedRound) {
+    if (r0 > 0) round_lookup_multi<SMALL, NW>(q, W, st, nk, r0, lane, sm, true, dummy);
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+      if (!ok[w]) continue;
+      uint64_t pl[P];
+#pragma unroll
+      for (int i = 0; i < P; ++i) pl[i] = sm.pl[w][lane * P + i];
+      round_emit(W.w[w].ix, W.w[w].t, gap, local, qlen, r0, lane, pl, wpos[w], valid[w], W.w[w].skey, W.w[w].sq,
+                 sm.u.stage.pl, sm.u.stage.qi);
+    }
+  }
+#pragma unroll
+  for (int w = 0; w < NW; ++w) {
+    const int v = (int)__reduce_add_sync(kFull, (unsigned)valid[w]);
+    if (lane == 0 && ok[w]) W.w[w].nvalid[s] = v;
+  }
+}
+
 __global__ void k_window_first(const int32_t* __restrict__ nvalid, const int32_t* __restrict__ wstart, int nwin,
                                int32_t* __restrict__ wfirst) {
   const int w = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -2057,6 +2316,25 @@ void seed_fused(const QueryView& q, const IndexView& ix, const TargetView& t, in
     k_seed_fused<false><<<grid, kSeedFusedThreads, 0, st>>>(q, ix, t, gap, local, cursors, n_kmers, off, cnt, nvalid,
                                                            skey, sq, part_cap);
   CLAST_LAUNCHED();
+}
+
+template <int NW>
+void launch_seed_multi(const QueryView& q, const SeedWins& W, int gap, int local, cudaStream_t st) {
+  const unsigned grid = blocks_for((int64_t)q.nstrands * 32, kSeedFusedThreads);
+  if (W.w[0].ix.l <= 16) k_seed_multi<true, NW><<<grid, kSeedFusedThreads, 0, st>>>(q, W, gap, local);
+  else k_seed_multi<false, NW><<<grid, kSeedFusedThreads, 0, st>>>(q, W, gap, local);
+  CLAST_LAUNCHED();
+}
+
+void seed_multi(const QueryView& q, const SeedWins& W, int nw, int gap, int local, cudaStream_t st) {
+  if (q.nstrands <= 0 || nw <= 0) return;
+  switch (nw) {
+    case 1: launch_seed_multi<1>(q, W, gap, local, st); break;
+    case 2: launch_seed_multi<2>(q, W, gap, local, st); break;
+    case 3: launch_seed_multi<3>(q, W, gap, local, st); break;
+    case 4: launch_seed_multi<4>(q, W, gap, local, st); break;
+    default: throw std::invalid_argument("seed_multi: 1 to 4 windows per pass");
+  }
 }
 
 template <class Load>

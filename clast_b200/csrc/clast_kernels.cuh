@@ -85,6 +85,26 @@ void seed_fused(const QueryView& q, const IndexView& ix, const TargetView& t, in
                 uint64_t* skey, uint32_t* sq, int64_t part_cap, cudaStream_t st);
 void window_first(const int32_t* nvalid, const int32_t* win_start, int n_windows, int32_t* win_first,
                   cudaStream_t st);
+// The same outputs as seed_fused for up to kMaxSeedWins target windows in one
+// pass over the query (each window with its own cursors, counters and seed
+// partitions).  Every window must have been built with the same l.
+struct SeedWin {
+  IndexView ix;
+  TargetView t;
+  unsigned long long* cursor;   // seed_parts() cursors
+  unsigned long long* n_kmers;  // seed_parts() l-mer counters
+  int64_t* off;
+  int32_t* cnt;
+  int32_t* nvalid;
+  uint64_t* skey;
+  uint32_t* sq;
+  int64_t part_cap;
+};
+constexpr int kMaxSeedWins = 4;
+struct SeedWins {
+  SeedWin w[kMaxSeedWins];
+};
+void seed_multi(const QueryView& q, const SeedWins& W, int nw, int gap, int local, cudaStream_t st);
 
 // Sorts every segment [off[i], off[i]+len[i]) of (k1, k2[, payload]) ascending by
 // (k1, k2).  Segments of <= 32 are sorted by one warp in registers, <= 2048 by one
