@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-tsv", action="store_true")
+    ap.add_argument("--tvram", type=float, default=None, help="target window budget in MBase (default 64)")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-lanes", type=int, default=2)
     ap.add_argument("--serve-batch", type=int, default=8_000_000)
@@ -85,11 +86,11 @@ def workload_config(args, t, q):
     return {
         "workload": "%s: %d bp target in %d contigs, %d reads of %s bp" % (
             args.workload, int(t.offsets[-1]), len(t), len(q),
-            "150" if args.workload != "uneven" else "50-10000"),
+            "150" if args.workload not in ("uneven",) else "50-10000"),
         "target_bp": int(t.offsets[-1]), "contigs": len(t), "reads": len(q),
         "query_bp": int(q.offsets[-1]),
         "settings": "reference defaults: lMer 15, stride 5, repeat 20, width 100, gap 8, global, cutOff 10, "
-                    "tRAM/qRAM/tVRAM 64, qVRAM 2 MBase",
+                    "tRAM %g, qRAM 64, tVRAM %g, qVRAM 2 MBase" % (T_RAM / 1e6, T_VRAM / 1e6),
         "l2": "inputs larger than L2 (target + reads + indexes >> 126 MB); no flush",
         "seed": args.seed,
     }
@@ -696,7 +697,17 @@ def run_reference(args):
 
 
 def main():
+    global T_RAM, T_VRAM
     args = parse()
+    if args.tvram:
+        T_VRAM = args.tvram * 1e6
+    if args.workload == "large":  # chromosomes of up to 250 Mbp: default tRAM 64 would skip every one
+        T_RAM = 260e6
+        T_VRAM = args.tvram * 1e6 if args.tvram else 260e6
+        args.no_plain = True  # per-window rebuilds of 3 Gbp of indexes: minutes per step
+        args.no_cpu_baseline = True  # one CPU index build of 3 Gbp is far beyond a bounded sample
+        if args.check == "load0":
+            args.check = "off"  # the large-window parity is a test of its own
     if args.impl == "reference":
         run_reference(args)
     else:

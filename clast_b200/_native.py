@@ -65,7 +65,8 @@ class clast_stats(C.Structure):
                 ("seed_launches", C.c_int64), ("dp_ms", C.c_double), ("dp_launches", C.c_int64),
                 ("sort_ms", C.c_double), ("final_ms", C.c_double), ("index_wall_ms", C.c_double),
                 ("map_wall_ms", C.c_double), ("map_prep_ms", C.c_double), ("map_call_ms", C.c_double),
-                ("index_bases", C.c_int64), ("index_keys", C.c_int64)]
+                ("index_bases", C.c_int64), ("index_keys", C.c_int64), ("dp_order_ms", C.c_double),
+                ("dp_order_kind", C.c_int32), ("dp_queue_chunk", C.c_int32)]
 
 
 # symbol name -> (restype, argtypes); the full export list of include/clast_gpu.h

@@ -377,21 +377,72 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
   o.evalue = ws.get<double>("d_e", H);
   o.keep = ws.get<uint8_t>("d_keep", H);
   DpParams dp{p->lmer, p->stride, p->gap, p->local, p->cutoff, p->total_db, p->K, p->lambda};
-  // reads of different lengths: the DP takes the hits longest first, so that a
+  // Reads of different lengths: the DP takes the hits longest first, so that a
   // warp's hits have about the same number of rows (the reference sorts them
-  // by rows before aligning too, CDeviceHitList_alignmentHits.cu:10-58)
-  const uint64_t* order = nullptr;
-  if (qb.max_len != qb.min_len && H > 1) {
-    const int rows_max = std::max(1, qb.max_len - p->lmer + 1);
-    int bits = 1;
-    while ((1ll << bits) <= rows_max) ++bits;
-    uint64_t* ok = ws.get<uint64_t>("h_order", H);
-    uint64_t* ok2 = ws.get<uint64_t>("h_order2", H);
-    dp_order_keys(hs, qb.len.p, H, p->lmer, rows_max, ok, st);
-    order = radix_sort_u64(ws, ok, nullptr, ok2, nullptr, H, 32, 32 + bits, st) ? ok2 : ok;
+  // by rows before aligning too, CDeviceHitList_alignmentHits.cu:10-58), by
+  // an exact sort or by length buckets; the kernel runs over a grid of all
+  // hits or as a persistent grid taking hits from a queue.  Which of these
+  // runs fastest is measured once per context and kind of batch (gap, mode,
+  // uneven or not) on a batch of at least kDpTuneHits hits; every variant
+  // writes the same results.
+  const bool uneven = qb.max_len != qb.min_len && H > 1;
+  auto make_order = [&](int kind) -> const uint64_t* {
+    if (kind == 0) return nullptr;
+    if (kind == 1) {
+      const int rows_max = std::max(1, qb.max_len - p->lmer + 1);
+      int bits = 1;
+      while ((1ll << bits) <= rows_max) ++bits;
+      uint64_t* ok = ws.get<uint64_t>("h_order", H);
+      uint64_t* ok2 = ws.get<uint64_t>("h_order2", H);
+      dp_order_keys(hs, qb.len.p, H, p->lmer, rows_max, ok, st);
+      return radix_sort_u64(ws, ok, nullptr, ok2, nullptr, H, 32, 32 + bits, st) ? ok2 : ok;
+    }
+    uint64_t* ob = ws.get<uint64_t>("h_border", H);
+    dp_bucket_order(ws, hs, qb.len.p, H, p->lmer, ob, st);
+    return ob;
+  };
+  unsigned long long* dp_head = ws.get<unsigned long long>("dp_head", 1);
+  auto launch_of = [&](const DpChoice& ch) {
+    DpLaunch m;
+    if (ch.queue) {
+      m.head = dp_head;
+      m.chunk = ch.chunk;
+    }
+    return m;
+  };
+  const int tune_key = (p->gap << 2) | (p->local ? 2 : 0) | (uneven ? 1 : 0);
+  auto it = c->dp_tuned.find(tune_key);
+  if (it == c->dp_tuned.end() && H >= kDpTuneHits && !std::getenv("CLAST_DP_NO_TUNE")) {
+    std::vector<DpChoice> cands;
+    for (int ord : (uneven ? std::vector<int>{1, 2} : std::vector<int>{0}))
+      for (int q_ : {0, 1})
+        for (int chunk : (q_ ? std::vector<int>{1, 2} : std::vector<int>{1})) cands.push_back(DpChoice{ord, q_ != 0, chunk});
+    float best = 1e30f;
+    DpChoice pick = cands[0];
+    for (const DpChoice& ch : cands) {
+      CLAST_CK(cudaEventRecord(c->ev_t0, st));
+      const uint64_t* order = make_order(ch.order);
+      banded_dp(tv, q, hk, hq, hs, order, H, dp, o, st, launch_of(ch));
+      CLAST_CK(cudaEventRecord(c->ev_t1, st));
+      CLAST_CK(cudaEventSynchronize(c->ev_t1));
+      float ms = 0;
+      CLAST_CK(cudaEventElapsedTime(&ms, c->ev_t0, c->ev_t1));
+      if (ms < best) {
+        best = ms;
+        pick = ch;
+      }
+    }
+    it = c->dp_tuned.emplace(tune_key, pick).first;
   }
+  DpChoice ch = it != c->dp_tuned.end() ? it->second : DpChoice{uneven ? 1 : 0, false, 1};
+  if (ch.order != 0 && !uneven) ch.order = 0;
+  c->stats.dp_order_kind = ch.order;
+  c->stats.dp_queue_chunk = ch.queue ? ch.chunk : 0;
   tm.begin(st);
-  banded_dp(tv, q, hk, hq, hs, order, H, dp, o, st);
+  const uint64_t* order = make_order(ch.order);
+  tm.end(StageTimer::DPORDER, st);
+  tm.begin(st);
+  banded_dp(tv, q, hk, hq, hs, order, H, dp, o, st, launch_of(ch));
   tm.end(StageTimer::DP, st);
   // resultSorting + deleteHits_duplicateResult, per read
   uint64_t* k1 = ws.get<uint64_t>("f_k1", H);
@@ -526,7 +577,8 @@ int clast_ctx_create(int device, clast_ctx** out) {
     (void)cudaGetLastError();
   }
   if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaEventCreate(&c->ev2) != cudaSuccess || cudaEventCreate(&c->ev3) != cudaSuccess)
+      cudaEventCreate(&c->ev2) != cudaSuccess || cudaEventCreate(&c->ev3) != cudaSuccess ||
+      cudaEventCreate(&c->ev_t0) != cudaSuccess || cudaEventCreate(&c->ev_t1) != cudaSuccess)
     return CLAST_ERR_CUDA;
   *out = c.release();
   return CLAST_OK;
@@ -550,6 +602,8 @@ void clast_ctx_destroy(clast_ctx* ctx) {
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->ev2) cudaEventDestroy(ctx->ev2);
   if (ctx->ev3) cudaEventDestroy(ctx->ev3);
+  if (ctx->ev_t0) cudaEventDestroy(ctx->ev_t0);
+  if (ctx->ev_t1) cudaEventDestroy(ctx->ev_t1);
   if (ctx->st_copy) {
     cudaStreamSynchronize(ctx->st_copy);
     cudaStreamDestroy(ctx->st_copy);
@@ -1015,6 +1069,7 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     S.dp_launches = ctx->timer.n[StageTimer::DP];
     S.sort_ms = ctx->timer.ms[StageTimer::SORT];
     S.final_ms = ctx->timer.ms[StageTimer::FINAL];
+    S.dp_order_ms = ctx->timer.ms[StageTimer::DPORDER];
     ctx->last_ms = up + ms;
     ctx->last_launches = g_kernel_launches;
     S.map_wall_ms = wall_ms() - w0;

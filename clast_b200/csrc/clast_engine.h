@@ -8,6 +8,7 @@
 
 #include <chrono>
 #include <cstdint>
+#include <map>
 #include <memory>
 #include <new>
 #include <stdexcept>
@@ -87,12 +88,12 @@ inline void upload_padded(const char* host, int64_t n, DevArray<char>& dev, cuda
 // CUDA-event timing of device stages on one stream: begin()/end() bracket
 // launches, flush() (after a stream synchronisation) adds up the intervals.
 struct StageTimer {
-  enum Stage { SEED = 0, DP = 1, SORT = 2, FINAL = 3, N_STAGES = 4 };
+  enum Stage { SEED = 0, DP = 1, SORT = 2, FINAL = 3, DPORDER = 4, N_STAGES = 5 };
   std::vector<cudaEvent_t> pool;
   struct Pending { int stage; cudaEvent_t a, b; };
   std::vector<Pending> pending;
-  double ms[N_STAGES] = {0, 0, 0, 0};
-  int64_t n[N_STAGES] = {0, 0, 0, 0};
+  double ms[N_STAGES] = {0, 0, 0, 0, 0};
+  int64_t n[N_STAGES] = {0, 0, 0, 0, 0};
   cudaEvent_t cur_a = nullptr;
 
   cudaEvent_t take() {
@@ -152,6 +153,16 @@ struct PinnedArena {
   } dev;
 };
 
+// How the banded DP of one kind of batch runs (measured, see search_seeded):
+// order 0 = none, 1 = exact sort by rows, 2 = length buckets; queue = the
+// persistent grid with `chunk` hits per lane per take.
+struct DpChoice {
+  int order = 0;
+  bool queue = false;
+  int chunk = 1;
+};
+constexpr int64_t kDpTuneHits = 1 << 16;
+
 }  // namespace clast
 
 struct clast_ctx {
@@ -171,6 +182,8 @@ struct clast_ctx {
   clast_stats stats{};
   StageTimer timer;
   int64_t seed_hint = 0;  // seed buffer capacity that sufficed before
+  std::map<int, clast::DpChoice> dp_tuned;  // by (gap, local, uneven)
+  cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;  // DP tuning
 };
 
 struct clast_index {

@@ -1970,17 +1970,20 @@ struct DpKernelArgs {
   DpOut o;
 };
 
-template <int GAP, bool LOCAL>
-__global__ void __launch_bounds__(128, GAP <= 9 ? 4 : (GAP <= 12 ? 3 : 2)) k_banded_dp(DpKernelArgs a) {
-  __shared__ int2 tab[32 * 32];  // [target letter][query letter], letters 'A'..'Z': (POINT + 7, match)
+// The letter-pair table (POINT + 7, match increment) of krnlMatrix.cuh in
+// shared memory: [target letter][query letter], letters 'A'..'Z'.
+__device__ __forceinline__ void dp_table_init(int2* tab) {
   for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
     const int2 w = cell_score(class_of_letter((i >> 5) < 26 ? (i >> 5) : kNClass),
                               class_of_letter((i & 31) < 26 ? (i & 31) : kNClass));
     tab[i] = make_int2(w.x - (kGapOpen + kGapExtend), w.y);
   }
-  __syncthreads();
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n) return;
+}
+
+// Extension of the hit at position i of the order (alignmentHits +
+// calculateEvalue + the two hit filters of deleteBadHits).
+template <int GAP, bool LOCAL>
+__device__ __forceinline__ void dp_one(const DpKernelArgs& a, const int2* tab, int64_t i) {
   const int64_t h = a.order ? (int64_t)(uint32_t)a.order[i] : i;
   const uint64_t k = a.hk[h];
   const int qidx = a.hq[h];
@@ -2009,13 +2012,113 @@ __global__ void __launch_bounds__(128, GAP <= 9 ? 4 : (GAP <= 12 ? 3 : 2)) k_ban
   a.o.keep[h] = keep ? 1 : 0;
 }
 
-template <int GAP>
-void launch_dp_gap(const DpKernelArgs& a, bool local, cudaStream_t st) {
+template <int GAP, bool LOCAL>
+__global__ void __launch_bounds__(128, GAP <= 9 ? 4 : (GAP <= 12 ? 3 : 2)) k_banded_dp(DpKernelArgs a) {
+  __shared__ int2 tab[32 * 32];
+  dp_table_init(tab);
+  __syncthreads();
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  dp_one<GAP, LOCAL>(a, tab, i);
+}
+
+// Persistent form: a grid that fills the GPU once; each warp takes the next
+// `chunk` x 32 hits of the order (longest first) from a queue head until the
+// queue is empty, so that warps which drew short hits go on to take more
+// while the long ones run.  No warp waits on another.
+template <int GAP, bool LOCAL>
+__global__ void __launch_bounds__(128, GAP <= 9 ? 4 : (GAP <= 12 ? 3 : 2))
+    k_banded_dp_queue(DpKernelArgs a, unsigned long long* __restrict__ head, int chunk) {
+  __shared__ int2 tab[32 * 32];
+  dp_table_init(tab);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned long long take = 32ull * (unsigned long long)chunk;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(head, take);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= (unsigned long long)a.n) break;
+    for (int c = 0; c < chunk; ++c) {
+      const int64_t i = (int64_t)base + 32 * c + lane;
+      if (i < a.n) dp_one<GAP, LOCAL>(a, tab, i);
+    }
+  }
+}
+
+// Length buckets of the hits for the DP order: 16 buckets per power of two of
+// the row count (rows within a bucket differ by at most 1/16), numbered so
+// that ascending bucket = longest first.
+constexpr int kDpBuckets = 16 * 33;
+__device__ __forceinline__ int dp_bucket(int rows) {
+  if (rows < 16) return kDpBuckets - 1 - rows;  // exact below 16
+  const int e = 31 - __clz(rows);                // rows in [2^e, 2^(e+1))
+  const int sub = (rows >> (e - 4)) & 15;
+  return kDpBuckets - 1 - (16 * (e - 3) + sub);
+}
+
+__global__ void k_dp_bucket_count(const int32_t* __restrict__ hs, const int32_t* __restrict__ q_len, int64_t n, int l,
+                                  unsigned int* __restrict__ count) {
+  __shared__ unsigned int c[kDpBuckets];
+  for (int i = threadIdx.x; i < kDpBuckets; i += blockDim.x) c[i] = 0;
+  __syncthreads();
+  for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < n; h += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&c[dp_bucket(max(0, q_len[hs[h]] - l))], 1u);
+  __syncthreads();
+  for (int i = threadIdx.x; i < kDpBuckets; i += blockDim.x)
+    if (c[i]) atomicAdd(&count[i], c[i]);
+}
+
+// exclusive scan of the bucket counts in one block (kDpBuckets <= 1024)
+__global__ void k_dp_bucket_scan(const unsigned int* __restrict__ count, unsigned long long* __restrict__ cursor) {
+  __shared__ unsigned long long v[1024];
+  const int i = threadIdx.x;
+  v[i] = i < kDpBuckets ? count[i] : 0;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const unsigned long long x = i >= o ? v[i - o] : 0;
+    __syncthreads();
+    v[i] += x;
+    __syncthreads();
+  }
+  if (i < kDpBuckets) cursor[i] = v[i] - count[i];
+}
+
+__global__ void k_dp_bucket_scatter(const int32_t* __restrict__ hs, const int32_t* __restrict__ q_len, int64_t n,
+                                    int l, unsigned long long* __restrict__ cursor, uint64_t* __restrict__ order) {
+  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= n) return;
+  const unsigned long long at = atomicAdd(&cursor[dp_bucket(max(0, q_len[hs[h]] - l))], 1ull);
+  order[at] = (uint64_t)h;
+}
+
+template <int GAP, bool LOCAL>
+void launch_dp_mode(const DpKernelArgs& a, const DpLaunch& m, cudaStream_t st) {
   const int threads = 128;
-  const unsigned grid = (unsigned)((a.n + threads - 1) / threads);
-  if (local) k_banded_dp<GAP, true><<<grid, threads, 0, st>>>(a);
-  else k_banded_dp<GAP, false><<<grid, threads, 0, st>>>(a);
+  if (m.head == nullptr) {
+    const unsigned grid = (unsigned)((a.n + threads - 1) / threads);
+    k_banded_dp<GAP, LOCAL><<<grid, threads, 0, st>>>(a);
+  } else {
+    static int sms = 0, per_sm = 0;
+    if (!sms) {
+      int dev = 0;
+      CLAST_CK(cudaGetDevice(&dev));
+      CLAST_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      CLAST_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_banded_dp_queue<GAP, LOCAL>, threads, 0));
+      per_sm = std::max(1, per_sm);
+    }
+    const int64_t need = (a.n + 32 * m.chunk - 1) / (32 * m.chunk) / (threads / 32) + 1;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, need));
+    CLAST_CK(cudaMemsetAsync(m.head, 0, sizeof(unsigned long long), st));
+    k_banded_dp_queue<GAP, LOCAL><<<grid, threads, 0, st>>>(a, m.head, m.chunk);
+  }
   CLAST_LAUNCHED();
+}
+
+template <int GAP>
+void launch_dp_gap(const DpKernelArgs& a, bool local, const DpLaunch& m, cudaStream_t st) {
+  if (local) launch_dp_mode<GAP, true>(a, m, st);
+  else launch_dp_mode<GAP, false>(a, m, st);
 }
 
 // ------------------------------------------------------------------------
@@ -2427,27 +2530,43 @@ void dp_order_keys(const int32_t* hs, const int32_t* q_len, int64_t n_hits, int 
   CLAST_LAUNCHED();
 }
 
+void dp_bucket_order(Workspace& ws, const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l, uint64_t* order,
+                     cudaStream_t st) {
+  if (n_hits <= 0) return;
+  unsigned int* count = ws.get<unsigned int>("dpb_count", kDpBuckets);
+  unsigned long long* cursor = ws.get<unsigned long long>("dpb_cursor", kDpBuckets);
+  CLAST_CK(cudaMemsetAsync(count, 0, kDpBuckets * sizeof(unsigned int), st));
+  k_dp_bucket_count<<<grid_cap(std::min<int64_t>(blocks_for(n_hits, 256), 1184)), 256, 0, st>>>(hs, q_len, n_hits, l,
+                                                                                                  count);
+  CLAST_LAUNCHED();
+  k_dp_bucket_scan<<<1, 1024, 0, st>>>(count, cursor);
+  CLAST_LAUNCHED();
+  k_dp_bucket_scatter<<<blocks_for(n_hits, 256), 256, 0, st>>>(hs, q_len, n_hits, l, cursor, order);
+  CLAST_LAUNCHED();
+}
+
 void banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq, const int32_t* hs,
-               const uint64_t* order, int64_t n_hits, const DpParams& p, const DpOut& o, cudaStream_t st) {
+               const uint64_t* order, int64_t n_hits, const DpParams& p, const DpOut& o, cudaStream_t st,
+               const DpLaunch& m) {
   if (n_hits <= 0) return;
   DpKernelArgs a{t, q, hk, hq, hs, order, n_hits, p, o};
   const bool local = p.local != 0;
   switch (p.gap) {
-    case 2: launch_dp_gap<2>(a, local, st); break;
-    case 3: launch_dp_gap<3>(a, local, st); break;
-    case 4: launch_dp_gap<4>(a, local, st); break;
-    case 5: launch_dp_gap<5>(a, local, st); break;
-    case 6: launch_dp_gap<6>(a, local, st); break;
-    case 7: launch_dp_gap<7>(a, local, st); break;
-    case 8: launch_dp_gap<8>(a, local, st); break;
-    case 9: launch_dp_gap<9>(a, local, st); break;
-    case 10: launch_dp_gap<10>(a, local, st); break;
-    case 11: launch_dp_gap<11>(a, local, st); break;
-    case 12: launch_dp_gap<12>(a, local, st); break;
-    case 13: launch_dp_gap<13>(a, local, st); break;
-    case 14: launch_dp_gap<14>(a, local, st); break;
-    case 15: launch_dp_gap<15>(a, local, st); break;
-    case 16: launch_dp_gap<16>(a, local, st); break;
+    case 2: launch_dp_gap<2>(a, local, m, st); break;
+    case 3: launch_dp_gap<3>(a, local, m, st); break;
+    case 4: launch_dp_gap<4>(a, local, m, st); break;
+    case 5: launch_dp_gap<5>(a, local, m, st); break;
+    case 6: launch_dp_gap<6>(a, local, m, st); break;
+    case 7: launch_dp_gap<7>(a, local, m, st); break;
+    case 8: launch_dp_gap<8>(a, local, m, st); break;
+    case 9: launch_dp_gap<9>(a, local, m, st); break;
+    case 10: launch_dp_gap<10>(a, local, m, st); break;
+    case 11: launch_dp_gap<11>(a, local, m, st); break;
+    case 12: launch_dp_gap<12>(a, local, m, st); break;
+    case 13: launch_dp_gap<13>(a, local, m, st); break;
+    case 14: launch_dp_gap<14>(a, local, m, st); break;
+    case 15: launch_dp_gap<15>(a, local, m, st); break;
+    case 16: launch_dp_gap<16>(a, local, m, st); break;
     default: throw std::invalid_argument("gap out of range 2..16");
   }
 }

@@ -132,11 +132,23 @@ struct DpParams {
   int l, stride, gap, local;
   double cutoff, total_db, K, lambda;
 };
+// How the DP kernel is launched: one thread per hit over a grid of all hits
+// (head null), or a persistent grid whose warps take `chunk` x 32 hits at a
+// time from a queue (head: a device counter the launch zeroes).  Results are
+// the same either way.
+struct DpLaunch {
+  unsigned long long* head = nullptr;
+  int chunk = 1;
+};
 // order (may be null): the hits in the order the threads take them, as words
 // whose low 32 bits are hit indices; outputs stay at the hit's own index.
 void banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq,
                const int32_t* hs, const uint64_t* order, int64_t n_hits, const DpParams& p, const DpOut& o,
-               cudaStream_t st);
+               cudaStream_t st, const DpLaunch& m = DpLaunch());
+// DP order by length buckets (16 per power of two of the row count, longest
+// first): order[k] = hit index, in one counting pass instead of a sort.
+void dp_bucket_order(Workspace& ws, const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l, uint64_t* order,
+                     cudaStream_t st);
 // keys[h] = (rows_max - rows of hit h) << 32 | h, rows = q_len[hs[h]] - l + 1:
 // ascending keys take the hits longest first.
 void dp_order_keys(const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l, int rows_max, uint64_t* keys,

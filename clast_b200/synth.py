@@ -14,6 +14,10 @@ machine.  Shapes:
 * ``uneven`` -- the medium target; 200,000 reads with log-uniform lengths in
   50 bp - 10 kbp, per-read error rate uniform in 1-12 % (70 % substitutions,
   30 % indels).
+* ``large``  -- a 3 Gbp genome of 24 chromosomes of 50-250 Mbp, 45 % of bases
+  in 1,000 repeat families of 300 bp - 6 kbp at 80-99 % identity, 1 % of bases
+  in N blocks (geometric length, mean 1 kbp); 5,000,000 reads of 150 bp
+  (medium's error model).  Chromosomes are labelled ``chr<i>``.
 
 Reads carry labels ``r<i>``; targets ``ctg<i>``.  Sizes scale with the
 arguments so tests can use small versions of each shape.
@@ -63,15 +67,17 @@ class SeqSet:
 
 
 def _rand_bases(rng, n):
-    return ACGT[rng.integers(0, 4, size=n)]
+    return ACGT[rng.integers(0, 4, size=n, dtype=np.uint8)]
 
 
 def make_target(rng, total_bp: int, n_contigs: int = 1, median: float | None = None,
                 n_frac: float = 0.001, n_run_mean: float = 10.0, repeat_frac: float = 0.0,
-                n_families: int = 0, fam_len=(300, 6000), fam_ident=(0.85, 0.99)) -> SeqSet:
-    """Random contigs (log-normal lengths when ``n_contigs > 1``) with N runs
-    and optional repeat families."""
-    if n_contigs == 1:
+                n_families: int = 0, fam_len=(300, 6000), fam_ident=(0.85, 0.99), lengths=None) -> SeqSet:
+    """Random contigs (log-normal lengths when ``n_contigs > 1``, or the given
+    ``lengths``) with N runs and optional repeat families."""
+    if lengths is not None:
+        lens = np.asarray(lengths, dtype=np.int64)
+    elif n_contigs == 1:
         lens = np.array([total_bp], dtype=np.int64)
     else:
         mean = total_bp / n_contigs
@@ -110,6 +116,15 @@ def make_target(rng, total_bp: int, n_contigs: int = 1, median: float | None = N
             bases[s:s + r] = ord("N")
     labels = ["ctg%d" % i for i in range(len(lens))]
     return SeqSet(labels, bases, offsets)
+
+
+def chromosome_lengths(rng, n: int, total_bp: int, lo: int, hi: int):
+    """n lengths in [lo, hi] summing to total_bp (uniform draws, rescaled)."""
+    x = rng.uniform(lo, hi, size=n)
+    x = x / x.sum() * total_bp
+    x = np.clip(x, lo, hi).astype(np.int64)
+    x[int(np.argmin(x))] += total_bp - int(x.sum())
+    return x
 
 
 def _mutate(rng, src: np.ndarray, out_len: int, sub: float, indel: float, indel_mean: float) -> np.ndarray:
@@ -319,6 +334,13 @@ def workload(name: str, seed: int = 0xC1A57, scale: float = 1.0, n_reads: int | 
                         median=300_000 * scale, repeat_frac=0.10, n_families=max(1, int(500 * scale)))
         q = make_reads(rng, t, n_reads or max(1, int(200_000 * scale)), log_uniform=(50, 10_000),
                        err_range=(0.01, 0.12), decoy_frac=0.0)
+    elif name == "large":
+        lens = chromosome_lengths(rng, 24, int(3_000_000_000 * scale), int(50_000_000 * scale),
+                                  int(250_000_000 * scale))
+        t = make_target(rng, int(lens.sum()), lengths=lens, n_frac=0.01, n_run_mean=1000.0, repeat_frac=0.45,
+                        n_families=max(1, int(1000 * scale)), fam_ident=(0.80, 0.99))
+        t.labels = ["chr%d" % (i + 1) for i in range(len(t))]
+        q = make_reads_fixed(rng, t, n_reads or max(1, int(5_000_000 * scale)))
     else:
         raise ValueError("unknown workload %r" % name)
     return t, q

@@ -270,6 +270,10 @@ typedef struct clast_stats {
   double map_call_ms;        /* host wall time of the whole clast_map call, buffers released */
   int64_t index_bases;       /* bases of every target window (joints included) of the last targets */
   int64_t index_keys;        /* distinct l-mers kept in those windows' indexes after the repeat cut */
+  double dp_order_ms;        /* the DP's hit order (sort or length buckets)  */
+  int32_t dp_order_kind;     /* DP order used last: 0 none, 1 sorted by rows, 2 length buckets */
+  int32_t dp_queue_chunk;    /* 0: one thread per hit over a full grid; k: persistent grid taking
+                                k x 32 hits per warp from a queue              */
 } clast_stats;
 int clast_get_stats(const clast_ctx* ctx, clast_stats* out);
 
