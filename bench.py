@@ -27,8 +27,10 @@ in the reference's output order.
 --impl reference times the reference's own CPU implementation (its sources
 built for the host CPU, oracle/_ref/clast_ref) on this box's cores.
 
-Multi-GPU (torchrun): each rank maps its own 1M reads (seed + rank) against a
-replicated target index; no data-path collective (weak scaling).
+Multi-GPU (torchrun): N ranks map N times the workload's reads, split on
+query-window boundaries (clast_b200/shard.py), against a replicated target
+index; no data-path collective (weak scaling); the shards are gathered and
+merged in rank order on rank 0 after timing.
 """
 from __future__ import annotations
 
@@ -430,12 +432,33 @@ def run_ours(args):
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    # data: same target on every rank, reads seeded by rank
-    t, q0 = synth.workload(args.workload, seed=args.seed, scale=args.scale)
-    q = q0 if rank == 0 else synth.workload(args.workload, seed=args.seed + 1000 * rank, scale=args.scale)[1]
+    # data: the same target on every rank.  One GPU maps the workload's reads;
+    # N GPUs map N times as many reads (weak scaling), split on query-window
+    # boundaries by shard.shard_reads: rank r maps its shard of the one read
+    # set, and the shards are merged in rank order after timing.
+    shard_info = None
+    if world == 1:
+        t, q = synth.workload(args.workload, seed=args.seed, scale=args.scale)
+        q_loads = None
+    else:
+        from clast_b200 import shard
+        per = synth.workload(args.workload, seed=args.seed, scale=args.scale, n_reads=1)  # the target only
+        t = per[0]
+        n_one = {"medium": 1_000_000, "large": 5_000_000}.get(args.workload)
+        if n_one is None:
+            raise SystemExit("multi-GPU runs shard the fixed-length workloads (medium, large)")
+        total = world * max(1, int(n_one * args.scale))
+        lengths = np.full(total, 150, dtype=np.int64)
+        _, loads_all = api.ram_loads(lengths, int(Q_RAM / 2))
+        shards = shard.shard_reads(lengths, loads_all, 15, int(Q_VRAM), world)
+        a, b, sizes, ids = shards[rank]
+        q = synth.workload(args.workload, seed=args.seed, scale=args.scale, n_reads=b - a, first=a)[1]
+        q_loads = list(sizes)
+        shard_info = (shards, len(loads_all), total)
     s = api.Setting(total_db=float(t.offsets[-1]))  # synthetic FASTA: every non-'>' line is bases
     t_keep, t_loads = api.ram_loads(np.diff(t.offsets), int(T_RAM))
-    q_keep, q_loads = api.ram_loads(np.diff(q.offsets), int(Q_RAM / 2))
+    q_keep, q_loads_rule = api.ram_loads(np.diff(q.offsets), int(Q_RAM / 2))
+    q_loads = q_loads if q_loads is not None else q_loads_rule
     assert t_keep.all() and q_keep.all()
     n_twin = len(target_windows(np.diff(t.offsets), t_loads, s.lmer, int(T_VRAM)))
     eng = api.Engine(local)
@@ -518,6 +541,19 @@ def run_ours(args):
         del res
         ms_e2e, _, res2, st2, hw_e2e = timed(t_pin, q_pin)
         assert np.array_equal(scores, res2["score"])
+        merged = None
+        if shard_info is not None:  # the shards, merged on rank 0 in rank order (untimed)
+            from clast_b200 import shard
+            mine = {f: np.array(res2[f]) for f in list(api.MAP_FIELDS) + ["load_offsets"]}
+            gathered = [None] * world if rank == 0 else None
+            dist.gather_object(mine, gathered, dst=0)
+            if rank == 0:
+                m = shard.merge_shards(gathered, shard_info[0], shard_info[1])
+                merged = {"reads": shard_info[2], "hits": int(len(m["read"])), "loads": shard_info[1],
+                          "shards": [[int(x[0]), int(x[1])] for x in shard_info[0]],
+                          "what": "shard.shard_reads split on query-window boundaries, shard.merge_shards in rank "
+                                  "order on rank 0, after timing"}
+            del gathered
         del res2
         tsv = None
         if not args.no_tsv:
@@ -526,8 +562,10 @@ def run_ours(args):
                    "host_ms": hw_tsv}
             del res3
     mbp_rank = q.offsets[-1] / 1e6
-    value = mbp_rank * world * args.steps / (ms_dev / 1e3)
-    e2e = mbp_rank * world * args.steps / (ms_e2e / 1e3)
+    # whole job: every rank's bases (the shards of one read set) over the slowest rank's time
+    mbp_all = shard_info[2] * 150 / 1e6 if shard_info is not None else mbp_rank
+    value = mbp_all * args.steps / (ms_dev / 1e3)
+    e2e = mbp_all * args.steps / (ms_e2e / 1e3)
     # roofline of the dominant device stage of one step
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
@@ -580,8 +618,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": round(ms_dev / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator clast_b200/synth.py; no public dataset)",
-        "config": dict(workload_config(args, t, q), parallelism="replicated index, reads sharded" if world > 1
-                       else "single GPU"),
+        "config": dict(workload_config(args, t, q), parallelism="replicated index, reads sharded on query windows"
+                       if world > 1 else "single GPU"),
         "e2e": {"value": round(e2e, 2), "unit": "Mbp/s", "ms_per_step": round(ms_e2e / args.steps, 3),
                 "h2d_bytes_per_step": int(t.offsets[-1] + q.offsets[-1]),
                 "d2h_bytes_per_step": int(st2["results"] * 48)},
@@ -593,8 +631,10 @@ def run_ours(args):
         "clocks": clk.summary(),
         "host_wall_ms_per_step": {"value_loop": hw_dev, "e2e_loop": hw_e2e},
     }
+    if merged is not None:
+        out["sharded"] = merged
     if tsv:
-        out["e2e_tsv"] = dict(tsv, value=round(mbp_rank * world / (tsv["ms_per_step"] / 1e3), 2), unit="Mbp/s",
+        out["e2e_tsv"] = dict(tsv, value=round(mbp_all / (tsv["ms_per_step"] / 1e3), 2), unit="Mbp/s",
                               what="targets + map from pinned host records, clast_format_tsv, file write")
     if rank == 0 and world == 1 and not args.no_plain:
         plain = PlainDropIn(eng, s, t, q, t_loads, q_loads)

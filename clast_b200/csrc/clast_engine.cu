@@ -1272,6 +1272,10 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
         most = std::max<int64_t>(most, (int64_t)cur[i]);
       }
       if (most <= part_cap) break;
+      if (most > fit)  // the partitions this window needs do not fit the scratch
+        throw std::invalid_argument("query window needs seed partitions of " + std::to_string(most) +
+                                    " seeds; clast_search_noalloc's scratch holds " + std::to_string(fit) +
+                                    " (use clast_search)");
       ws.arena_rewind(mark);  // strands past a full partition wrote nothing: run again, larger
       part_cap = most;
     }
@@ -1300,7 +1304,20 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
     o.evalue = ws.get<double>("d_e", H);
     o.keep = ws.get<uint8_t>("d_keep", H);
     DpParams dp{p->lmer, p->stride, p->gap, p->local, p->cutoff, p->total_db, p->K, p->lambda};
-    banded_dp(tv, q, hk, hq, hs, nullptr, H, dp, o, st);
+    // reads of different lengths: hits longest first (length buckets), as clast_search
+    // orders them, so that a warp's hits have about the same number of rows
+    const uint64_t* order = nullptr;
+    int32_t lmin = INT32_MAX, lmax = 0;
+    for (int32_t i = 0; i < n_qseqs; ++i) {
+      lmin = std::min(lmin, q_lengths[i]);
+      lmax = std::max(lmax, q_lengths[i]);
+    }
+    if (lmin != lmax && H > 1) {
+      uint64_t* ob = ws.get<uint64_t>("h_border", H);
+      dp_bucket_order(ws, hs, qlen, H, p->lmer, ob, st);
+      order = ob;
+    }
+    banded_dp(tv, q, hk, hq, hs, order, H, dp, o, st);
     // resultSorting + deleteHits_duplicateResult, per read
     uint64_t* k1 = ws.get<uint64_t>("f_k1", H);
     uint64_t* k2 = ws.get<uint64_t>("f_k2", H);

@@ -203,9 +203,13 @@ def make_reads(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, indel=0.
 
 
 def make_reads_fixed(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, indel=0.005, indel_mean=2.0,
-                     rev_frac=0.5, decoy_frac=0.05, batch=65536) -> SeqSet:
+                     rev_frac=0.5, decoy_frac=0.05, batch=65536, first: int = 0) -> SeqSet:
     """Vectorised fixed-length version of :func:`make_reads` (same error model:
-    substitutions, indel events of geometric length, reverse strand, decoys)."""
+    substitutions, indel events of geometric length, reverse strand, decoys).
+    Reads come in batches of ``batch``, batch k drawn from its own stream
+    (``rng``'s bit generator jumped k + 1 times), so reads [first, first +
+    n_reads) of the sequence can be made without the ones before them."""
+    base_bg = rng.bit_generator
     tl = target.lengths
     cum = np.concatenate([[0], np.cumsum(tl)])
     pad = 16 + 8 * int(np.ceil(length * indel * indel_mean))
@@ -216,10 +220,10 @@ def make_reads_fixed(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, in
     w = tl[ok].astype(np.float64)
     w /= w.sum()
     out = np.empty((n_reads, length), dtype=np.uint8)
-    for b0 in range(0, n_reads, batch):
-        # every batch draws `batch` reads, so a smaller n_reads gives a prefix
-        # of a larger one
-        B = batch
+    k0 = first // batch
+    for k in range(k0, (first + n_reads + batch - 1) // batch):
+        rng = np.random.Generator(base_bg.jumped(k + 1))
+        B = batch  # every batch draws `batch` reads: any range is a slice of the same sequence
         c = ok[rng.choice(len(ok), size=B, p=w)]
         start = target.offsets[c] + (rng.random(B) * (tl[c] - M + 1)).astype(np.int64)
         src = target.bases[start[:, None] + np.arange(M)[None, :]]
@@ -247,8 +251,8 @@ def make_reads_fixed(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, in
         j = np.searchsorted(flat, o, side="right").reshape(B, length) - np.arange(B)[:, None] * M
         j = np.minimum(j, M - 1)
         before = np.take_along_axis(cs, j, axis=1) - np.take_along_axis(emit, j, axis=1)
-        k = np.arange(length)[None, :] - before   # rank within position j's emission
-        is_ins = k < np.take_along_axis(n_ins, j, axis=1)
+        rank = np.arange(length)[None, :] - before   # rank within position j's emission
+        is_ins = rank < np.take_along_axis(n_ins, j, axis=1)
         r = np.take_along_axis(src, j, axis=1)
         r = np.where(is_ins, ACGT[rng.integers(0, 4, size=(B, length))], r)
         m = rng.random((B, length)) < sub
@@ -260,9 +264,10 @@ def make_reads_fixed(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, in
         r[rev] = _COMP[r[rev, ::-1]]
         dec = rng.random(B) < decoy_frac
         r[dec] = ACGT[rng.integers(0, 4, size=(int(dec.sum()), length))]
-        out[b0:b0 + B] = r[:min(B, n_reads - b0)]
+        lo, hi = max(first, k * batch), min(first + n_reads, (k + 1) * batch)
+        out[lo - first:hi - first] = r[lo - k * batch:hi - k * batch]
     offsets = np.arange(n_reads + 1, dtype=np.int64) * length
-    return SeqSet(["r%d" % i for i in range(n_reads)], out.ravel(), offsets)
+    return SeqSet(["r%d" % i for i in range(first, first + n_reads)], out.ravel(), offsets)
 
 
 def make_reads_var(rng, target: SeqSet, n_reads: int, len_range=(100, 5000), sub=0.02, rev_frac=0.5,
@@ -317,10 +322,10 @@ def served_requests(rng, n_requests: int, pool: SeqSet, count_range=(1, 10_000))
     return out
 
 
-def workload(name: str, seed: int = 0xC1A57, scale: float = 1.0, n_reads: int | None = None):
+def workload(name: str, seed: int = 0xC1A57, scale: float = 1.0, n_reads: int | None = None, first: int = 0):
     """(target, reads) for a named shape; ``scale`` shrinks sizes for tests,
-    ``n_reads`` sets the read count (for ``medium``, the first n_reads of
-    the full read set)."""
+    ``n_reads`` sets the read count; for ``medium`` and ``large`` the reads
+    are reads [first, first + n_reads) of one fixed sequence."""
     rng = np.random.Generator(np.random.PCG64(seed))
     if name == "small":
         t = make_target(rng, int(1_000_000 * scale))
@@ -328,7 +333,7 @@ def workload(name: str, seed: int = 0xC1A57, scale: float = 1.0, n_reads: int | 
     elif name == "medium":
         t = make_target(rng, int(100_000_000 * scale), n_contigs=max(1, int(200 * min(1.0, scale * 10))),
                         median=300_000 * scale, repeat_frac=0.10, n_families=max(1, int(500 * scale)))
-        q = make_reads_fixed(rng, t, n_reads or max(1, int(1_000_000 * scale)))
+        q = make_reads_fixed(rng, t, n_reads or max(1, int(1_000_000 * scale)), first=first)
     elif name == "uneven":
         t = make_target(rng, int(100_000_000 * scale), n_contigs=max(1, int(200 * min(1.0, scale * 10))),
                         median=300_000 * scale, repeat_frac=0.10, n_families=max(1, int(500 * scale)))
@@ -340,7 +345,7 @@ def workload(name: str, seed: int = 0xC1A57, scale: float = 1.0, n_reads: int | 
         t = make_target(rng, int(lens.sum()), lengths=lens, n_frac=0.01, n_run_mean=1000.0, repeat_frac=0.45,
                         n_families=max(1, int(1000 * scale)), fam_ident=(0.80, 0.99))
         t.labels = ["chr%d" % (i + 1) for i in range(len(t))]
-        q = make_reads_fixed(rng, t, n_reads or max(1, int(5_000_000 * scale)))
+        q = make_reads_fixed(rng, t, n_reads or max(1, int(5_000_000 * scale)), first=first)
     else:
         raise ValueError("unknown workload %r" % name)
     return t, q

@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Builds the CLAST reference itself for the host CPU -- test infrastructure only.
 
-Recipe: every translation unit of the reference (the flat source directory,
-default /root/reference) is compiled with g++ against Thrust's sequential CPP
+Recipe: every translation unit of the reference (the flat source directory:
+--ref, or CLAST_REFERENCE_DIR, or the build container's mount point) is compiled with g++ against Thrust's sequential CPP
 device system, so thrust::device_vector storage is host memory and every
 Thrust algorithm runs on the CPU.  The reference sources are read where they
 lie and are not edited on disk; the only rewrite is mechanical and happens on
@@ -34,6 +34,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_REF = "/root/reference"  # where the build container mounts the reference sources
 OUT = os.path.join(HERE, "_ref")
 SRC = os.path.join(OUT, "src")
 SHIM = os.path.join(HERE, "refshim")
@@ -67,7 +68,8 @@ def rewrite(text):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("CLAST_REFERENCE_DIR", DEFAULT_REF),
+                    help="the reference's source directory (also CLAST_REFERENCE_DIR)")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--cxx", default="g++")
     args = ap.parse_args()

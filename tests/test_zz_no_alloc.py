@@ -57,6 +57,19 @@ def test_other_settings(eng, gap, local):
     ix.close()
 
 
+def test_uneven_read_lengths(eng):
+    # reads of 50 bp - 3 kbp: the DP takes the hits longest first here too
+    s, tl, ql = make_case(71, target_bp=200_000, n_contigs=4, n_reads=60, log_uniform=(50, 3000),
+                          err_range=(0.01, 0.12), decoy_frac=0.0)
+    ix = eng.hash_table(s, tl, 0, len(tl.lengths))
+    nq = len(ql.lengths) // 2
+    want = eng.hit_list(s, ix, ql, 0, nq)
+    assert len(want["t_id"]) > 20
+    for _ in range(2):
+        same(eng.hit_list_noalloc(s, ix, ql, 0, nq, capacity=len(want["t_id"])), want)
+    ix.close()
+
+
 def test_capacity_too_small_reports_count(eng):
     s, tl, ql = make_case(8)
     ix = eng.hash_table(s, tl, 0, len(tl.lengths))
