@@ -76,6 +76,10 @@ def parse():
     ap.add_argument("--no-tsv", action="store_true")
     ap.add_argument("--tvram", type=float, default=None, help="target window budget in MBase (default 64)")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true")
+    ap.add_argument("--uneven-reads", type=int, default=200_000)
+    ap.add_argument("--uneven-steps", type=int, default=3)
+    ap.add_argument("--uneven-warmup", type=int, default=2)
     ap.add_argument("--serve-lanes", type=int, default=2)
     ap.add_argument("--serve-batch", type=int, default=8_000_000)
     ap.add_argument("--serve-pool", type=int, default=60_000)
@@ -422,12 +426,76 @@ def served_leg(eng, s, t, t_loads, args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def run_ours(args):
+def uneven_leg(eng, s, t, t_loads, reads, args):
+    """The batched uneven-read shape: the medium target and reads of 50 bp -
+    10 kbp (per-read error 1-12 %), mapped in one clast_map per step with the
+    DP's order and launch chosen by the context's autotuner; beside it the
+    same job with the autotuner off (exact sort, one thread per hit over a
+    full grid).  Mbp/s with inputs in HBM, CUDA events."""
     import torch
-    import torch.distributed as dist
+    qb, ql = reads
+    q_off = np.concatenate([[0], np.cumsum(ql)]).astype(np.int64)
+    _, q_loads = api.ram_loads(ql, int(Q_RAM / 2))
+    t_dev = torch.from_numpy(t.bases).to("cuda")
+    q_dev = torch.from_numpy(qb).to("cuda")
+    mbp = q_off[-1] / 1e6
+    out = {"reads": int(len(ql)), "query_bp": int(q_off[-1]),
+           "config": "medium target; %d reads of 50-10,000 bp (log-uniform), per-read error 1-12 %% (70 %% "
+                     "substitutions, 30 %% indels); reference defaults" % len(ql)}
+
+    def run(engine, tag):
+        T = engine.targets(s, t_dev, t.offsets, t_loads, int(T_VRAM))
+        for _ in range(args.uneven_warmup):
+            r = engine.map(s, T, q_dev, q_off, q_loads, int(Q_VRAM))
+            del r
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.uneven_steps):
+            r = engine.map(s, T, q_dev, q_off, q_loads, int(Q_VRAM))
+            st = engine.stats()
+            del r
+        e1.record()
+        torch.cuda.synchronize()
+        T.close()
+        ms = e0.elapsed_time(e1) / args.uneven_steps
+        int32_peak = engine.int32_peak()
+        dp_frac = 13 * st["dp_cells"] / (st["dp_ms"] / 1e3) / 1e12 / int32_peak if st["dp_ms"] > 0 else None
+        out[tag] = {"value": round(mbp / (ms / 1e3), 2), "unit": "Mbp/s", "ms_per_step": round(ms, 2),
+                    "dp_ms": round(st["dp_ms"], 2), "dp_order_ms": round(st["dp_order_ms"], 2),
+                    "dp_gcups": round(st["dp_cells"] / (st["dp_ms"] / 1e3) / 1e9, 1) if st["dp_ms"] > 0 else None,
+                    "dp_frac_int32": round(dp_frac, 4) if dp_frac else None,
+                    "dp_order": {0: "none", 1: "sorted by rows", 2: "length buckets"}[st["dp_order_kind"]],
+                    "dp_launch": ("persistent queue, %d x 32 hits per take" % st["dp_queue_chunk"])
+                    if st["dp_queue_chunk"] else "one thread per hit, full grid"}
+
+    run(eng, "tuned")
+    os.environ["CLAST_DP_NO_TUNE"] = "1"
+    plain = api.Engine(torch.cuda.current_device())
+    try:
+        run(plain, "untuned")
+    finally:
+        plain.close()
+        del os.environ["CLAST_DP_NO_TUNE"]
+    out["tuned_over_untuned"] = round(out["tuned"]["value"] / out["untuned"]["value"], 3)
+    return out
+
+
+def run_ours(args):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    # the uneven-read leg's reads, made in spawned processes before CUDA starts
+    uneven_job = None
+    if world == 1 and args.workload == "medium" and not args.no_uneven:
+        import multiprocessing as mp
+        chunks = 8
+        per = args.uneven_reads // chunks
+        pool = mp.get_context("spawn").Pool(min(chunks, os.cpu_count() or 1))
+        uneven_job = (pool, pool.starmap_async(synth.uneven_chunk, [(args.seed, k, per, args.scale)
+                                                                     for k in range(chunks)]))
+    import torch
+    import torch.distributed as dist
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -483,8 +551,7 @@ def run_ours(args):
         res = eng.map(s, T, qb, q.offsets, q_loads, int(Q_VRAM))
         c2 = time.perf_counter()
         if tsv:  # the result text, written to a file
-            with open(tsv_path, "wb") as f:
-                n = eng.format_tsv(T, res, qlab, tlab, out=f)
+            n = eng.format_tsv(T, res, qlab, tlab, out=tsv_path)
             c2b = time.perf_counter()
             host["write"].append((c2b - c2) * 1e3)
             res.tsv_bytes = n
@@ -657,6 +724,16 @@ def run_ours(args):
                     "holder merge on the host; wall time",
             "map_e2e_over_plain": round(e2e / (mbp_rank / (p_ms / 1e3)), 2)}
         del plain
+    if uneven_job is not None:
+        try:
+            parts = uneven_job[1].get(timeout=1200)
+            uneven_job[0].close()
+            reads = (np.concatenate([p[0] for p in parts]), np.concatenate([p[1] for p in parts]))
+            out["uneven"] = uneven_leg(eng, s, t, t_loads, reads, args)
+        except Exception as e:  # reported, never fatal
+            out["uneven"] = {"error": str(e)[:300]}
+        finally:
+            uneven_job[0].terminate()
     if rank == 0 and world == 1 and not args.no_serve:
         try:
             out["served"] = served_leg(eng, s, t, t_loads, args)

@@ -202,6 +202,51 @@ def make_reads(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, indel=0.
     return SeqSet(["r%d" % i for i in range(n_reads)], bases, offsets)
 
 
+def _mutated_batch(rng, target: SeqSet, B: int, length: int, M: int, sub, indel, indel_mean: float, ok, w):
+    """B reads of `length` bases: sources of M bases at uniform target
+    positions with substitutions and indel events (rates scalar or per read),
+    vectorised.  Returns a (B, length) uint8 array."""
+    tl = target.lengths
+    sub = np.broadcast_to(np.asarray(sub, dtype=np.float64), (B,))[:, None]
+    indel = np.broadcast_to(np.asarray(indel, dtype=np.float64), (B,))[:, None]
+    c = ok[rng.choice(len(ok), size=B, p=w)]
+    start = target.offsets[c] + (rng.random(B) * (tl[c] - M + 1)).astype(np.int64)
+    src = target.bases[start[:, None] + np.arange(M)[None, :]]
+    ev = rng.random((B, M)) < indel
+    ins = ev & (rng.random((B, M)) < 0.5)
+    dele = ev & ~ins
+    ln = rng.geometric(1.0 / indel_mean, size=(B, M))
+    diff = np.zeros((B, M + 1), dtype=np.int32)
+    rb, rc = np.nonzero(dele)
+    np.add.at(diff, (rb, rc), 1)
+    np.add.at(diff, (rb, np.minimum(rc + ln[rb, rc], M)), -1)
+    covered = np.cumsum(diff[:, :M], axis=1) > 0
+    n_ins = np.where(ins & ~covered, ln, 0)
+    emit = n_ins + (~covered).astype(np.int64)
+    cs = np.cumsum(emit, axis=1)
+    total = cs[:, -1]
+    if (total < length).any():  # pathological deletions: fall back to the source
+        short = total < length
+        emit[short] = 1
+        n_ins[short] = 0
+        cs = np.cumsum(emit, axis=1)
+    big = int(cs[:, -1].max()) + 1
+    flat = (cs + (np.arange(B) * big)[:, None]).ravel()
+    o = (np.arange(length)[None, :] + (np.arange(B) * big)[:, None]).ravel()
+    j = np.searchsorted(flat, o, side="right").reshape(B, length) - np.arange(B)[:, None] * M
+    j = np.minimum(j, M - 1)
+    before = np.take_along_axis(cs, j, axis=1) - np.take_along_axis(emit, j, axis=1)
+    rank = np.arange(length)[None, :] - before   # rank within position j's emission
+    is_ins = rank < np.take_along_axis(n_ins, j, axis=1)
+    r = np.take_along_axis(src, j, axis=1)
+    r = np.where(is_ins, ACGT[rng.integers(0, 4, size=(B, length))], r)
+    m = rng.random((B, length)) < sub
+    idx = np.searchsorted(ACGT, r)
+    valid = (idx < 4) & (ACGT[np.minimum(idx, 3)] == r)
+    newb = ACGT[(np.where(valid, idx, 0) + rng.integers(1, 4, size=(B, length))) % 4]
+    return np.where(m & valid, newb, r)
+
+
 def make_reads_fixed(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, indel=0.005, indel_mean=2.0,
                      rev_frac=0.5, decoy_frac=0.05, batch=65536, first: int = 0) -> SeqSet:
     """Vectorised fixed-length version of :func:`make_reads` (same error model:
@@ -224,42 +269,7 @@ def make_reads_fixed(rng, target: SeqSet, n_reads: int, length=150, sub=0.02, in
     for k in range(k0, (first + n_reads + batch - 1) // batch):
         rng = np.random.Generator(base_bg.jumped(k + 1))
         B = batch  # every batch draws `batch` reads: any range is a slice of the same sequence
-        c = ok[rng.choice(len(ok), size=B, p=w)]
-        start = target.offsets[c] + (rng.random(B) * (tl[c] - M + 1)).astype(np.int64)
-        src = target.bases[start[:, None] + np.arange(M)[None, :]]
-        ev = rng.random((B, M)) < indel
-        ins = ev & (rng.random((B, M)) < 0.5)
-        dele = ev & ~ins
-        ln = rng.geometric(1.0 / indel_mean, size=(B, M))
-        diff = np.zeros((B, M + 1), dtype=np.int32)
-        rb, rc = np.nonzero(dele)
-        np.add.at(diff, (rb, rc), 1)
-        np.add.at(diff, (rb, np.minimum(rc + ln[rb, rc], M)), -1)
-        covered = np.cumsum(diff[:, :M], axis=1) > 0
-        n_ins = np.where(ins & ~covered, ln, 0)
-        emit = n_ins + (~covered).astype(np.int64)
-        cs = np.cumsum(emit, axis=1)
-        total = cs[:, -1]
-        if (total < length).any():  # pathological deletions: fall back to the source
-            short = total < length
-            emit[short] = 1
-            n_ins[short] = 0
-            cs = np.cumsum(emit, axis=1)
-        big = int(cs[:, -1].max()) + 1
-        flat = (cs + (np.arange(B) * big)[:, None]).ravel()
-        o = (np.arange(length)[None, :] + (np.arange(B) * big)[:, None]).ravel()
-        j = np.searchsorted(flat, o, side="right").reshape(B, length) - np.arange(B)[:, None] * M
-        j = np.minimum(j, M - 1)
-        before = np.take_along_axis(cs, j, axis=1) - np.take_along_axis(emit, j, axis=1)
-        rank = np.arange(length)[None, :] - before   # rank within position j's emission
-        is_ins = rank < np.take_along_axis(n_ins, j, axis=1)
-        r = np.take_along_axis(src, j, axis=1)
-        r = np.where(is_ins, ACGT[rng.integers(0, 4, size=(B, length))], r)
-        m = rng.random((B, length)) < sub
-        idx = np.searchsorted(ACGT, r)
-        valid = (idx < 4) & (ACGT[np.minimum(idx, 3)] == r)
-        newb = ACGT[(np.where(valid, idx, 0) + rng.integers(1, 4, size=(B, length))) % 4]
-        r = np.where(m & valid, newb, r)
+        r = _mutated_batch(rng, target, B, length, M, sub, indel, indel_mean, ok, w)
         rev = rng.random(B) < rev_frac
         r[rev] = _COMP[r[rev, ::-1]]
         dec = rng.random(B) < decoy_frac
@@ -320,6 +330,23 @@ def served_requests(rng, n_requests: int, pool: SeqSet, count_range=(1, 10_000))
         out.append((at, at + int(c)))
         at += int(c)
     return out
+
+
+def medium_target(seed: int = 0xC1A57, scale: float = 1.0) -> SeqSet:
+    """The target of the ``medium`` (and ``uneven``) workload alone."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return make_target(rng, int(100_000_000 * scale), n_contigs=max(1, int(200 * min(1.0, scale * 10))),
+                       median=300_000 * scale, repeat_frac=0.10, n_families=max(1, int(500 * scale)))
+
+
+def uneven_chunk(seed: int, k: int, n: int, scale: float = 1.0):
+    """Chunk k of a chunked uneven read set (reads of 50 bp - 10 kbp, per-read
+    error 1-12 %, as ``uneven``) on the medium target, from its own stream, so
+    that chunks can be made in parallel processes.  Returns (bases, lengths)."""
+    t = medium_target(seed, scale)
+    rng = np.random.Generator(np.random.PCG64([seed, 7, k]))
+    q = make_reads(rng, t, n, log_uniform=(50, 10_000), err_range=(0.01, 0.12), decoy_frac=0.0)
+    return q.bases, np.diff(q.offsets)
 
 
 def workload(name: str, seed: int = 0xC1A57, scale: float = 1.0, n_reads: int | None = None, first: int = 0):
