@@ -57,9 +57,8 @@ namespace {
 // window whose padded bases are already in ix->bases.
 // *failed (zeroed by the caller, read once all windows are queued) counts
 // table records that fell outside the table.
-void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix, unsigned long long* failed) {
-  cudaStream_t st = c->st;
-  Workspace& ws = c->ws;
+void build_index_device(Workspace& ws, cudaStream_t st, const clast_params* p, clast_index* ix,
+                        unsigned long long* failed) {
   const int l = p->lmer;
   const int64_t n = ix->n;
   const char* bases = ix->bases.p + kPad;
@@ -147,9 +146,9 @@ void build_index_device(clast_ctx* c, const clast_params* p, clast_index* ix, un
 }
 
 // Index of a window whose padded base array is already on the device.
-clast_index* make_index_resident(clast_ctx* c, const clast_params* p, DevArray<char>&& padded, int64_t n_bases,
-                                 DevArray<int32_t>&& gateway, DevArray<int32_t>&& lengths, int32_t n_seqs,
-                                 int32_t t_begin, unsigned long long* failed) {
+clast_index* make_index_resident(Workspace& ws, cudaStream_t st, const clast_params* p, DevArray<char>&& padded,
+                                 int64_t n_bases, DevArray<int32_t>&& gateway, DevArray<int32_t>&& lengths,
+                                 int32_t n_seqs, int32_t t_begin, unsigned long long* failed) {
   std::unique_ptr<clast_index> ix(new clast_index());
   ix->l = p->lmer;
   ix->stride = p->stride;
@@ -160,7 +159,7 @@ clast_index* make_index_resident(clast_ctx* c, const clast_params* p, DevArray<c
   ix->bases = std::move(padded);
   ix->gateway = std::move(gateway);
   ix->lengths = std::move(lengths);
-  build_index_device(c, p, ix.get(), failed);
+  build_index_device(ws, st, p, ix.get(), failed);
   return ix.release();
 }
 
@@ -183,7 +182,8 @@ clast_index* make_index(clast_ctx* c, const clast_params* p, const char* bases, 
   const int64_t k0 = g_kernel_launches;
   unsigned long long* failed = reinterpret_cast<unsigned long long*>(c->ws.get<int64_t>("ix_failed", 1));
   CLAST_CK(cudaMemsetAsync(failed, 0, sizeof(unsigned long long), c->st));
-  std::unique_ptr<clast_index> ix(make_index_resident(c, p, std::move(padded), n_bases, std::move(gw), std::move(ln),
+  std::unique_ptr<clast_index> ix(make_index_resident(c->ws, c->st, p, std::move(padded), n_bases, std::move(gw),
+                                                      std::move(ln),
                                                       n_seqs, t_begin, failed));
   CLAST_CK(cudaEventRecord(c->ev2, c->st));
   CLAST_CK(cudaEventSynchronize(c->ev2));
@@ -568,6 +568,8 @@ int clast_ctx_create(int device, clast_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess) return CLAST_ERR_CUDA;
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
   if (cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
+  for (int b = 0; b < kBuildStreams; ++b)
+    if (cudaStreamCreateWithFlags(&c->st_build[b], cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
   {  // keep freed pool memory for reuse by later calls of this process
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -593,7 +595,10 @@ void clast_ctx_destroy(clast_ctx* ctx) {
     a->dev.load_offsets.release();
   }
   if (ctx->st) cudaStreamSynchronize(ctx->st);
+  for (int b = 0; b < kBuildStreams; ++b)
+    if (ctx->st_build[b]) cudaStreamSynchronize(ctx->st_build[b]);
   ctx->ws.release_all();
+  for (auto& w : ctx->ws_build) w.release_all();
   for (auto& a : ctx->arenas)
     if (a->p) cudaFreeHost(a->p);
   for (auto& a : ctx->tsv_arenas)
@@ -608,6 +613,8 @@ void clast_ctx_destroy(clast_ctx* ctx) {
     cudaStreamSynchronize(ctx->st_copy);
     cudaStreamDestroy(ctx->st_copy);
   }
+  for (int b = 0; b < kBuildStreams; ++b)
+    if (ctx->st_build[b]) cudaStreamDestroy(ctx->st_build[b]);
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
 }
@@ -796,7 +803,18 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
       CLAST_CK(cudaMemcpyAsync(all_ln.p, ln.data(), ln.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
       CLAST_CK(cudaMemcpyAsync(all_so.p, so.data(), so.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
     }
-    for (const Plan& w : plan) {
+    // Windows are built alternately on the context's build streams, each with
+    // its own scratch, so that two builds run at once (a build is a chain of
+    // small, latency-bound kernels); every build stream starts after the plan's
+    // upload above and the compute stream waits for all of them at the end.
+    cudaEvent_t planned = ctx->timer.take();
+    win_ev.push_back(planned);
+    CLAST_CK(cudaEventRecord(planned, st));
+    for (int b = 0; b < kBuildStreams; ++b) CLAST_CK(cudaStreamWaitEvent(ctx->st_build[b], planned, 0));
+    for (size_t wi = 0; wi < plan.size(); ++wi) {
+      const Plan& w = plan[wi];
+      const int b = (int)(wi % kBuildStreams);
+      cudaStream_t bs = ctx->st_build[b];
       if (host_src) {  // the window's records: source bytes up to the end of its last record
         const int64_t last = so[w.meta + w.nseqs - 1] + ln[w.meta + w.nseqs - 1];
         if (last > copied) {
@@ -806,31 +824,48 @@ int clast_targets_create(clast_ctx* ctx, const clast_params* p, int32_t t_vram, 
         }
         win_ev.push_back(ctx->timer.take());
         CLAST_CK(cudaEventRecord(win_ev.back(), cs));
-        CLAST_CK(cudaStreamWaitEvent(st, win_ev.back(), 0));
+        CLAST_CK(cudaStreamWaitEvent(bs, win_ev.back(), 0));
       }
+      g_alloc_stream = bs;
       DevArray<char> padded;
       DevArray<int32_t> dgw, dln;
       padded.alloc((size_t)w.n + 2 * kPad);
       dgw.alloc(w.nseqs);
       dln.alloc(w.nseqs);
-      CLAST_CK(cudaMemcpyAsync(dgw.p, all_gw.p + w.meta, w.nseqs * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
-      CLAST_CK(cudaMemcpyAsync(dln.p, all_ln.p + w.meta, w.nseqs * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
-      CLAST_CK(cudaMemsetAsync(padded.p, 'N', (size_t)w.n + 2 * kPad, st));
-      build_window(src, all_so.p + w.meta, dgw.p, dln.p, w.nseqs, w.n, padded.p + kPad, st);
+      CLAST_CK(cudaMemcpyAsync(dgw.p, all_gw.p + w.meta, w.nseqs * sizeof(int32_t), cudaMemcpyDeviceToDevice, bs));
+      CLAST_CK(cudaMemcpyAsync(dln.p, all_ln.p + w.meta, w.nseqs * sizeof(int32_t), cudaMemcpyDeviceToDevice, bs));
+      CLAST_CK(cudaMemsetAsync(padded.p, 'N', (size_t)w.n + 2 * kPad, bs));
+      build_window(src, all_so.p + w.meta, dgw.p, dln.p, w.nseqs, w.n, padded.p + kPad, bs);
       clast_targets::Win win;
       win.load = w.load;
       win.first = w.first;
-      win.ix.reset(make_index_resident(ctx, p, std::move(padded), w.n, std::move(dgw), std::move(dln), w.nseqs,
-                                       w.first, failed));
+      win.ix.reset(make_index_resident(ctx->ws_build[b], bs, p, std::move(padded), w.n, std::move(dgw),
+                                       std::move(dln), w.nseqs, w.first, failed));
+      g_alloc_stream = st;
+      // the index is used and finally freed in the compute stream's order
+      clast_index& ix = *win.ix;
+      ix.bases.st = ix.gateway.st = ix.lengths.st = ix.filter.st = ix.table.st = ix.entries.st = ix.kept.st = st;
       T->wins.push_back(std::move(win));
+    }
+    // the builds end on build stream 0 (which waits for the others): ev_done
+    // there; the compute stream is not held up (clast_map prepares the query
+    // while the builds run and waits for ev_done before its first search), and
+    // the buffers the builds read are freed on build stream 0 after them
+    cudaStream_t b0 = ctx->st_build[0];
+    for (int b = 1; b < kBuildStreams; ++b) {
+      win_ev.push_back(ctx->timer.take());
+      CLAST_CK(cudaEventRecord(win_ev.back(), ctx->st_build[b]));
+      CLAST_CK(cudaStreamWaitEvent(b0, win_ev.back(), 0));
     }
     if (host_src) {
       if (tbytes > copied)
         CLAST_CK(cudaMemcpyAsync(traw.p + copied, hsrc + copied, (size_t)(tbytes - copied), cudaMemcpyHostToDevice,
                                  cs));
       CLAST_CK(cudaEventRecord(T->ev_up, cs));
+      CLAST_CK(cudaStreamWaitEvent(b0, T->ev_up, 0));  // the whole upload is done before traw goes
     }
-    CLAST_CK(cudaEventRecord(T->ev_done, st));
+    CLAST_CK(cudaEventRecord(T->ev_done, b0));
+    traw.st = all_gw.st = all_ln.st = all_so.st = b0;
     T->launches = g_kernel_launches - k0;
     // a host source must stay readable until its copy has been made
     if (host_src) CLAST_CK(cudaEventSynchronize(T->ev_up));
@@ -949,6 +984,7 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     S.query_bases = qb.n;
     // the index builds of clast_targets_create end before the first search
     settle_targets(ctx, T);
+    CLAST_CK(cudaStreamWaitEvent(st, T->ev_done, 0));
     // every target window, in holder order (target load, window)
     std::vector<DevHits> per_win(T->wins.size());
     // seeding several windows per pass over the query (CLAST_SEED_WINDOWS, 1..4)

@@ -162,6 +162,7 @@ struct DpChoice {
   int chunk = 1;
 };
 constexpr int64_t kDpTuneHits = 1 << 16;
+constexpr int kBuildStreams = 2;  // target windows indexed at once by clast_targets_create
 
 }  // namespace clast
 
@@ -173,7 +174,9 @@ struct clast_ctx {
   std::vector<std::unique_ptr<PinnedArena>> tsv_arenas;  // clast_format_tsv texts
   int device = 0;
   cudaStream_t st = nullptr;
-  cudaStream_t st_copy = nullptr;  // query uploads, overlapping index builds still running on st
+  cudaStream_t st_copy = nullptr;  // query uploads, overlapping index builds still running
+  cudaStream_t st_build[clast::kBuildStreams] = {};  // index builds of clast_targets_create
+  Workspace ws_build[clast::kBuildStreams];          // their scratch
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
   Workspace ws;
   std::string err;
