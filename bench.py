@@ -550,11 +550,12 @@ def run_ours(args):
         c1 = time.perf_counter()
         res = eng.map(s, T, qb, q.offsets, q_loads, int(Q_VRAM))
         c2 = time.perf_counter()
-        if tsv:  # the result text, written to a file
-            n = eng.format_tsv(T, res, qlab, tlab, out=tsv_path)
+        if tsv:  # the result text, written to a file while the next step runs (streamed)
+            text = eng.format_tsv_text(T, res, qlab, tlab)
             c2b = time.perf_counter()
-            host["write"].append((c2b - c2) * 1e3)
-            res.tsv_bytes = n
+            host["tsv"].append((c2b - c2) * 1e3)
+            res.tsv_bytes = text.n_bytes
+            writer.submit(text)
         T.close()
         c3 = time.perf_counter()
         host["targets"].append((c1 - c0) * 1e3)
@@ -566,6 +567,44 @@ def run_ours(args):
         host["map_device"].append(sm["map_ms"] + sm["map_upload_ms"])
         return res
 
+    class Writer:
+        """Writes each step's text to the file on a thread of its own, one
+        text at a time; the text's buffer is released once written."""
+
+        def __init__(self):
+            import queue
+            self.q = queue.Queue(maxsize=1)  # at most one text waiting: the next step blocks behind a slow disk
+            self.th = threading.Thread(target=self.run, daemon=True)
+            self.th.start()
+            self.err = None
+
+        def run(self):
+            while True:
+                text = self.q.get()
+                if text is None:
+                    return
+                try:
+                    w0 = time.perf_counter()
+                    text.write(tsv_path)
+                    host["write"].append((time.perf_counter() - w0) * 1e3)
+                except Exception as e:  # reported below
+                    self.err = e
+                finally:
+                    text.release()
+                    self.q.task_done()
+
+        def submit(self, text):
+            self.q.put(text)
+
+        def drain(self):
+            self.q.join()
+
+        def close(self):
+            self.q.put(None)
+            self.th.join()
+
+    writer = Writer()
+
     def timed(tb, qb, tsv=False, steps=None, warmup=None):
         steps = args.steps if steps is None else steps
         warmup = args.warmup if warmup is None else warmup
@@ -575,6 +614,8 @@ def run_ours(args):
         for _ in range(warmup):
             res = step(tb, qb, tsv)
         del res
+        if tsv:
+            writer.drain()
         for v in host.values():
             v.clear()
         if world > 1:
@@ -587,6 +628,8 @@ def run_ours(args):
             res = step(tb, qb, tsv)
             st = eng.stats()
             launches += st["index_launches"] + st["map_launches"]
+        if tsv:
+            writer.drain()  # the last text is on disk before the clock stops
         e1.record()
         torch.cuda.synchronize()
         if world > 1:
@@ -702,7 +745,8 @@ def run_ours(args):
         out["sharded"] = merged
     if tsv:
         out["e2e_tsv"] = dict(tsv, value=round(mbp_all / (tsv["ms_per_step"] / 1e3), 2), unit="Mbp/s",
-                              what="targets + map from pinned host records, clast_format_tsv, file write")
+                              what="targets + map from pinned host records, clast_format_tsv (GPU), the file written by a writer "
+                 "thread while the next step runs; the clock stops after the last write")
     if rank == 0 and world == 1 and not args.no_plain:
         plain = PlainDropIn(eng, s, t, q, t_loads, q_loads)
         pr = plain.step()  # warm-up, and the check against the map
@@ -780,6 +824,10 @@ def run_ours(args):
             out["cpu_baseline_reference"] = {"error": str(e)[:300]}
     if rank == 0:
         print(json.dumps(out), flush=True)
+    writer.close()
+    if writer.err is not None:
+        out_err = str(writer.err)[:300]
+        print(json.dumps({"tsv_write_error": out_err}), file=sys.stderr)
     try:
         os.remove(tsv_path)
     except OSError:

@@ -244,6 +244,29 @@ def _write_parallel(path, mv, threads: int = 4, min_piece: int = 8 << 20):
         os.close(fd)
 
 
+class TsvText:
+    """A result text held in the library's pinned buffer (clast_format_tsv)."""
+
+    def __init__(self, engine, t, n_loads):
+        self._lib = engine._lib
+        self.t = t
+        n = int(t.n_bytes)
+        self.n_bytes = n
+        self.view = memoryview((C.c_char * max(n, 1)).from_address(t.text))[:n]
+        self.load_offsets = np.ctypeslib.as_array(t.load_offsets, shape=(n_loads + 1,)).copy()
+
+    def write(self, path, threads: int = 4):
+        _write_parallel(path, self.view, threads)
+
+    def release(self):
+        if self.t is not None:
+            self.view = None
+            self._lib.clast_tsv_free(C.byref(self.t))
+            self.t = None
+
+    __del__ = release
+
+
 class MapResult(dict):
     """Fields of a clast_map result (numpy views of the library's pinned
     arrays); ``owner`` keeps the library result alive."""
@@ -448,6 +471,26 @@ class Engine:
         out = _map_result_arrays(self, r, len(ls))
         self.last_map_py_ms = ((t1 - t0) * 1e3, (t2 - t1) * 1e3, (time.perf_counter() - t2) * 1e3)
         return out
+
+    def format_tsv_text(self, targets: Targets, result: dict, read_labels, target_labels, start_idx=None,
+                        num_out: int = -1) -> "TsvText":
+        """clast_format_tsv, keeping the library's text buffer: a TsvText whose
+        ``view`` is the text (valid until ``release()``), so that it can be
+        written while the next map runs."""
+        rl = read_labels if isinstance(read_labels, tuple) else flat_labels(read_labels)
+        tl = target_labels if isinstance(target_labels, tuple) else flat_labels(target_labels)
+        roff = np.ascontiguousarray(rl[1], dtype=np.int64)
+        toff = np.ascontiguousarray(tl[1], dtype=np.int64)
+        rlab = N.clast_labels(len(roff) - 1, C.cast(C.c_char_p(rl[0]), C.c_void_p),
+                              roff.ctypes.data_as(C.POINTER(C.c_int64)))
+        tlab = N.clast_labels(len(toff) - 1, C.cast(C.c_char_p(tl[0]), C.c_void_p),
+                              toff.ctypes.data_as(C.POINTER(C.c_int64)))
+        si = None if start_idx is None else np.ascontiguousarray(start_idx, dtype=np.int32)
+        t = N.clast_tsv()
+        self._check(self._lib.clast_format_tsv(self.ctx, targets.handle, C.byref(result.owner.r), result.n_loads,
+                                               C.byref(rlab), C.byref(tlab), None if si is None else si.ctypes.data,
+                                               int(num_out), C.byref(t)))
+        return TsvText(self, t, result.n_loads)
 
     def format_tsv(self, targets: Targets, result: dict, read_labels, target_labels, start_idx=None,
                    num_out: int = -1, out=None):

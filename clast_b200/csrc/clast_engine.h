@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <cstdint>
 #include <map>
@@ -140,7 +141,7 @@ struct StageTimer {
 struct PinnedArena {
   void* p = nullptr;
   size_t bytes = 0;
-  bool in_use = false;
+  std::atomic<bool> in_use{false};  // released by the result's owner, possibly on another thread
   // The result's arrays on the device, kept until the arena is reused (so the
   // text of a result can be formatted on the GPU): read strand t_load t_seq
   // t_idx q_idx t_len q_len match score, evalue, and the per-load offsets.
