@@ -357,6 +357,7 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
   int64_t* hoff = ws.get<int64_t>("s_hoff", ns + 1);
   scan_i32(ws, hcnt, ns, hoff, st);
   const int64_t H = read_scalar(hoff + ns, st);
+  if (H >= ((int64_t)1 << 32)) throw std::invalid_argument("more than 2^32 hits in one window");  // DP order words
   c->stats.hits += H;
   if (H == 0) {
     add_counters();
@@ -912,6 +913,7 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     S.map_launches = S.query_bases = S.query_kmers = S.seeds = S.hits = S.results = S.dp_cells = 0;
     ctx->timer.reset();
     const int64_t nreads = reads->n_seqs;
+    if (nreads >= ((int64_t)1 << 30)) throw std::invalid_argument("at most 2^30 reads per map (2^31 strands)");
     const int64_t nb = reads->offsets[nreads] - reads->offsets[0];
     // The reads' bases go up first, on the copy stream (allocated there, so
     // nothing waits for the compute stream, which may still be building the

@@ -70,6 +70,42 @@ def test_uneven_read_lengths(eng):
     ix.close()
 
 
+def test_overlapping_calls_are_rejected_not_raced(eng):
+    # two contexts on one device in two threads: the shared scratch admits one
+    # call at a time; every call either returns clast_search's hits or is
+    # rejected as overlapping, and a later call succeeds
+    import threading
+    s, tl, ql = make_case(8, target_bp=150_000, n_contigs=4, n_reads=400)
+    ix = eng.hash_table(s, tl, 0, len(tl.lengths))
+    nq = len(ql.lengths) // 2
+    want = eng.hit_list(s, ix, ql, 0, nq)
+    other = api.Engine(0)
+    ix2 = other.hash_table(s, tl, 0, len(tl.lengths))
+    outcomes, barrier = [], threading.Barrier(2)
+
+    def worker(e, x):
+        barrier.wait()
+        for _ in range(6):
+            try:
+                got = e.hit_list_noalloc(s, x, ql, 0, nq, capacity=len(want["t_id"]))
+                same(got, want)
+                outcomes.append("ok")
+            except api.ClastError as err:
+                assert err.code == -1 and "scratch" in str(err), str(err)
+                outcomes.append("busy")
+
+    ts = [threading.Thread(target=worker, args=(eng, ix)), threading.Thread(target=worker, args=(other, ix2))]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert len(outcomes) == 12 and "ok" in outcomes
+    same(eng.hit_list_noalloc(s, ix, ql, 0, nq, capacity=len(want["t_id"])), want)
+    ix2.close()
+    other.close()
+    ix.close()
+
+
 def test_capacity_too_small_reports_count(eng):
     s, tl, ql = make_case(8)
     ix = eng.hash_table(s, tl, 0, len(tl.lengths))
