@@ -643,6 +643,7 @@ def run_ours(args):
         hw = {k: [round(statistics.median(v), 3), round(max(v), 3)] for k, v in host.items() if v}
         hw["fields"] = ("[median, max] ms per step; ctypes = the clast_map call, inside = measured in clast_map, "
                         "map_device = CUDA-event time of the map's uploads and stages")
+        hw["map_per_step"] = [round(x, 1) for x in host["map"]]
         return ms, launches, res, st, hw
 
     with ClockSampler(local) as clk:

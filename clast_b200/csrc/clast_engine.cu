@@ -285,7 +285,13 @@ void seed_windows(clast_ctx* c, const clast_params* p, const QueryBatch& qb, std
                        z.nvalid, z.skey, z.sq, z.part_cap};
     }
     tm.begin(st);
-    seed_multi(q, W, (int)todo.size(), p->gap, p->local, st);
+    if (todo.size() == 1) {  // one window: the single-window kernel (round 0 staged while its range is reserved)
+      const SeedWin& w = W.w[0];
+      seed_fused(q, w.ix, w.t, p->gap, p->local, w.cursor, w.n_kmers, w.off, w.cnt, w.nvalid, w.skey, w.sq,
+                 w.part_cap, st);
+    } else {
+      seed_multi(q, W, (int)todo.size(), p->gap, p->local, st);
+    }
     tm.end(StageTimer::SEED, st);
     std::vector<unsigned long long> cur(todo.size() * 2 * parts);
     for (size_t j = 0; j < todo.size(); ++j)
@@ -989,8 +995,9 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     CLAST_CK(cudaStreamWaitEvent(st, T->ev_done, 0));
     // every target window, in holder order (target load, window)
     std::vector<DevHits> per_win(T->wins.size());
-    // seeding several windows per pass over the query (CLAST_SEED_WINDOWS, 1..4)
-    int group = 2;
+    // windows seeded per pass over the query (CLAST_SEED_WINDOWS, 1..4; one
+    // by default: the several-window pass measured slower on the medium job)
+    int group = 1;
     if (const char* e = std::getenv("CLAST_SEED_WINDOWS")) group = std::max(1, std::min(kMaxSeedWins, std::atoi(e)));
     for (size_t g0 = 0; g0 < T->wins.size(); g0 += (size_t)group) {
       std::vector<SeedSet> sets;

@@ -101,14 +101,26 @@ struct TsvArgs {
   int32_t num_out;
 };
 
-__host__ __device__ __forceinline__ int put_u(char* o, uint64_t v) {
-  char b[20];
-  int k = 0;
-  do {
-    b[k++] = (char)('0' + v % 10);
+// Decimal digits of v.
+__host__ __device__ __forceinline__ int len_u(uint64_t v) {
+  int k = 1;
+  while (v >= 10) {
     v /= 10;
-  } while (v);
-  for (int i = 0; i < k; ++i) o[i] = b[k - 1 - i];
+    ++k;
+  }
+  return k;
+}
+// Writes the `cnt` low decimal digits of v (zero-padded) at o, straight into
+// the output (no local buffer).
+__host__ __device__ __forceinline__ void put_digits(char* o, uint64_t v, int cnt) {
+  for (int i = cnt - 1; i >= 0; --i) {
+    o[i] = (char)('0' + v % 10);
+    v /= 10;
+  }
+}
+__host__ __device__ __forceinline__ int put_u(char* o, uint64_t v) {
+  const int k = len_u(v);
+  put_digits(o, v, k);
   return k;
 }
 __host__ __device__ __forceinline__ int put_i(char* o, int64_t v) {
@@ -118,13 +130,10 @@ __host__ __device__ __forceinline__ int put_i(char* o, int64_t v) {
   }
   return put_u(o, (uint64_t)v);
 }
-__host__ __device__ __forceinline__ int len_u(uint64_t v) {
-  int k = 1;
-  while (v >= 10) {
-    v /= 10;
-    ++k;
-  }
-  return k;
+__host__ __device__ __forceinline__ uint64_t ipow10(int k) {
+  uint64_t x = 1;
+  for (int i = 0; i < k; ++i) x *= 10;
+  return x;
 }
 __host__ __device__ __forceinline__ int len_i(int64_t v) { return v < 0 ? 1 + len_u((uint64_t)(-v)) : len_u((uint64_t)v); }
 
@@ -177,20 +186,27 @@ __host__ __device__ bool round6(const double2* p10, double v, int e, int64_t& n)
   return true;
 }
 
-// %g with precision 6 (the default of std::ostream).  Returns the length
-// written (o may be null: length only), or -1 when the host must format v.
+// %g with precision 6 (the default of std::ostream).  Returns the length,
+// writing the text at o unless o is null (length only), or -1 when the host
+// must format v.  Digits go straight into o: no local buffers.
 __host__ __device__ int fmt_g6(const double2* p10, double v, char* o) {
   if (!isfinite(v)) return -1;
-  char tmp[32];
-  char* w = o ? o : tmp;
   int len = 0;
+  auto put = [&](char c) {
+    if (o) o[len] = c;
+    ++len;
+  };
+  auto digits = [&](uint64_t x, int cnt) {
+    if (o) put_digits(o + len, x, cnt);
+    len += cnt;
+  };
   if (v == 0.0) {
-    if (signbit(v)) w[len++] = '-';
-    w[len++] = '0';
+    if (signbit(v)) put('-');
+    put('0');
     return len;
   }
   if (v < 0) {
-    w[len++] = '-';
+    put('-');
     v = -v;
   }
   int e = (int)floor(log10(v));
@@ -205,35 +221,38 @@ __host__ __device__ int fmt_g6(const double2* p10, double v, char* o) {
     break;
   }
   if (!ok) return -1;
-  char d[6];
-  for (int i = 5; i >= 0; --i) {
-    d[i] = (char)('0' + n % 10);
-    n /= 10;
+  // the 6 significant digits without their trailing zeros: m, nd digits
+  uint64_t m = (uint64_t)n;
+  int nd = 6;
+  while (nd > 1 && m % 10 == 0) {
+    m /= 10;
+    --nd;
   }
-  int nd = 6;  // significant digits kept: trailing zeros go
-  while (nd > 1 && d[nd - 1] == '0') --nd;
   if (e < -4 || e >= 6) {
-    w[len++] = d[0];
+    const uint64_t rest = ipow10(nd - 1);
+    digits(m / rest, 1);
     if (nd > 1) {
-      w[len++] = '.';
-      for (int i = 1; i < nd; ++i) w[len++] = d[i];
+      put('.');
+      digits(m % rest, nd - 1);
     }
-    w[len++] = 'e';
-    w[len++] = e < 0 ? '-' : '+';
+    put('e');
+    put(e < 0 ? '-' : '+');
     const int ae = e < 0 ? -e : e;
-    if (ae < 10) w[len++] = '0';
-    len += put_u(w + len, (uint64_t)ae);
+    digits((uint64_t)ae, ae < 100 ? 2 : 3);
   } else if (e >= 0) {
-    for (int i = 0; i <= e; ++i) w[len++] = d[i];
-    if (nd > e + 1) {
-      w[len++] = '.';
-      for (int i = e + 1; i < nd; ++i) w[len++] = d[i];
+    if (nd <= e + 1) {
+      digits(m * ipow10(e + 1 - nd), e + 1);
+    } else {
+      const uint64_t frac = ipow10(nd - e - 1);
+      digits(m / frac, e + 1);
+      put('.');
+      digits(m % frac, nd - e - 1);
     }
   } else {
-    w[len++] = '0';
-    w[len++] = '.';
-    for (int i = 0; i < -e - 1; ++i) w[len++] = '0';
-    for (int i = 0; i < nd; ++i) w[len++] = d[i];
+    put('0');
+    put('.');
+    for (int i = 0; i < -e - 1; ++i) put('0');
+    digits(m, nd);
   }
   return len;
 }
@@ -256,9 +275,8 @@ __device__ int tsv_line(const TsvArgs& a, int64_t i, int64_t trec, char* o) {
   const int64_t ql = a.q_off[r + 1] - a.q_off[r], tl = a.t_off[trec + 1] - a.t_off[trec];
   const int tidx = a.t_idx[i] + (a.t_start ? a.t_start[trec] : 0);
   const double pct = (double)(a.match[i] * 100) / (double)a.q_len[i];
-  char pbuf[32], ebuf[32];
-  const int lp = fmt_g6(g_pow10, pct, pbuf);
-  const int le = fmt_g6(g_pow10, a.evalue[i], ebuf);
+  const int lp = fmt_g6(g_pow10, pct, nullptr);
+  const int le = fmt_g6(g_pow10, a.evalue[i], nullptr);
   if (lp < 0 || le < 0) return -1;
   if (!o) {
     return (int)ql + (int)tl + 9 + len_i(a.q_idx[i]) + len_i(a.q_len[i]) + 1 + len_i(tidx) + len_i(a.t_len[i]) +
@@ -281,13 +299,13 @@ __device__ int tsv_line(const TsvArgs& a, int64_t i, int64_t trec, char* o) {
   o[k++] = '\t';
   k += put_i(o + k, a.match[i]);
   o[k++] = '(';
-  for (int j = 0; j < lp; ++j) o[k++] = pbuf[j];
+  k += fmt_g6(g_pow10, pct, o + k);
   o[k++] = '%';
   o[k++] = ')';
   o[k++] = '\t';
   k += put_i(o + k, a.score[i]);
   o[k++] = '\t';
-  for (int j = 0; j < le; ++j) o[k++] = ebuf[j];
+  k += fmt_g6(g_pow10, a.evalue[i], o + k);
   o[k++] = '\n';
   return k;
 }
@@ -587,6 +605,42 @@ extern "C" int clast_format_g6_host(const double* v, int64_t n, char* out, int32
     o[L < 0 ? 0 : L] = '\0';
   }
   return CLAST_OK;
+}
+
+namespace {
+__global__ void k_fmt_g6(const double* __restrict__ v, int64_t n, char* __restrict__ out, int32_t* __restrict__ lens) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  char* o = out + 32 * i;
+  const int L = fmt_g6(g_pow10, v[i], o);
+  lens[i] = L;
+  o[L < 0 ? 0 : L] = '\0';
+}
+}  // namespace
+
+// The same formatter run as a kernel on the context's GPU (the path
+// clast_format_tsv takes), for checking the device's digits against the C
+// library's printf: host arrays in and out, as clast_format_g6_host.  Not
+// part of the public interface.
+extern "C" int clast_format_g6_device(clast_ctx* ctx, const double* v, int64_t n, char* out, int32_t* lens) {
+  if (!ctx || !v || !out || !lens || n < 0) return CLAST_ERR_ARG;
+  return guarded(ctx, [&]() -> int {
+    CLAST_CK(cudaSetDevice(ctx->device));
+    ensure_pow10(ctx->device);
+    cudaStream_t st = ctx->st;
+    double* dv = ctx->ws.get<double>("fmt_v", (size_t)n);
+    char* dout = ctx->ws.get<char>("fmt_out", (size_t)n * 32);
+    int32_t* dl = ctx->ws.get<int32_t>("fmt_len", (size_t)n);
+    if (n) {
+      CLAST_CK(cudaMemcpyAsync(dv, v, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st));
+      k_fmt_g6<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dv, n, dout, dl);
+      CLAST_LAUNCHED();
+      CLAST_CK(cudaMemcpyAsync(out, dout, (size_t)n * 32, cudaMemcpyDeviceToHost, st));
+      CLAST_CK(cudaMemcpyAsync(lens, dl, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    }
+    CLAST_CK(cudaStreamSynchronize(st));
+    return CLAST_OK;
+  });
 }
 
 extern "C" void clast_tsv_free(clast_tsv* t) {
