@@ -38,3 +38,28 @@ def test_sharded_map_merges_to_oracle(engine, world):
             np.testing.assert_allclose(merged[f], want[f], rtol=1e-12, atol=0)
         else:
             np.testing.assert_array_equal(merged[f], want[f], err_msg=f)
+
+
+@pytest.mark.parametrize("group", ["2", "4"])
+def test_several_windows_per_seeding_pass(engine, group, monkeypatch):
+    # CLAST_SEED_WINDOWS > 1: the seeds of several target windows in one pass
+    # over the query (k_seed_multi); the hits must equal the oracle's
+    rng = np.random.Generator(np.random.PCG64(405))
+    t = synth.make_target(rng, 300_000, n_contigs=7, median=40_000, repeat_frac=0.05, n_families=5)
+    q = synth.make_reads(rng, t, 700, log_uniform=(60, 800))
+    s = api.Setting(total_db=float(t.offsets[-1]))
+    q_loads, q_vram, t_vram = [700], 30_000, 45_000  # five or more target windows
+    monkeypatch.setenv("CLAST_SEED_WINDOWS", group)
+    T = engine.targets(s, t.bases, t.offsets, [len(t)], t_vram)
+    res = engine.map(s, T, q.bases, q.offsets, q_loads, q_vram)
+    got = {f: np.array(res[f]) for f in list(api.MAP_FIELDS) + ["load_offsets"]}
+    del res
+    T.close()
+    want = oracle_map(s, [t.seq(i).tobytes() for i in range(len(t))], [len(t)], t_vram,
+                      [q.seq(i).tobytes() for i in range(len(q))], q_loads, q_vram)
+    assert len(want["read"]) > 200
+    for f in api.MAP_FIELDS:
+        if f == "evalue":
+            np.testing.assert_allclose(got[f], want[f], rtol=1e-12, atol=0)
+        else:
+            np.testing.assert_array_equal(got[f], want[f], err_msg=f)
