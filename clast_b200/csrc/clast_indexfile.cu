@@ -152,10 +152,6 @@ void read_window(FILE* f, const FileHeader& h, HostWindow& w) {
     if (g < prev_end || len < 0 || g + len + (h.l - 1) > w.n) bad("sequence " + std::to_string(i) + " outside the window");
     prev_end = g + len;
   }
-  for (int64_t e = 0; e < n_entries; ++e) {
-    const int2 x = w.entries[e];
-    if (x.x < 0 || x.x >= w.nseqs || x.y < 0 || x.y >= w.lengths[x.x]) bad("entry " + std::to_string(e));
-  }
   // every probe ends at a free record inside the table: the last one is free
   if (w.table.back().y != kNoPayload) bad("last table record in use");
   for (int64_t r = 0; r < w.n_records; ++r) {
@@ -164,6 +160,11 @@ void read_window(FILE* f, const FileHeader& h, HostWindow& w) {
     if (pl & kMulti) {
       const int64_t start = (int64_t)((pl >> 32) & 0x7fffffffu), cnt = (int64_t)(uint32_t)pl;
       if (cnt < 1 || start + cnt > n_entries) bad("record " + std::to_string(r) + " points past the entries");
+      // the entries a record refers to (the array's tail past the kept ones is unused)
+      for (int64_t e = start; e < start + cnt; ++e) {
+        const int2 x = w.entries[e];
+        if (x.x < 0 || x.x >= w.nseqs || x.y < 0 || x.y >= w.lengths[x.x]) bad("entry " + std::to_string(e));
+      }
     } else {
       const int64_t seq = (int64_t)(pl >> 32), idx = (int64_t)(uint32_t)pl;
       if (seq >= w.nseqs || idx >= w.lengths[seq]) bad("record " + std::to_string(r) + " names no target base");

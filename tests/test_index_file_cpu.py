@@ -64,6 +64,17 @@ def test_consistent_file_passes(tmp_path):
     assert ok, why
 
 
+def test_unused_entry_tail_is_not_checked(tmp_path):
+    # the entry array is sized by the samples; entries past the kept ones
+    # hold whatever the build left there and no record refers to them
+    w = window()
+    w["entries"][-5:] = (-7, 10 ** 6)
+    p = tmp_path / "tail.clastix"
+    write(p, w)
+    ok, why = verify(p)
+    assert ok, why
+
+
 @pytest.mark.parametrize("edit,expect", [
     (dict(magic=b"CLASTIX1"), "older index layout"),
     (dict(magic=b"NOTANIDX"), "not a clast index file"),
@@ -100,7 +111,7 @@ def edited(field_fn):
     ("single_seq", lambda w: w["table"].__setitem__(0, (7, (5 << 32) | 1)), "names no target base"),
     ("gateway", lambda w: w["gateway"].__setitem__(1, w["n"] - 10), "outside the window"),
     ("length", lambda w: w["lengths"].__setitem__(0, 10_000), "outside the window"),
-    ("entry", lambda w: w["entries"].__setitem__(3, (0, 999)), "entry 3"),
+    ("entry", lambda w: w["entries"].__setitem__(3, (0, 999)), "entry 3"),  # inside record 2's range 3..6
     ("load", lambda w: w.update(load=1), "target load"),
     ("filter", lambda w: w.update(fshift=40), "filter size"),
 ])
