@@ -1836,7 +1836,7 @@ struct Band {
       B[c] = v + kGapExtend;
       M[c] = m;
       const int64_t ib = ib0 + (int64_t)step * c;
-      tc[c] = ((ib < lo || ib >= hi) ? kBadClass : base_class(tb[tstart + ib])) << 5;
+      tc[c] = ((ib < lo || ib >= hi) ? kBadClass : base_class(tb[tstart + ib])) << 8;  // byte offset of its table row
     }
   }
   // select end node (global mode), krnlAlignment.cu:170-185
@@ -1916,7 +1916,9 @@ __device__ __forceinline__ void banded_hit(const int2* __restrict__ tab, const c
     t_ib += t_step;
     const char q_next = (r + 1 < row_end) ? q_ptr[q_step] : 'N';
     q_ptr += q_step;
-    const int qc = base_class(q_cur);
+    // the query letter's column in every target row: one add per cell finds
+    // the (point + 7, match) pair (byte offsets; no index arithmetic)
+    const char* rowp = reinterpret_cast<const char*>(tab) + (base_class(q_cur) << 3);
     int hA = kMarginA, hB = kMarginB, hM = kMarginScore;  // row 0 of the band (left margin)
 #pragma unroll
     for (int c = 0; c < W; ++c) {
@@ -1925,7 +1927,7 @@ __device__ __forceinline__ void banded_hit(const int2* __restrict__ tab, const c
       const int vM = (c + 1 < W) ? bd.M[(c + 1) % W] : 0;
       const int nV = max(vA, vB);
       const int nH = max(hA, hB);
-      const int2 w = tab[bd.tc[c] | qc];  // (POINT + 7, match increment)
+      const int2 w = *reinterpret_cast<const int2*>(rowp + bd.tc[c]);  // (POINT + 7, match increment)
       const int pt = bd.A[c] + w.x;
       // (plain compares and maxima: fewer instructions than __vibmax_s32 here)
       const bool h_wins = nH >= nV;
@@ -1947,7 +1949,7 @@ __device__ __forceinline__ void banded_hit(const int2* __restrict__ tab, const c
     }
 #pragma unroll
     for (int c = 0; c < W - 1; ++c) bd.tc[c] = bd.tc[c + 1];
-    bd.tc[W - 1] = base_class(t_next) << 5;  // 'X' above is the bad-area letter itself
+    bd.tc[W - 1] = base_class(t_next) << 8;  // 'X' above is the bad-area letter itself
     q_cur = q_next;
     ++qrow;
   }
