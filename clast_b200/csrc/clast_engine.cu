@@ -130,10 +130,11 @@ void build_index_device(Workspace& ws, cudaStream_t st, const clast_params* p, c
   ix->n_records = 2 * nb + (1 << 16);
   ix->table.alloc((size_t)ix->n_records);
   CLAST_CK(cudaMemsetAsync(ix->table.p, 0xff, (size_t)ix->n_records * sizeof(ulonglong2), st));
-  // Bloom filter: about 24 bits per sample, between 2^12 and 2^F bits; F = 28
-  // (32 MB, L2-resident next to the streams that pass through L2 while
-  // seeding) unless CLAST_FILTER_BITS says otherwise (16..32)
-  int fbits = 28;
+  // Bloom filter: about 24 bits per sample, between 2^12 and 2^F bits; F = 27
+  // (16 MB: the filters of the two windows a seeding pass reads stay in L2
+  // beside the streams that pass through it) unless CLAST_FILTER_BITS says
+  // otherwise (16..32)
+  int fbits = 27;
   if (const char* e = std::getenv("CLAST_FILTER_BITS")) fbits = std::max(16, std::min(32, std::atoi(e)));
   int bits = 12;
   while (bits < fbits && (1ll << bits) < ns * 24) ++bits;
@@ -995,9 +996,8 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     CLAST_CK(cudaStreamWaitEvent(st, T->ev_done, 0));
     // every target window, in holder order (target load, window)
     std::vector<DevHits> per_win(T->wins.size());
-    // windows seeded per pass over the query (CLAST_SEED_WINDOWS, 1..4; one
-    // by default: the several-window pass measured slower on the medium job)
-    int group = 1;
+    // windows seeded per pass over the query (CLAST_SEED_WINDOWS, 1..4)
+    int group = 2;
     if (const char* e = std::getenv("CLAST_SEED_WINDOWS")) group = std::max(1, std::min(kMaxSeedWins, std::atoi(e)));
     for (size_t g0 = 0; g0 < T->wins.size(); g0 += (size_t)group) {
       std::vector<SeedSet> sets;

@@ -9,7 +9,7 @@ the host cores), byte-identical TSV.
   full, and the first 250,000 of its reads -- two query RAM loads (32 Mbase
   per load) against both 64 Mbase target windows, at default settings.  At
   this size the index paths that only large windows reach run: the filter
-  at its 2^28-bit cap, the seed partitions sized from the query and rerun
+  at its size cap, the seed partitions sized from the query and rerun
   when one overflows (the first map of a fresh context), and the deferred
   table-overflow check.
 """

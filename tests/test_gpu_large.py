@@ -3,7 +3,7 @@ chromosomes of 125 Mbp from the 3 Gbp shape (45 % repeats in families at
 80-99 % identity, 1 % N blocks) in ONE target window of 250 Mbp
 (-tRAM 260 -tVRAM 260, as that configuration needs), 6,000 reads of 150 bp.
 At this size the index holds 50 M samples: its hash table is past 100 M
-records, the filter is at its 2^28-bit cap with about 5 bits per key, and
+records, the filter is at its size cap with under 3 bits per key, and
 entry offsets and record homes use their full ranges.  The drop-in command
 line on the GPU and the oracle's command line must write the same bytes."""
 import os
