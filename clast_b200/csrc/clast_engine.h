@@ -58,10 +58,17 @@ struct DevArray {
     n = count;
     st = g_alloc_stream;
     if (cudaMallocAsync(reinterpret_cast<void**>(&p), (count ? count : 1) * sizeof(T), st) != cudaSuccess) {
+      // blocks freed on other streams become reusable once their frees have
+      // run: wait for the device, then try once more
       (void)cudaGetLastError();
-      p = nullptr;
-      n = 0;
-      throw std::bad_alloc();
+      cudaDeviceSynchronize();
+      (void)cudaGetLastError();
+      if (cudaMallocAsync(reinterpret_cast<void**>(&p), (count ? count : 1) * sizeof(T), st) != cudaSuccess) {
+        (void)cudaGetLastError();
+        p = nullptr;
+        n = 0;
+        throw std::bad_alloc();
+      }
     }
   }
   void release() {

@@ -98,9 +98,21 @@ struct Workspace {
       b.bytes = 0;
       const size_t nb = bytes + bytes / 4;
       if (cudaMalloc(&b.p, nb) != cudaSuccess) {
+        // memory freed by stream-ordered frees stays cached in the device's
+        // pool for later stream-ordered allocations; hand it back and retry
         (void)cudaGetLastError();
-        b.p = nullptr;
-        throw std::bad_alloc();
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+          cudaDeviceSynchronize();
+          cudaMemPoolTrimTo(pool, 0);
+        }
+        (void)cudaGetLastError();
+        if (cudaMalloc(&b.p, nb) != cudaSuccess) {
+          (void)cudaGetLastError();
+          b.p = nullptr;
+          throw std::bad_alloc();
+        }
       }
       b.bytes = nb;
     }
