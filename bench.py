@@ -657,7 +657,11 @@ def run_ours(args):
         ms_dev, launches, res, st, hw_dev = timed(t_dev, q_dev)
         scores = res["score"].copy()
         del res
+        print("value loop: %.1f ms per step; %s" % (ms_dev / args.steps, {k: st[k] for k in (
+            "seeds", "hits", "results", "dp_cells", "index_ms", "map_ms", "seed_ms", "dp_ms")}), file=sys.stderr,
+            flush=True)
         ms_e2e, _, res2, st2, hw_e2e = timed(t_pin, q_pin)
+        print("e2e loop: %.1f ms per step" % (ms_e2e / args.steps), file=sys.stderr, flush=True)
         assert np.array_equal(scores, res2["score"])
         merged = None
         if shard_info is not None:  # the shards, merged on rank 0 in rank order (untimed)
