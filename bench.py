@@ -797,6 +797,7 @@ def run_ours(args):
             uneven_job[0].terminate()
     if rank == 0 and world == 1 and not args.no_serve:
         try:
+            eng.trim()  # the served lanes get the memory the loops above kept cached
             out["served"] = served_leg(eng, s, t, t_loads, args)
         except Exception as e:  # reported, never fatal
             out["served"] = {"error": str(e)[:300]}
@@ -888,6 +889,7 @@ def main():
         T_VRAM = args.tvram * 1e6 if args.tvram else 260e6
         args.no_plain = True  # per-window rebuilds of 3 Gbp of indexes: minutes per step
         args.no_cpu_baseline = True  # one CPU index build of 3 Gbp is far beyond a bounded sample
+        args.no_tsv = True  # ~640 M result lines (38 GB of text) per step
         if args.check == "load0":
             args.check = "off"  # the large-window parity is a test of its own
     if args.impl == "reference":

@@ -100,6 +100,7 @@ SIGNATURES = {
     "clast_last_map_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "clast_get_stats": (C.c_int, [C.c_void_p, C.POINTER(clast_stats)]),
     "clast_int32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "clast_ctx_trim": (C.c_int, [C.c_void_p]),
     "clast_server_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(clast_params),
                                       C.POINTER(clast_server_config), C.POINTER(C.c_void_p)]),
     "clast_server_submit": (C.c_int, [C.c_void_p, C.POINTER(clast_seqs), C.POINTER(C.c_int64)]),

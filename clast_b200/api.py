@@ -535,6 +535,10 @@ class Engine:
         self._check(self._lib.clast_get_stats(self.ctx, C.byref(st)))
         return {f: getattr(st, f) for f, _ in N.clast_stats._fields_}
 
+    def trim(self) -> None:
+        """clast_ctx_trim: hand back the device memory kept for reuse."""
+        self._check(self._lib.clast_ctx_trim(self.ctx))
+
     def int32_peak(self) -> float:
         """Measured INT32 tera-ops/s of this GPU (clast_int32_peak)."""
         v = C.c_double()

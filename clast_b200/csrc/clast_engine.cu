@@ -1129,6 +1129,27 @@ void clast_map_result_free(clast_map_result* r) {
   std::memset(r, 0, sizeof(*r));
 }
 
+int clast_ctx_trim(clast_ctx* ctx) {
+  if (!ctx) return CLAST_ERR_ARG;
+  return guarded(ctx, [&]() -> int {
+    CLAST_CK(cudaSetDevice(ctx->device));
+    CLAST_CK(cudaDeviceSynchronize());
+    for (auto& a : ctx->arenas)
+      if (!a->in_use) {
+        for (auto& f : a->dev.f) f.release();
+        a->dev.evalue.release();
+        a->dev.load_offsets.release();
+      }
+    ctx->ws.release_all();
+    for (auto& w : ctx->ws_build) w.release_all();
+    CLAST_CK(cudaDeviceSynchronize());
+    cudaMemPool_t pool;
+    CLAST_CK(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+    CLAST_CK(cudaMemPoolTrimTo(pool, 0));
+    return CLAST_OK;
+  });
+}
+
 int clast_int32_peak(clast_ctx* ctx, double* tera_ops) {
   if (!ctx || !tera_ops) return CLAST_ERR_ARG;
   return guarded(ctx, [&]() -> int {

@@ -238,6 +238,12 @@ int clast_format_tsv(clast_ctx* ctx, const clast_targets* t, const clast_map_res
                      int32_t num_out, clast_tsv* out);
 void clast_tsv_free(clast_tsv* t);
 
+/* Hands back the device memory a context keeps for reuse between calls: its
+ * scratch buffers, the device copies of released results, and the blocks
+ * the device's memory pool holds after stream-ordered frees.  Results and
+ * targets still in use are kept.  Waits for the device first. */
+int clast_ctx_trim(clast_ctx* ctx);
+
 /* Device-side timing of the last clast_map call in milliseconds (kernels and
  * copies on the context's stream), and how many kernels it launched. */
 int clast_last_map_stats(const clast_ctx* ctx, double* device_ms, int64_t* kernel_launches);
