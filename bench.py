@@ -415,10 +415,12 @@ def served_leg(eng, s, t, t_loads, args):
     return {
         "peak_mbps": round(peak_bps / 1e6, 1), "levels": levels,
         "p99_ms_at_80pct": next(x["p99_ms"] for x in levels if x["offered_frac"] == 0.8),
-        "config": "medium target resident (100 Mbp, 2 windows); requests of 1-10,000 reads (log-uniform count) of "
+        "config": "%s target resident (%d bp, %d windows); requests of 1-10,000 reads (log-uniform count) of "
                   "100-5,000 bp (log-uniform), 2 %% substitutions, 5 %% decoys, from a pool of %d reads; lanes %d, "
                   "max batch %d bases; peak from a backlog of %d requests; %.0f s per level" % (
-                      args.serve_pool, args.serve_lanes, args.serve_batch, args.serve_backlog, args.serve_seconds),
+                      getattr(args, "workload", "medium"), int(t.offsets[-1]),
+                      len(target_windows(np.diff(t.offsets), t_loads, s.lmer, int(T_VRAM))), args.serve_pool,
+                      args.serve_lanes, args.serve_batch, args.serve_backlog, args.serve_seconds),
         "latency": "request queued -> its hits in host memory (server steady-clock stamps)",
         "max_batch_requests": st["max_batch_requests"]}
 
@@ -589,7 +591,7 @@ def run_ours(args):
                     return
                 try:
                     w0 = time.perf_counter()
-                    text.write(tsv_path)
+                    text.write(tsv_path, threads=8)
                     host["write"].append((time.perf_counter() - w0) * 1e3)
                 except Exception as e:  # reported below
                     self.err = e
