@@ -52,10 +52,10 @@ import numpy as np  # noqa: E402
 from clast_b200 import api, synth  # noqa: E402
 
 METRIC = "query Mbp/s (bit-exact hits)"
-# DRAM bytes (read + write) per looked-up l-mer of k_seed_fused, from an ncu
-# capture of one launch on the half-size medium workload (50 Mbp target
-# window, 500,000 reads)
-SEED_DRAM_BYTES_PER_KMER = 12.2
+# DRAM bytes (read + write) per l-mer looked up in one window by the
+# two-window seeding pass, from an ncu capture of one launch on the half-size
+# medium workload (2 windows of 25 Mbp, 500,000 reads): 1.82 GB / 271 M
+SEED_DRAM_BYTES_PER_KMER = 6.7
 T_RAM, Q_RAM, T_VRAM, Q_VRAM = 64e6, 64e6, 64e6, 2e6  # common.hpp:12-15, x 1e6 (CHostSetting.cu:133-136)
 
 
@@ -710,7 +710,8 @@ def run_ours(args):
     ix_bytes = st["index_bases"] / 4 + 12 * st["index_bases"] / s.stride + 16 * st["index_keys"]
     filt_bytes = 16 * st["seeds"] + 16 * st["hits"]
     roofline = {
-        "kernel": "seeding (k_seed_fused: l-mer keys, filter + table lookups, seed writes)",
+        "kernel": "seeding (k_seed_multi: l-mer keys, filter + table lookups of two target windows per pass, "
+                  "seed writes)",
         "bound": "hbm", "achieved": round(seed_gbs, 1), "peak": hbm_peak, "unit": "GB/s",
         "frac": round(seed_gbs / hbm_peak, 4),
         "peak_source": peak_src,
@@ -718,7 +719,8 @@ def run_ours(args):
         "ms_per_launch": round(st["seed_ms"] / max(1, st["seed_launches"]), 3),
         "launches_per_step": st["seed_launches"], "target_windows": n_twin,
         "traffic": int(SEED_DRAM_BYTES_PER_KMER * st["query_kmers"] / max(1, st["seed_launches"])),
-        "traffic_source": "ncu DRAM bytes per l-mer on the half-size workload x l-mers per launch",
+        "traffic_source": "ncu DRAM bytes per (l-mer, window) on the half-size workload (2 x 25 Mbp windows, "
+                          "500,000 reads) x (l-mer, window) lookups per launch",
         "stage_ms_per_step": {k: round(v, 3) for k, v in stages.items()},
         "step_device_ms": round(st["index_ms"] + st["map_ms"], 3),
         "index_ms": round(st["index_ms"], 3), "map_ms": round(st["map_ms"], 3),

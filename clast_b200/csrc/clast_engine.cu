@@ -286,7 +286,8 @@ void seed_windows(clast_ctx* c, const clast_params* p, const QueryBatch& qb, std
                        z.nvalid, z.skey, z.sq, z.part_cap};
     }
     tm.begin(st);
-    if (todo.size() == 1) {  // one window: the single-window kernel (round 0 staged while its range is reserved)
+    static const bool force_multi = std::getenv("CLAST_SEED_MULTI_ONLY") != nullptr;
+    if (todo.size() == 1 && !force_multi) {  // one window: the single-window kernel (round 0 staged while its range is reserved)
       const SeedWin& w = W.w[0];
       seed_fused(q, w.ix, w.t, p->gap, p->local, w.cursor, w.n_kmers, w.off, w.cnt, w.nvalid, w.skey, w.sq,
                  w.part_cap, st);
