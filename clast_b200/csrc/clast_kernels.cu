@@ -1808,14 +1808,18 @@ __device__ __forceinline__ int2 cell_score(int t, int q) {
 // so the threads of a warp stay converged although each switches from the
 // backward to the forward pass at its own row.
 //
-// Per band column the registers hold S (score), B = V - 2 (vertical state
-// minus gap extend) and M (matches); along a row the chain carries hS and
-// hB = H - 2 of the previous column.  Then, exactly as calcutlateCell
-// (krnlAlignment.cu:42-77):
-//   V = max(Sv - 7, Vv - 2) = max(S_v - 7, B_v)    H = max(Sh - 7, Hh - 2) = max(hS - 7, hB)
-//   pt = S_diag + POINT
+// Per band column the registers hold A = S - 7 (score minus gap open +
+// extend), B = V - 2 (vertical state minus gap extend) and M (matches); along
+// a row the chain carries hA = S - 7 and hB = H - 2 of the previous column.
+// Then, exactly as calcutlateCell (krnlAlignment.cu:42-77):
+//   V = max(Sv - 7, Vv - 2) = max(A_v, B_v)        H = max(Sh - 7, Hh - 2) = max(hA, hB)
+//   pt = S_diag + POINT = A_diag + (POINT + 7)      (the table stores POINT + 7)
 //   H wins over V iff H >= V; the diagonal wins iff pt > max(V, H)
-// (each "max(x - 7, y)" is one fused add-and-max).
+// Storing S itself and folding the "- 7" into a fused add-and-max per
+// maximum takes one add per cell less, but the row's chain through it is
+// slower: a lone thread took 6.8 against 2.7 ms on one 5 kbp hit, with no gain
+// on full batches of 150 bp reads.  A long hit's chain sets the latency of
+// small batches, so the band keeps S - 7.
 template <int GAP>
 struct Band {
   static constexpr int W = 2 * GAP + 1;
@@ -1832,7 +1836,7 @@ struct Band {
       if (r < GAP + 1) { sc = kMarginScore; v = kMarginScore; m = kMarginScore; }
       else if (r == GAP + 1) { sc = 0; v = kGapOpen; m = 0; }
       else { sc = (r - GAP - 1) * kGapExtend + kGapOpen; v = sc + kGapOpen; m = 0; }
-      A[c] = sc;
+      A[c] = sc + kGapOpen + kGapExtend;
       B[c] = v + kGapExtend;
       M[c] = m;
       const int64_t ib = ib0 + (int64_t)step * c;
@@ -1846,7 +1850,7 @@ struct Band {
     ep = -1;
 #pragma unroll
     for (int c = 0; c < W; ++c) {
-      const int sc = A[c];
+      const int sc = A[c] - (kGapOpen + kGapExtend);
       if (best < sc) { best = sc; best_m = M[c]; ep = c; }
     }
   }
@@ -1859,9 +1863,9 @@ __device__ __forceinline__ void banded_hit(const int2* __restrict__ tab, const c
                                            int& o_tidx, int& o_qidx) {
   constexpr int W = Band<GAP>::W;
   constexpr int kGapSO = kGapOpen + kGapExtend;  // -7
-  constexpr int kBotA = (GAP + 1) * kGapExtend + kGapOpen;  // score of the fixed band row 2*GAP+2
+  constexpr int kBotA = (GAP + 1) * kGapExtend + kGapOpen + kGapSO;  // fixed band row 2*GAP+2
   constexpr int kBotB = (GAP + 1) * kGapExtend + kGapOpen + kGapOpen + kGapExtend;
-  constexpr int kMarginA = kMarginScore, kMarginB = kMarginScore + kGapExtend;
+  constexpr int kMarginA = kMarginScore + kGapSO, kMarginB = kMarginScore + kGapExtend;
   constexpr int kNoLow = INT_MIN / 2, kNoHigh = INT_MAX / 2;
   const int rows_b = qlen - (qidx + l);  // alignmentSize of the backward pass
   const int rows_f = qidx;              // rows of the forward pass
@@ -1917,7 +1921,7 @@ __device__ __forceinline__ void banded_hit(const int2* __restrict__ tab, const c
     const char q_next = (r + 1 < row_end) ? q_ptr[q_step] : 'N';
     q_ptr += q_step;
     // the query letter's column in every target row: one add per cell finds
-    // the (point, match) pair (byte offsets; no index arithmetic)
+    // the (point + 7, match) pair (byte offsets; no index arithmetic)
     const char* rowp = reinterpret_cast<const char*>(tab) + (base_class(q_cur) << 3);
     int hA = kMarginA, hB = kMarginB, hM = kMarginScore;  // row 0 of the band (left margin)
 #pragma unroll
@@ -1925,9 +1929,9 @@ __device__ __forceinline__ void banded_hit(const int2* __restrict__ tab, const c
       const int vA = (c + 1 < W) ? bd.A[(c + 1) % W] : kBotA;
       const int vB = (c + 1 < W) ? bd.B[(c + 1) % W] : kBotB;
       const int vM = (c + 1 < W) ? bd.M[(c + 1) % W] : 0;
-      const int nV = max(vA + kGapSO, vB);
-      const int nH = max(hA + kGapSO, hB);
-      const int2 w = *reinterpret_cast<const int2*>(rowp + bd.tc[c]);  // (POINT, match increment)
+      const int nV = max(vA, vB);
+      const int nH = max(hA, hB);
+      const int2 w = *reinterpret_cast<const int2*>(rowp + bd.tc[c]);  // (POINT + 7, match increment)
       const int pt = bd.A[c] + w.x;
       // (plain compares and maxima: fewer instructions than __vibmax_s32 here)
       const bool h_wins = nH >= nV;
@@ -1936,10 +1940,11 @@ __device__ __forceinline__ void banded_hit(const int2* __restrict__ tab, const c
       const int nS = max(mx, pt);
       const int side_m = h_wins ? hM : vM;
       const int nM = not_diag ? side_m : (bd.M[c] + w.y);
-      bd.A[c] = nS;
+      const int nA = nS + kGapSO;
+      bd.A[c] = nA;
       bd.B[c] = nV + kGapExtend;
       bd.M[c] = nM;
-      hA = nS;
+      hA = nA;
       hB = nH + kGapExtend;
       hM = nM;
       if (LOCAL) {
@@ -1971,13 +1976,13 @@ struct DpKernelArgs {
   DpOut o;
 };
 
-// The letter-pair table (POINT, match increment) of krnlMatrix.cuh in
+// The letter-pair table (POINT + 7, match increment) of krnlMatrix.cuh in
 // shared memory: [target letter][query letter], letters 'A'..'Z'.
 __device__ __forceinline__ void dp_table_init(int2* tab) {
   for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
     const int2 w = cell_score(class_of_letter((i >> 5) < 26 ? (i >> 5) : kNClass),
                               class_of_letter((i & 31) < 26 ? (i & 31) : kNClass));
-    tab[i] = w;
+    tab[i] = make_int2(w.x - (kGapOpen + kGapExtend), w.y);
   }
 }
 
