@@ -80,7 +80,7 @@ def parse():
     ap.add_argument("--uneven-reads", type=int, default=200_000)
     ap.add_argument("--uneven-steps", type=int, default=3)
     ap.add_argument("--uneven-warmup", type=int, default=2)
-    ap.add_argument("--serve-lanes", type=int, default=2)
+    ap.add_argument("--serve-lanes", type=int, default=4)
     ap.add_argument("--serve-batch", type=int, default=8_000_000)
     ap.add_argument("--serve-pool", type=int, default=60_000)
     ap.add_argument("--serve-backlog", type=int, default=1500)
@@ -469,7 +469,8 @@ def uneven_leg(eng, s, t, t_loads, reads, args):
                     "dp_frac_int32": round(dp_frac, 4) if dp_frac else None,
                     "dp_order": {0: "none", 1: "sorted by rows", 2: "length buckets"}[st["dp_order_kind"]],
                     "dp_launch": ("persistent queue, %d x 32 hits per take" % st["dp_queue_chunk"])
-                    if st["dp_queue_chunk"] else "one thread per hit, full grid"}
+                    if st["dp_queue_chunk"] else "one thread per hit, full grid",
+                    "dp_warp_hits": st["dp_warp_hits"]}
 
     run(eng, "tuned")
     os.environ["CLAST_DP_NO_TUNE"] = "1"

@@ -66,7 +66,8 @@ class clast_stats(C.Structure):
                 ("sort_ms", C.c_double), ("final_ms", C.c_double), ("index_wall_ms", C.c_double),
                 ("map_wall_ms", C.c_double), ("map_prep_ms", C.c_double), ("map_call_ms", C.c_double),
                 ("index_bases", C.c_int64), ("index_keys", C.c_int64), ("dp_order_ms", C.c_double),
-                ("dp_order_kind", C.c_int32), ("dp_queue_chunk", C.c_int32)]
+                ("dp_order_kind", C.c_int32), ("dp_queue_chunk", C.c_int32),
+                ("dp_warp_hits", C.c_int64)]
 
 
 # symbol name -> (restype, argtypes); the full export list of include/clast_gpu.h
@@ -97,6 +98,7 @@ SIGNATURES = {
                                    C.POINTER(clast_labels), C.POINTER(clast_labels), C.c_void_p, C.c_int32,
                                    C.POINTER(clast_tsv)]),
     "clast_tsv_free": (None, [C.POINTER(clast_tsv)]),
+    "clast_write_file": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int64, C.c_int32]),
     "clast_last_map_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "clast_get_stats": (C.c_int, [C.c_void_p, C.POINTER(clast_stats)]),
     "clast_int32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),

@@ -213,37 +213,6 @@ class _MapResultOwner:
         self.r = None
 
 
-def _write_parallel(path, mv, threads: int = 4, min_piece: int = 8 << 20):
-    """Writes a buffer to a new file with several positional writes in
-    parallel (the copies into the page cache run on several cores)."""
-    import threading
-    n = len(mv)
-    fd = os.open(path, os.O_WRONLY | os.O_CREAT | os.O_TRUNC, 0o644)
-    try:
-        if n:
-            os.ftruncate(fd, n)
-        k = max(1, min(threads, n // min_piece))
-        cuts = [n * i // k for i in range(k + 1)]
-        errs = []
-
-        def part(a, b):
-            try:
-                while a < b:
-                    a += os.pwrite(fd, mv[a:b], a)
-            except OSError as e:
-                errs.append(e)
-
-        ts = [threading.Thread(target=part, args=(cuts[i], cuts[i + 1])) for i in range(k)]
-        for x in ts:
-            x.start()
-        for x in ts:
-            x.join()
-        if errs:
-            raise errs[0]
-    finally:
-        os.close(fd)
-
-
 class TsvText:
     """A result text held in the library's pinned buffer (clast_format_tsv)."""
 
@@ -255,8 +224,12 @@ class TsvText:
         self.view = memoryview((C.c_char * max(n, 1)).from_address(t.text))[:n]
         self.load_offsets = np.ctypeslib.as_array(t.load_offsets, shape=(n_loads + 1,)).copy()
 
-    def write(self, path, threads: int = 4):
-        _write_parallel(path, self.view, threads)
+    def write(self, path, threads: int = 8):
+        """The text as a new file at path (clast_write_file)."""
+        rc = self._lib.clast_write_file(os.fsencode(path), self.t.text if self.n_bytes else None, self.n_bytes,
+                                        threads)
+        if rc != 0:
+            raise OSError("cannot write %s" % path)
 
     def release(self):
         if self.t is not None:
@@ -519,11 +492,11 @@ class Engine:
             self.last_tsv_load_offsets = np.ctypeslib.as_array(t.load_offsets, shape=(result.n_loads + 1,)).copy()
             if out is None:
                 return C.string_at(t.text, n) if n else b""
-            mv = memoryview((C.c_char * max(n, 1)).from_address(t.text))[:n]
             if isinstance(out, (str, bytes, os.PathLike)):
-                _write_parallel(out, mv)
+                if self._lib.clast_write_file(os.fsencode(out), t.text if n else None, n, 8) != 0:
+                    raise OSError("cannot write %s" % os.fsdecode(out))
             elif n:
-                out.write(mv)
+                out.write(memoryview((C.c_char * n).from_address(t.text)))
             return n
         finally:
             self._lib.clast_tsv_free(C.byref(t))

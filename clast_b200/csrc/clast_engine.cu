@@ -343,11 +343,15 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
   unsigned long long* counters = z.counters;
   uint64_t* skey = z.skey;
   uint32_t* sq = z.sq;
+  const long long* warp_dev = nullptr;  // the DP's split, when it was made on the device
   auto add_counters = [&]() {
     unsigned long long cells = 0;
+    long long warp = 0;
     CLAST_CK(cudaMemcpyAsync(&cells, counters + 1, sizeof(cells), cudaMemcpyDeviceToHost, st));
+    if (warp_dev) CLAST_CK(cudaMemcpyAsync(&warp, warp_dev, sizeof(warp), cudaMemcpyDeviceToHost, st));
     CLAST_CK(cudaStreamSynchronize(st));
     c->stats.dp_cells += (int64_t)cells;
+    c->stats.dp_warp_hits += warp;
     tm.flush();
   };
   c->stats.seeds += S;
@@ -394,8 +398,13 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
   // runs fastest is measured once per context and kind of batch (gap, mode,
   // uneven or not) on a batch of at least kDpTuneHits hits; every variant
   // writes the same results.
+  // The longest hits of the order may run one per warp (banded_dp decides
+  // from the length buckets, or for equal lengths from the row count).
   const bool uneven = qb.max_len != qb.min_len && H > 1;
+  const int warp_mode = dp_warp_mode_from_env();
+  DpBuckets buckets;  // of the order last made
   auto make_order = [&](int kind) -> const uint64_t* {
+    buckets = DpBuckets();
     if (kind == 0) return nullptr;
     if (kind == 1) {
       const int rows_max = std::max(1, qb.max_len - p->lmer + 1);
@@ -404,19 +413,29 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
       uint64_t* ok = ws.get<uint64_t>("h_order", H);
       uint64_t* ok2 = ws.get<uint64_t>("h_order2", H);
       dp_order_keys(hs, qb.len.p, H, p->lmer, rows_max, ok, st);
-      return radix_sort_u64(ws, ok, nullptr, ok2, nullptr, H, 32, 32 + bits, st) ? ok2 : ok;
+      const uint64_t* sorted = radix_sort_u64(ws, ok, nullptr, ok2, nullptr, H, 32, 32 + bits, st) ? ok2 : ok;
+      if (warp_mode == kDpWarpAuto) buckets = dp_bucket_count(ws, hs, qb.len.p, H, p->lmer, st);
+      return sorted;
     }
     uint64_t* ob = ws.get<uint64_t>("h_border", H);
-    dp_bucket_order(ws, hs, qb.len.p, H, p->lmer, ob, st);
+    buckets = dp_bucket_order(ws, hs, qb.len.p, H, p->lmer, ob, st);
     return ob;
   };
   unsigned long long* dp_head = ws.get<unsigned long long>("dp_head", 1);
+  long long* dp_warp_n = ws.get<long long>("dp_warp_n", 1);
   auto launch_of = [&](const DpChoice& ch) {
     DpLaunch m;
     if (ch.queue) {
       m.head = dp_head;
       m.chunk = ch.chunk;
     }
+    m.warp = warp_mode;
+    m.buckets = buckets;
+    m.warp_n = dp_warp_n;
+    m.aux = c->st_dp;
+    m.ev_fork = c->ev_dp_fork;
+    m.ev_join = c->ev_dp_join;
+    if (!uneven) m.uniform_rows = std::max(0, qb.max_len - p->lmer);
     return m;
   };
   const int tune_key = (p->gap << 2) | (p->local ? 2 : 0) | (uneven ? 1 : 0);
@@ -451,8 +470,11 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
   const uint64_t* order = make_order(ch.order);
   tm.end(StageTimer::DPORDER, st);
   tm.begin(st);
-  banded_dp(tv, q, hk, hq, hs, order, H, dp, o, st, launch_of(ch));
+  const DpLaunch dl = launch_of(ch);
+  const long long warp_fixed = banded_dp(tv, q, hk, hq, hs, order, H, dp, o, st, dl);
   tm.end(StageTimer::DP, st);
+  if (warp_fixed >= 0) c->stats.dp_warp_hits += warp_fixed;
+  else warp_dev = dl.warp_n;
   // resultSorting + deleteHits_duplicateResult, per read
   uint64_t* k1 = ws.get<uint64_t>("f_k1", H);
   uint64_t* k2 = ws.get<uint64_t>("f_k2", H);
@@ -577,6 +599,10 @@ int clast_ctx_create(int device, clast_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess) return CLAST_ERR_CUDA;
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
   if (cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
+  if (cudaStreamCreateWithFlags(&c->st_dp, cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
+  if (cudaEventCreateWithFlags(&c->ev_dp_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_dp_join, cudaEventDisableTiming) != cudaSuccess)
+    return CLAST_ERR_CUDA;
   for (int b = 0; b < kBuildStreams; ++b)
     if (cudaStreamCreateWithFlags(&c->st_build[b], cudaStreamNonBlocking) != cudaSuccess) return CLAST_ERR_CUDA;
   {  // keep freed pool memory for reuse by later calls of this process
@@ -618,6 +644,12 @@ void clast_ctx_destroy(clast_ctx* ctx) {
   if (ctx->ev3) cudaEventDestroy(ctx->ev3);
   if (ctx->ev_t0) cudaEventDestroy(ctx->ev_t0);
   if (ctx->ev_t1) cudaEventDestroy(ctx->ev_t1);
+  if (ctx->ev_dp_fork) cudaEventDestroy(ctx->ev_dp_fork);
+  if (ctx->ev_dp_join) cudaEventDestroy(ctx->ev_dp_join);
+  if (ctx->st_dp) {
+    cudaStreamSynchronize(ctx->st_dp);
+    cudaStreamDestroy(ctx->st_dp);
+  }
   if (ctx->st_copy) {
     cudaStreamSynchronize(ctx->st_copy);
     cudaStreamDestroy(ctx->st_copy);
@@ -919,6 +951,7 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     const double w0 = wall_ms();
     S.map_ms = S.map_upload_ms = 0;
     S.map_launches = S.query_bases = S.query_kmers = S.seeds = S.hits = S.results = S.dp_cells = 0;
+    S.dp_warp_hits = 0;
     ctx->timer.reset();
     const int64_t nreads = reads->n_seqs;
     if (nreads >= ((int64_t)1 << 30)) throw std::invalid_argument("at most 2^30 reads per map (2^31 strands)");
@@ -1373,18 +1406,27 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
     DpParams dp{p->lmer, p->stride, p->gap, p->local, p->cutoff, p->total_db, p->K, p->lambda};
     // reads of different lengths: hits longest first (length buckets), as clast_search
     // orders them, so that a warp's hits have about the same number of rows
+    // (and the longest one per warp, as there)
     const uint64_t* order = nullptr;
     int32_t lmin = INT32_MAX, lmax = 0;
     for (int32_t i = 0; i < n_qseqs; ++i) {
       lmin = std::min(lmin, q_lengths[i]);
       lmax = std::max(lmax, q_lengths[i]);
     }
+    DpLaunch m;
+    m.warp = dp_warp_mode_from_env();
+    m.aux = ctx->st_dp;
+    m.ev_fork = ctx->ev_dp_fork;
+    m.ev_join = ctx->ev_dp_join;
     if (lmin != lmax && H > 1) {
       uint64_t* ob = ws.get<uint64_t>("h_border", H);
-      dp_bucket_order(ws, hs, qlen, H, p->lmer, ob, st);
+      m.buckets = dp_bucket_order(ws, hs, qlen, H, p->lmer, ob, st);
+      m.warp_n = ws.get<long long>("dp_warp_n", 1);
       order = ob;
+    } else {
+      m.uniform_rows = std::max(0, lmax - p->lmer);
     }
-    banded_dp(tv, q, hk, hq, hs, order, H, dp, o, st);
+    banded_dp(tv, q, hk, hq, hs, order, H, dp, o, st, m);
     // resultSorting + deleteHits_duplicateResult, per read
     uint64_t* k1 = ws.get<uint64_t>("f_k1", H);
     uint64_t* k2 = ws.get<uint64_t>("f_k2", H);

@@ -195,6 +195,10 @@ struct clast_ctx {
   int64_t seed_hint = 0;  // seed buffer capacity that sufficed before
   std::map<int, clast::DpChoice> dp_tuned;  // by (gap, local, uneven)
   cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;  // DP tuning
+  // the DP's one-hit-per-warp kernel runs on st_dp beside the one-per-thread
+  // kernels on st (forked and joined by these events)
+  cudaStream_t st_dp = nullptr;
+  cudaEvent_t ev_dp_fork = nullptr, ev_dp_join = nullptr;
 };
 
 struct clast_index {

@@ -9,6 +9,8 @@
 
 #include <cerrno>
 #include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
 #include <unistd.h>
 #include <chrono>
 #include <climits>
@@ -551,36 +553,69 @@ int run(int argc, const char* const* argv, std::string& err) {
   }
   std::unique_ptr<clast_tsv, void (*)(clast_tsv*)> text_guard(&text, clast_tsv_free);
   clock.mark("TSV text");
-  // the file was truncated at start; the text goes in with several positional
-  // writes in parallel (the copies into the page cache run on several cores)
-  const int fd = ::open(s.out.c_str(), O_WRONLY);
-  if (fd < 0) throw UsageError(3, "cannot open output file " + s.out);
-  const int64_t n = text.n_bytes;
-  const int parts = (int)std::max<int64_t>(1, std::min<int64_t>(4, n / (8 << 20)));
-  std::vector<int> ok(parts, 1);
-  std::vector<std::thread> writers;
-  for (int k = 0; k < parts; ++k)
-    writers.emplace_back([&, k]() {
-      int64_t a = n * k / parts;
-      const int64_t b = n * (k + 1) / parts;
-      while (a < b) {
-        const ssize_t w = ::pwrite(fd, text.text + a, (size_t)(b - a), (off_t)a);
-        if (w <= 0) {
-          ok[k] = 0;
-          return;
-        }
-        a += w;
-      }
-    });
-  for (auto& w : writers) w.join();
-  const bool closed = ::close(fd) == 0;
-  for (int k = 0; k < parts; ++k)
-    if (!ok[k] || !closed) throw UsageError(3, "cannot write output file " + s.out);
+  // the file was truncated at start; the text goes in with several threads
+  if (clast_write_file(s.out.c_str(), text.text, text.n_bytes, 8) != CLAST_OK)
+    throw UsageError(3, "cannot write output file " + s.out);
   clock.mark("TSV write");
   return 0;
 }
 
 }  // namespace
+
+#ifndef MADV_POPULATE_WRITE
+#define MADV_POPULATE_WRITE 23  // Linux 5.14 (uapi/asm-generic/mman-common.h)
+#endif
+
+namespace {
+// positional writes of buf[a, b) at the same offsets
+bool pwrite_range(int fd, const char* buf, int64_t a, int64_t b) {
+  while (a < b) {
+    const ssize_t w = ::pwrite(fd, buf + a, (size_t)std::min<int64_t>(b - a, (int64_t)1 << 30), (off_t)a);
+    if (w < 0 && errno == EINTR) continue;
+    if (w <= 0) return false;
+    a += w;
+  }
+  return true;
+}
+}  // namespace
+
+extern "C" int clast_write_file(const char* path, const char* buf, int64_t n, int32_t threads) {
+  if (!path || n < 0 || (n > 0 && !buf)) return CLAST_ERR_ARG;
+  const int fd = ::open(path, O_RDWR | O_CREAT | O_TRUNC, 0644);
+  if (fd < 0) return CLAST_ERR_ARG;
+  bool ok = true;
+  if (n > 0) {
+    struct stat sb;
+    void* map = MAP_FAILED;
+    if (::fstat(fd, &sb) == 0 && S_ISREG(sb.st_mode) && ::ftruncate(fd, (off_t)n) == 0)
+      map = ::mmap(nullptr, (size_t)n, PROT_READ | PROT_WRITE, MAP_SHARED, fd, 0);
+    if (map == MAP_FAILED) {
+      ok = pwrite_range(fd, buf, 0, n);  // one write at a time holds the file's lock anyway
+    } else {
+      // Each thread makes the pages of its own range in one call and copies
+      // into them.  Where that call fails (no space, or a kernel without it)
+      // the range goes in with positional writes, which report the error
+      // instead of faulting on a page that cannot be made.
+      char* dst = static_cast<char*>(map);
+      const int64_t page = std::max<long>(4096, ::sysconf(_SC_PAGESIZE));
+      const int parts = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(1, (int)threads), n >> 22));
+      std::vector<int> part_ok(parts, 1);
+      std::vector<std::thread> ts;
+      for (int k = 0; k < parts; ++k)
+        ts.emplace_back([&, k]() {
+          const int64_t a = n * k / parts, b = n * (k + 1) / parts;
+          const int64_t pa = a / page * page;
+          if (::madvise(dst + pa, (size_t)(b - pa), MADV_POPULATE_WRITE) == 0) std::memcpy(dst + a, buf + a, (size_t)(b - a));
+          else part_ok[k] = pwrite_range(fd, buf, a, b) ? 1 : 0;
+        });
+      for (auto& t : ts) t.join();
+      for (int v : part_ok) ok = ok && v;
+      if (::munmap(map, (size_t)n) != 0) ok = false;
+    }
+  }
+  if (::close(fd) != 0) ok = false;
+  return ok ? CLAST_OK : CLAST_ERR_ARG;
+}
 
 extern "C" int clast_cli_main(int argc, const char* const* argv, char* err_buf, int err_len) {
   std::string err;

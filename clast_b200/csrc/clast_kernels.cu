@@ -13,6 +13,8 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
+#include <cstring>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -1964,6 +1966,186 @@ __device__ __forceinline__ void banded_hit(const int2* __restrict__ tab, const c
   }
 }
 
+// The same extension with one warp per hit: the band's anti-diagonal
+// wavefront.  Cell (r, c) of the band needs (r, c-1), (r-1, c+1) and (r-1, c),
+// so the cells with equal 2r + c are independent.  Lane j owns band columns 2j
+// and 2j + 1 and runs row r - j while lane 0 runs row r: column 2j at the even
+// step, taking its left neighbour from lane j - 1 (shuffle) and its upper-right
+// one from its own odd column; column 2j + 1 at the odd step, with its left
+// neighbour its own even column and its upper-right one from lane j + 1
+// (shuffle).  A row costs two steps instead of W dependent cells, which is
+// what one long hit in a small batch waits for.  Same cell arithmetic as
+// banded_hit, same tie rules (the local best is the first maximum in
+// row-major order, the global end node the first maximum in column order),
+// so every output equals banded_hit's.  Results are returned in every lane.
+template <int GAP, bool LOCAL>
+__device__ __forceinline__ void banded_hit_warp(const int2* __restrict__ tab, const char* __restrict__ tb,
+                                                int64_t tstart, int tlen, const char* __restrict__ qb, int64_t qstart,
+                                                int qlen, int tidx, int qidx, int l, int& t_hl, int& q_hl, int& match,
+                                                int& score, int& o_tidx, int& o_qidx) {
+  constexpr int W = 2 * GAP + 1;
+  constexpr int kGapSO = kGapOpen + kGapExtend;  // -7
+  constexpr int kBotA = (GAP + 1) * kGapExtend + kGapOpen + kGapSO;
+  constexpr int kBotB = (GAP + 1) * kGapExtend + kGapOpen + kGapOpen + kGapExtend;
+  constexpr int kMarginA = kMarginScore + kGapSO, kMarginB = kMarginScore + kGapExtend;
+  const int lane = threadIdx.x & 31;
+  const int ce = 2 * lane, co = 2 * lane + 1;  // this lane's band columns
+  const bool has_e = ce < W, has_o = co < W;
+  // lane 0's left neighbour is lane 31 (GAP <= 16 leaves it idle), which holds
+  // the band's left margin; lane GAP, without an odd column, holds the fixed
+  // band row below the last column there instead
+  const int left = (lane + 31) & 31, right = (lane + 1) & 31;
+  const char* tabb = reinterpret_cast<const char*>(tab);
+  const char* __restrict__ t_seq = tb + tstart;
+  const char* __restrict__ q_seq = qb + qstart;
+  const int rows_b = qlen - (qidx + l);
+  const int rows_f = qidx;
+  for (int pass = 0; pass < 2; ++pass) {
+    const int rows_p = pass == 0 ? rows_b : rows_f;
+    if (rows_p <= 0) continue;
+    // target base of cell (r, c): ib0 + step * (r + c), the bad-area letter
+    // outside [lo, hi); query base of row r: qi0 + step * r (banded_hit's
+    // indices, pass by pass)
+    const int step = pass == 0 ? 1 : -1;
+    const int ib0 = pass == 0 ? tidx + l - GAP : tidx + GAP - 1;
+    const int lo = pass == 0 ? INT_MIN : 0, hi = pass == 0 ? tlen : INT_MAX;
+    const int qi0 = pass == 0 ? qidx + l : qidx - 1;
+    auto t_byte = [&](int ib) -> char { return (ib < lo || ib >= hi) ? 'X' : t_seq[ib]; };
+    auto q_byte = [&](int r) -> char { return (unsigned)r < (unsigned)rows_p ? q_seq[qi0 + step * r] : 'N'; };
+    // initTempNodeArray for this lane's two columns (the state before row 0)
+    auto init_col = [&](int c, int& A, int& B, int& M) {
+      const int rr = c + 1;
+      int sc, v, m;
+      if (rr < GAP + 1) { sc = kMarginScore; v = kMarginScore; m = kMarginScore; }
+      else if (rr == GAP + 1) { sc = 0; v = kGapOpen; m = 0; }
+      else { sc = (rr - GAP - 1) * kGapExtend + kGapOpen; v = sc + kGapOpen; m = 0; }
+      A = sc + kGapSO;
+      B = v + kGapExtend;
+      M = m;
+    };
+    int eA, eB, eM, oA = 0, oB = 0, oM = 0, eH = 0, oH = 0;
+    init_col(ce, eA, eB, eM);
+    if (has_o) {
+      init_col(co, oA, oB, oM);
+    } else if (lane == 31) {
+      oA = kMarginA;
+      oH = kMarginB;
+      oM = kMarginScore;
+    } else {
+      oA = kBotA;
+      oB = kBotB;
+      oM = 0;
+    }
+    int bs = 0, bm = 0, calc = -1, ep = GAP;
+    // Row r of this lane uses the target bases r + 2j (even column; the odd
+    // column's base of row r - 1) and r + 2j + 1, and query base r.  Bytes are
+    // loaded four rows ahead and turned into table offsets one row ahead, so
+    // that no load's latency falls inside a row.
+    int r = -lane;
+    int te = base_class(t_byte(ib0 + step * (r + ce))) << 8;
+    int to = base_class(t_byte(ib0 + step * (r + co))) << 8;
+    char t1 = t_byte(ib0 + step * (r + 1 + co)), t2 = t_byte(ib0 + step * (r + 2 + co));
+    char t3 = t_byte(ib0 + step * (r + 3 + co));
+    int qc = base_class(q_byte(r)) << 3;
+    char q1 = q_byte(r + 1), q2 = q_byte(r + 2), q3 = q_byte(r + 3);
+    int tk = ib0 + step * (r + 4 + co);
+    const int n_iter = rows_p + GAP;  // lane GAP runs the last row at rows_p - 1 + GAP
+#pragma unroll 2
+    for (int it = 0; it < n_iter; ++it, ++r) {
+      const char t4 = t_byte(tk);
+      tk += step;
+      const char q4 = q_byte(r + 4);
+      const bool on = (unsigned)r < (unsigned)rows_p;
+      {  // even step: column 2j of row r; left neighbour from lane j - 1, upper right from our odd column
+        const int hA = __shfl_sync(kFull, oA, left);
+        const int hB = __shfl_sync(kFull, oH, left);
+        const int hM = __shfl_sync(kFull, oM, left);
+        const int nV = max(oA, oB);
+        const int nH = max(hA, hB);
+        const int2 w = *reinterpret_cast<const int2*>(tabb + te + qc);
+        const int pt = eA + w.x;
+        const bool h_wins = nH >= nV;
+        const int mx = max(nH, nV);
+        const bool not_diag = mx >= pt;
+        const int nS = max(mx, pt);
+        const int nM = not_diag ? (h_wins ? hM : oM) : (eM + w.y);
+        if (on && has_e) {
+          eA = nS + kGapSO;
+          eB = nV + kGapExtend;
+          eH = nH + kGapExtend;
+          eM = nM;
+          if (LOCAL && bs < nS) { bs = nS; bm = nM; calc = r; ep = ce; }
+        }
+      }
+      {  // odd step: column 2j + 1 of row r; left neighbour our even column, upper right from lane j + 1
+        const int vA = __shfl_sync(kFull, eA, right);
+        const int vB = __shfl_sync(kFull, eB, right);
+        const int vM = __shfl_sync(kFull, eM, right);
+        const int nV = max(vA, vB);
+        const int nH = max(eA, eH);
+        const int2 w = *reinterpret_cast<const int2*>(tabb + to + qc);
+        const int pt = oA + w.x;
+        const bool h_wins = nH >= nV;
+        const int mx = max(nH, nV);
+        const bool not_diag = mx >= pt;
+        const int nS = max(mx, pt);
+        const int nM = not_diag ? (h_wins ? eM : vM) : (oM + w.y);
+        if (on && has_o) {
+          oA = nS + kGapSO;
+          oB = nV + kGapExtend;
+          oH = nH + kGapExtend;
+          oM = nM;
+          if (LOCAL && bs < nS) { bs = nS; bm = nM; calc = r; ep = co; }
+        }
+      }
+      te = to;
+      to = base_class(t1) << 8;
+      t1 = t2;
+      t2 = t3;
+      t3 = t4;
+      qc = base_class(q1) << 3;
+      q1 = q2;
+      q2 = q3;
+      q3 = q4;
+    }
+    int best, best_m, e, move;
+    if (LOCAL) {  // first maximum in row-major order: (score desc, row asc, column asc)
+#pragma unroll
+      for (int off = 16; off; off >>= 1) {
+        const int xs = __shfl_xor_sync(kFull, bs, off), xm = __shfl_xor_sync(kFull, bm, off);
+        const int xc = __shfl_xor_sync(kFull, calc, off), xe = __shfl_xor_sync(kFull, ep, off);
+        if (xs > bs || (xs == bs && (xc < calc || (xc == calc && xe < ep)))) { bs = xs; bm = xm; calc = xc; ep = xe; }
+      }
+      best = bs;
+      best_m = bm;
+      e = ep;
+      move = calc + 1;
+    } else {  // end node: the first column of the last row with the highest score above the margin
+      int sc = INT_MIN, c = W, m = 0;
+      if (has_e) { sc = eA - kGapSO; c = ce; m = eM; }
+      if (has_o && oA - kGapSO > sc) { sc = oA - kGapSO; c = co; m = oM; }
+#pragma unroll
+      for (int off = 16; off; off >>= 1) {
+        const int xs = __shfl_xor_sync(kFull, sc, off), xc = __shfl_xor_sync(kFull, c, off);
+        const int xm = __shfl_xor_sync(kFull, m, off);
+        if (xs > sc || (xs == sc && xc < c)) { sc = xs; c = xc; m = xm; }
+      }
+      if (sc > kMarginScore) { best = sc; best_m = m; e = c; }
+      else { best = kMarginScore; best_m = kMarginScore; e = -1; }
+      move = rows_p;
+    }
+    e -= GAP;
+    if (pass == 1) {
+      o_tidx -= move + e;
+      o_qidx -= move;
+    }
+    t_hl += move + e;
+    q_hl += move;
+    match += best_m;
+    score += best;
+  }
+}
+
 struct DpKernelArgs {
   TargetView t;
   QueryView q;
@@ -1974,7 +2156,16 @@ struct DpKernelArgs {
   int64_t n;
   DpParams p;
   DpOut o;
+  // the first n_warp hits of the order run one per warp (k_banded_dp_warp),
+  // the others one per thread: n_warp = *warp_n when given, else warp_fixed
+  const long long* warp_n;
+  long long warp_fixed;
 };
+
+__device__ __forceinline__ int64_t dp_warp_hits(const DpKernelArgs& a) {
+  const int64_t w = a.warp_n ? (int64_t)*a.warp_n : (int64_t)a.warp_fixed;
+  return w < a.n ? w : a.n;
+}
 
 // The letter-pair table (POINT + 7, match increment) of krnlMatrix.cuh in
 // shared memory: [target letter][query letter], letters 'A'..'Z'.
@@ -1984,6 +2175,22 @@ __device__ __forceinline__ void dp_table_init(int2* tab) {
                               class_of_letter((i & 31) < 26 ? (i & 31) : kNClass));
     tab[i] = make_int2(w.x - (kGapOpen + kGapExtend), w.y);
   }
+}
+
+// calculateEvalue (krnlCalculateEvalue.cu:21, same operation order) and the
+// two hit filters of deleteBadHits, then the hit's outputs at its own index.
+__device__ __forceinline__ void dp_store(const DpKernelArgs& a, int64_t h, int qlen, int o_tidx, int o_qidx, int t_hl,
+                                         int q_hl, int match, int score) {
+  const double e = a.p.K * a.p.total_db * (double)qlen * exp(-a.p.lambda * (double)score);
+  const bool keep = !(a.p.cutoff != -1.0 && a.p.cutoff < e) && !(a.p.l + a.p.stride > q_hl);
+  a.o.t_idx[h] = o_tidx;
+  a.o.q_idx[h] = o_qidx;
+  a.o.t_len[h] = t_hl;
+  a.o.q_len[h] = q_hl;
+  a.o.match[h] = match;
+  a.o.score[h] = score;
+  a.o.evalue[h] = e;
+  a.o.keep[h] = keep ? 1 : 0;
 }
 
 // Extension of the hit at position i of the order (alignmentHits +
@@ -2005,17 +2212,7 @@ __device__ __forceinline__ void dp_one(const DpKernelArgs& a, const int2* tab, i
   int o_tidx = tidx, o_qidx = qidx;
   banded_hit<GAP, LOCAL>(tab, a.t.bases, tstart, tlen, a.q.bases, qstart, qlen, tidx, qidx, l, t_hl, q_hl, match,
                          score, o_tidx, o_qidx);
-  // calculateEvalue, krnlCalculateEvalue.cu:21 (same operation order)
-  const double e = a.p.K * a.p.total_db * (double)qlen * exp(-a.p.lambda * (double)score);
-  const bool keep = !(a.p.cutoff != -1.0 && a.p.cutoff < e) && !(l + a.p.stride > q_hl);
-  a.o.t_idx[h] = o_tidx;
-  a.o.q_idx[h] = o_qidx;
-  a.o.t_len[h] = t_hl;
-  a.o.q_len[h] = q_hl;
-  a.o.match[h] = match;
-  a.o.score[h] = score;
-  a.o.evalue[h] = e;
-  a.o.keep[h] = keep ? 1 : 0;
+  dp_store(a, h, qlen, o_tidx, o_qidx, t_hl, q_hl, match, score);
 }
 
 template <int GAP, bool LOCAL>
@@ -2023,7 +2220,7 @@ __global__ void __launch_bounds__(128, GAP <= 9 ? 4 : (GAP <= 12 ? 3 : 2)) k_ban
   __shared__ int2 tab[32 * 32];
   dp_table_init(tab);
   __syncthreads();
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = dp_warp_hits(a) + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   dp_one<GAP, LOCAL>(a, tab, i);
 }
@@ -2040,15 +2237,46 @@ __global__ void __launch_bounds__(128, GAP <= 9 ? 4 : (GAP <= 12 ? 3 : 2))
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned long long take = 32ull * (unsigned long long)chunk;
+  const int64_t first = dp_warp_hits(a);  // the hits before it run one per warp
   for (;;) {
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(head, take);
     base = __shfl_sync(kFull, base, 0);
-    if (base >= (unsigned long long)a.n) break;
+    if (first + (int64_t)base >= a.n) break;
     for (int c = 0; c < chunk; ++c) {
-      const int64_t i = (int64_t)base + 32 * c + lane;
+      const int64_t i = first + (int64_t)base + 32 * c + lane;
       if (i < a.n) dp_one<GAP, LOCAL>(a, tab, i);
     }
+  }
+}
+
+// One hit per warp (banded_hit_warp) for the first n_warp hits of the order,
+// the longest ones: a grid-stride loop over them, one warp each.
+template <int GAP, bool LOCAL>
+__global__ void __launch_bounds__(128) k_banded_dp_warp(DpKernelArgs a) {
+  __shared__ int2 tab[32 * 32];
+  dp_table_init(tab);
+  __syncthreads();
+  const int64_t nw = dp_warp_hits(a);
+  const int lane = threadIdx.x & 31;
+  const int64_t wpb = blockDim.x >> 5;
+  for (int64_t i = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); i < nw; i += (int64_t)gridDim.x * wpb) {
+    const int64_t h = a.order ? (int64_t)(uint32_t)a.order[i] : i;
+    const uint64_t k = a.hk[h];
+    const int qidx = a.hq[h];
+    const int s = a.hs[h];
+    const int tid = (int)(k >> 32);
+    const int tidx = (int)((uint32_t)k ^ 0x80000000u) + qidx;
+    const int64_t tstart = a.t.gateway[tid];
+    const int tlen = a.t.lengths[tid];
+    const int64_t qstart = a.q.start[s];
+    const int qlen = a.q.len[s];
+    const int l = a.p.l;
+    int t_hl = l, q_hl = l, match = l, score = l;  // CDeviceHitList.cu:283-286
+    int o_tidx = tidx, o_qidx = qidx;
+    banded_hit_warp<GAP, LOCAL>(tab, a.t.bases, tstart, tlen, a.q.bases, qstart, qlen, tidx, qidx, l, t_hl, q_hl,
+                                match, score, o_tidx, o_qidx);
+    if (lane == 0) dp_store(a, h, qlen, o_tidx, o_qidx, t_hl, q_hl, match, score);
   }
 }
 
@@ -2064,15 +2292,101 @@ __device__ __forceinline__ int dp_bucket(int rows) {
 }
 
 __global__ void k_dp_bucket_count(const int32_t* __restrict__ hs, const int32_t* __restrict__ q_len, int64_t n, int l,
-                                  unsigned int* __restrict__ count) {
+                                  unsigned int* __restrict__ count, unsigned long long* __restrict__ rows) {
   __shared__ unsigned int c[kDpBuckets];
-  for (int i = threadIdx.x; i < kDpBuckets; i += blockDim.x) c[i] = 0;
+  __shared__ unsigned long long sr[kDpBuckets];
+  for (int i = threadIdx.x; i < kDpBuckets; i += blockDim.x) {
+    c[i] = 0;
+    sr[i] = 0;
+  }
   __syncthreads();
-  for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < n; h += (int64_t)gridDim.x * blockDim.x)
-    atomicAdd(&c[dp_bucket(max(0, q_len[hs[h]] - l))], 1u);
+  for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < n; h += (int64_t)gridDim.x * blockDim.x) {
+    const int r = max(0, q_len[hs[h]] - l);
+    const int b = dp_bucket(r);
+    atomicAdd(&c[b], 1u);
+    atomicAdd(&sr[b], (unsigned long long)r);
+  }
   __syncthreads();
   for (int i = threadIdx.x; i < kDpBuckets; i += blockDim.x)
-    if (c[i]) atomicAdd(&count[i], c[i]);
+    if (c[i]) {
+      atomicAdd(&count[i], c[i]);
+      atomicAdd(&rows[i], sr[i]);
+    }
+}
+
+// Rows of bucket b (ascending b = longest first): [dp_bucket_lo(b), dp_bucket_hi(b)].
+__host__ __device__ __forceinline__ long long dp_bucket_lo(int b) {
+  const int x = kDpBuckets - 1 - b;
+  if (x < 16) return x;
+  const int e = x / 16 + 3, sub = x % 16;
+  return (long long)(16 + sub) << (e - 4);
+}
+__host__ __device__ __forceinline__ long long dp_bucket_hi(int b) {
+  const int x = kDpBuckets - 1 - b;
+  if (x < 16) return x;
+  return dp_bucket_lo(b) + (1ll << (x / 16 - 1)) - 1;
+}
+
+// Cost model of the warp / thread split, in SM clock cycles, fitted on the
+// B200 at gap 8 (W = 17): a hit in thread mode takes kDpThreadCellCycles per
+// cell when its warp has the SM sub-partition to itself (a row is W dependent
+// cells), and a full grid runs kDpThreadCellsPerCycle cells per cycle; a hit
+// in warp mode takes kDpWarpRowCycles per row alone (two wavefront steps),
+// and warps run kDpWarpRowsPerCycle rows per cycle over the GPU.  The two
+// kernels run side by side: with L the longer of the two longest hits' times
+// and I the issue time of both kernels' work, the batch takes max(L + I/2, I)
+// (measured: a lone hit's rows slow down as other warps share its
+// sub-partition, and the GPU cannot issue faster than I).  Forking the second
+// stream and the launch cost kDpLaunchCycles.  Only the split depends on
+// these; results do not.
+constexpr double kDpThreadCellCycles = 34.0;
+constexpr double kDpThreadCellsPerCycle = 490.0;
+constexpr double kDpWarpRowCycles = 289.0;
+constexpr double kDpWarpRowsPerCycle = 4.7;
+constexpr double kDpLaunchCycles = 10000.0;
+constexpr long long kDpWarpMinRows = 16;
+
+// Estimated time of the DP with the `s` longest hits (rows summed: sw, the
+// longest r1) one per warp and the rest (rows summed: rest, the longest rn)
+// one per thread.
+__host__ __device__ __forceinline__ double dp_split_cycles(int W, long long s, double r1, double sw, double rn,
+                                                           double rest) {
+  double lat = s > 0 ? r1 * kDpWarpRowCycles : 0.0;
+  if (rest > 0) lat = fmax(lat, rn * W * kDpThreadCellCycles);
+  const double issue = (s > 0 ? sw / kDpWarpRowsPerCycle : 0.0) + rest * W / kDpThreadCellsPerCycle;
+  return fmax(lat + 0.5 * issue, issue) + (s > 0 ? kDpLaunchCycles : 0.0);
+}
+
+// The split on the device: every bucket boundary (longest first) is a
+// candidate; the earliest estimated end wins.  One thread; ~500 buckets.
+__global__ void k_dp_warp_split(const unsigned int* __restrict__ count, const unsigned long long* __restrict__ rows,
+                                int W, long long cap, long long* __restrict__ warp_n) {
+  if (threadIdx.x != 0) return;
+  double total = 0;
+  for (int b = 0; b < kDpBuckets; ++b) total += (double)rows[b];
+  long long s = 0, best_s = 0;
+  double sw = 0, r1 = -1, best = 0;
+  bool all_taken = true;
+  for (int b = 0; b < kDpBuckets; ++b) {
+    if (!count[b]) continue;
+    const double rn = (double)dp_bucket_hi(b);
+    // candidate: the buckets before b one per warp, b and the rest one per thread
+    if (r1 < 0) {
+      r1 = rn;
+      best = dp_split_cycles(W, 0, 0, 0, rn, total);
+    } else {
+      const double t = dp_split_cycles(W, s, r1, sw, rn, total - sw);
+      if (t < best) { best = t; best_s = s; }
+    }
+    if (dp_bucket_lo(b) < kDpWarpMinRows || s + count[b] > cap) {
+      all_taken = false;
+      break;
+    }
+    s += count[b];
+    sw += (double)rows[b];
+  }
+  if (all_taken && s > 0 && dp_split_cycles(W, s, r1, sw, 0, 0) < best) best_s = s;  // every hit one per warp
+  *warp_n = best_s;
 }
 
 // exclusive scan of the bucket counts in one block (kDpBuckets <= 1024)
@@ -2099,32 +2413,80 @@ __global__ void k_dp_bucket_scatter(const int32_t* __restrict__ hs, const int32_
 }
 
 template <int GAP, bool LOCAL>
-void launch_dp_mode(const DpKernelArgs& a, const DpLaunch& m, cudaStream_t st) {
+long long launch_dp_mode(DpKernelArgs a, const DpLaunch& m, cudaStream_t st) {
+  constexpr int W = 2 * GAP + 1;
   const int threads = 128;
-  if (m.head == nullptr) {
-    const unsigned grid = (unsigned)((a.n + threads - 1) / threads);
+  struct Occupancy {
+    int sms = 0, per_sm = 1, warp_per_sm = 1;
+  };
+  static const Occupancy occ = [] {  // once per kernel pair (thread-safe static initialisation)
+    Occupancy o;
+    int dev = 0;
+    CLAST_CK(cudaGetDevice(&dev));
+    CLAST_CK(cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev));
+    CLAST_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_banded_dp_queue<GAP, LOCAL>, 128, 0));
+    CLAST_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.warp_per_sm, k_banded_dp_warp<GAP, LOCAL>, 128, 0));
+    o.per_sm = std::max(1, o.per_sm);
+    o.warp_per_sm = std::max(1, o.warp_per_sm);
+    return o;
+  }();
+  const int sms = occ.sms, per_sm = occ.per_sm, warp_per_sm = occ.warp_per_sm;
+  // hits one per warp: at most one wave of the warp kernel's resident warps
+  // (the cost model has no waves)
+  const long long cap = (long long)sms * warp_per_sm * (threads / 32);
+  a.warp_n = nullptr;
+  a.warp_fixed = 0;
+  if (m.warp == kDpWarpAll) {
+    a.warp_fixed = a.n;
+  } else if (m.warp == kDpWarpAuto) {
+    if (m.buckets.count && m.warp_n) {
+      k_dp_warp_split<<<1, 32, 0, st>>>(m.buckets.count, m.buckets.rows, W, cap, m.warp_n);
+      CLAST_LAUNCHED();
+      a.warp_n = m.warp_n;
+    } else if (m.uniform_rows >= kDpWarpMinRows && a.n <= cap) {
+      const double r = (double)m.uniform_rows, rows = r * (double)a.n;
+      if (dp_split_cycles(W, a.n, r, rows, 0, 0) < dp_split_cycles(W, 0, 0, 0, r, rows)) a.warp_fixed = a.n;
+    }
+  }
+  const int64_t rest = a.n - (a.warp_n ? 0 : a.warp_fixed);  // hits left for the one-per-thread kernels (at most)
+  bool joined = false;
+  if (a.warp_n || a.warp_fixed > 0) {
+    const long long most = a.warp_n ? std::min<long long>(cap, a.n) : a.warp_fixed;
+    const long long blocks = std::min<long long>((most + 3) / 4, (long long)sms * warp_per_sm);
+    cudaStream_t sw = st;
+    if (m.aux && m.ev_fork && m.ev_join && rest > 0) {  // beside the one-per-thread kernel
+      CLAST_CK(cudaEventRecord(m.ev_fork, st));
+      CLAST_CK(cudaStreamWaitEvent(m.aux, m.ev_fork, 0));
+      sw = m.aux;
+    }
+    k_banded_dp_warp<GAP, LOCAL><<<(unsigned)std::max<long long>(1, blocks), threads, 0, sw>>>(a);
+    CLAST_LAUNCHED();
+    if (sw != st) {
+      CLAST_CK(cudaEventRecord(m.ev_join, sw));
+      joined = true;
+    }
+  }
+  const long long warp_hits = a.warp_n ? -1 : a.warp_fixed;
+  if (rest <= 0) return warp_hits;
+  // a batch that fits in one wave of the grid runs one hit per thread: the
+  // queue's takes of several hits per lane would only lengthen the longest
+  if (m.head == nullptr || rest <= (int64_t)sms * per_sm * threads) {
+    const unsigned grid = (unsigned)((rest + threads - 1) / threads);
     k_banded_dp<GAP, LOCAL><<<grid, threads, 0, st>>>(a);
   } else {
-    static int sms = 0, per_sm = 0;
-    if (!sms) {
-      int dev = 0;
-      CLAST_CK(cudaGetDevice(&dev));
-      CLAST_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-      CLAST_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_banded_dp_queue<GAP, LOCAL>, threads, 0));
-      per_sm = std::max(1, per_sm);
-    }
-    const int64_t need = (a.n + 32 * m.chunk - 1) / (32 * m.chunk) / (threads / 32) + 1;
+    const int64_t need = (rest + 32 * m.chunk - 1) / (32 * m.chunk) / (threads / 32) + 1;
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, need));
     CLAST_CK(cudaMemsetAsync(m.head, 0, sizeof(unsigned long long), st));
     k_banded_dp_queue<GAP, LOCAL><<<grid, threads, 0, st>>>(a, m.head, m.chunk);
   }
   CLAST_LAUNCHED();
+  if (joined) CLAST_CK(cudaStreamWaitEvent(st, m.ev_join, 0));
+  return warp_hits;
 }
 
 template <int GAP>
-void launch_dp_gap(const DpKernelArgs& a, bool local, const DpLaunch& m, cudaStream_t st) {
-  if (local) launch_dp_mode<GAP, true>(a, m, st);
-  else launch_dp_mode<GAP, false>(a, m, st);
+long long launch_dp_gap(const DpKernelArgs& a, bool local, const DpLaunch& m, cudaStream_t st) {
+  return local ? launch_dp_mode<GAP, true>(a, m, st) : launch_dp_mode<GAP, false>(a, m, st);
 }
 
 // ------------------------------------------------------------------------
@@ -2536,43 +2898,65 @@ void dp_order_keys(const int32_t* hs, const int32_t* q_len, int64_t n_hits, int 
   CLAST_LAUNCHED();
 }
 
-void dp_bucket_order(Workspace& ws, const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l, uint64_t* order,
-                     cudaStream_t st) {
-  if (n_hits <= 0) return;
+DpBuckets dp_bucket_count(Workspace& ws, const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l,
+                          cudaStream_t st) {
   unsigned int* count = ws.get<unsigned int>("dpb_count", kDpBuckets);
-  unsigned long long* cursor = ws.get<unsigned long long>("dpb_cursor", kDpBuckets);
+  unsigned long long* rows = ws.get<unsigned long long>("dpb_rows", kDpBuckets);
   CLAST_CK(cudaMemsetAsync(count, 0, kDpBuckets * sizeof(unsigned int), st));
-  k_dp_bucket_count<<<grid_cap(std::min<int64_t>(blocks_for(n_hits, 256), 1184)), 256, 0, st>>>(hs, q_len, n_hits, l,
-                                                                                                  count);
-  CLAST_LAUNCHED();
-  k_dp_bucket_scan<<<1, 1024, 0, st>>>(count, cursor);
+  CLAST_CK(cudaMemsetAsync(rows, 0, kDpBuckets * sizeof(unsigned long long), st));
+  if (n_hits > 0) {
+    k_dp_bucket_count<<<grid_cap(std::min<int64_t>(blocks_for(n_hits, 256), 1184)), 256, 0, st>>>(hs, q_len, n_hits,
+                                                                                                    l, count, rows);
+    CLAST_LAUNCHED();
+  }
+  DpBuckets b;
+  b.count = count;
+  b.rows = rows;
+  return b;
+}
+
+DpBuckets dp_bucket_order(Workspace& ws, const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l,
+                          uint64_t* order, cudaStream_t st) {
+  const DpBuckets b = dp_bucket_count(ws, hs, q_len, n_hits, l, st);
+  if (n_hits <= 0) return b;
+  unsigned long long* cursor = ws.get<unsigned long long>("dpb_cursor", kDpBuckets);
+  k_dp_bucket_scan<<<1, 1024, 0, st>>>(b.count, cursor);
   CLAST_LAUNCHED();
   k_dp_bucket_scatter<<<blocks_for(n_hits, 256), 256, 0, st>>>(hs, q_len, n_hits, l, cursor, order);
   CLAST_LAUNCHED();
+  return b;
 }
 
-void banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq, const int32_t* hs,
-               const uint64_t* order, int64_t n_hits, const DpParams& p, const DpOut& o, cudaStream_t st,
-               const DpLaunch& m) {
-  if (n_hits <= 0) return;
-  DpKernelArgs a{t, q, hk, hq, hs, order, n_hits, p, o};
+int dp_warp_mode_from_env() {
+  const char* v = std::getenv("CLAST_DP_WARP");
+  if (!v) return kDpWarpAuto;
+  if (!std::strcmp(v, "off")) return kDpWarpOff;
+  if (!std::strcmp(v, "all")) return kDpWarpAll;
+  return kDpWarpAuto;
+}
+
+long long banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq,
+                    const int32_t* hs, const uint64_t* order, int64_t n_hits, const DpParams& p, const DpOut& o,
+                    cudaStream_t st, const DpLaunch& m) {
+  if (n_hits <= 0) return 0;
+  DpKernelArgs a{t, q, hk, hq, hs, order, n_hits, p, o, nullptr, 0};
   const bool local = p.local != 0;
   switch (p.gap) {
-    case 2: launch_dp_gap<2>(a, local, m, st); break;
-    case 3: launch_dp_gap<3>(a, local, m, st); break;
-    case 4: launch_dp_gap<4>(a, local, m, st); break;
-    case 5: launch_dp_gap<5>(a, local, m, st); break;
-    case 6: launch_dp_gap<6>(a, local, m, st); break;
-    case 7: launch_dp_gap<7>(a, local, m, st); break;
-    case 8: launch_dp_gap<8>(a, local, m, st); break;
-    case 9: launch_dp_gap<9>(a, local, m, st); break;
-    case 10: launch_dp_gap<10>(a, local, m, st); break;
-    case 11: launch_dp_gap<11>(a, local, m, st); break;
-    case 12: launch_dp_gap<12>(a, local, m, st); break;
-    case 13: launch_dp_gap<13>(a, local, m, st); break;
-    case 14: launch_dp_gap<14>(a, local, m, st); break;
-    case 15: launch_dp_gap<15>(a, local, m, st); break;
-    case 16: launch_dp_gap<16>(a, local, m, st); break;
+    case 2: return launch_dp_gap<2>(a, local, m, st);
+    case 3: return launch_dp_gap<3>(a, local, m, st);
+    case 4: return launch_dp_gap<4>(a, local, m, st);
+    case 5: return launch_dp_gap<5>(a, local, m, st);
+    case 6: return launch_dp_gap<6>(a, local, m, st);
+    case 7: return launch_dp_gap<7>(a, local, m, st);
+    case 8: return launch_dp_gap<8>(a, local, m, st);
+    case 9: return launch_dp_gap<9>(a, local, m, st);
+    case 10: return launch_dp_gap<10>(a, local, m, st);
+    case 11: return launch_dp_gap<11>(a, local, m, st);
+    case 12: return launch_dp_gap<12>(a, local, m, st);
+    case 13: return launch_dp_gap<13>(a, local, m, st);
+    case 14: return launch_dp_gap<14>(a, local, m, st);
+    case 15: return launch_dp_gap<15>(a, local, m, st);
+    case 16: return launch_dp_gap<16>(a, local, m, st);
     default: throw std::invalid_argument("gap out of range 2..16");
   }
 }

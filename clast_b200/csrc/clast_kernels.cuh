@@ -136,19 +136,50 @@ struct DpParams {
 // (head null), or a persistent grid whose warps take `chunk` x 32 hits at a
 // time from a queue (head: a device counter the launch zeroes).  Results are
 // the same either way.
+//
+// Independently of that, the first hits of the order (the longest, when the
+// order is longest first) may run one per warp (an anti-diagonal wavefront
+// over the band) instead of one per thread: a long hit alone takes about 1/7
+// of the time there, at a lower throughput per cell.  `warp` says how many:
+// kDpWarpAuto splits where the cost model puts the end of both launches
+// earliest -- on the device from the length buckets' counts and row sums
+// (buckets + warp_n), or, for hits that all have `uniform_rows` rows, all or
+// none on the host; kDpWarpOff runs every hit one per thread, kDpWarpAll one
+// per warp.  Results are the same either way.
+constexpr int kDpWarpAuto = 0, kDpWarpOff = 1, kDpWarpAll = 2;
+struct DpBuckets {
+  const unsigned int* count = nullptr;      // hits per length bucket (longest first)
+  const unsigned long long* rows = nullptr;  // their rows, summed
+};
 struct DpLaunch {
   unsigned long long* head = nullptr;
   int chunk = 1;
+  int warp = kDpWarpAuto;
+  DpBuckets buckets;
+  long long* warp_n = nullptr;  // device word for the split (with buckets)
+  int uniform_rows = -1;
+  // with aux, the one-per-warp kernel runs there, beside the others (forked
+  // from and joined back into the launch stream by the two events)
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 // order (may be null): the hits in the order the threads take them, as words
 // whose low 32 bits are hit indices; outputs stay at the hit's own index.
-void banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq,
+// Returns how many hits ran one per warp, or -1 when the split was made on the
+// device (the count is then in *m.warp_n).
+long long banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq,
                const int32_t* hs, const uint64_t* order, int64_t n_hits, const DpParams& p, const DpOut& o,
                cudaStream_t st, const DpLaunch& m = DpLaunch());
-// DP order by length buckets (16 per power of two of the row count, longest
-// first): order[k] = hit index, in one counting pass instead of a sort.
-void dp_bucket_order(Workspace& ws, const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l, uint64_t* order,
-                     cudaStream_t st);
+// Hits per length bucket (16 per power of two of the row count, longest
+// first) and their row sums, in the workspace.
+DpBuckets dp_bucket_count(Workspace& ws, const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l,
+                          cudaStream_t st);
+// DP order by length buckets: order[k] = hit index, in one counting pass
+// instead of a sort (the counts of dp_bucket_count, which it runs).
+DpBuckets dp_bucket_order(Workspace& ws, const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l,
+                          uint64_t* order, cudaStream_t st);
+// CLAST_DP_WARP=off|all overrides kDpWarpAuto (for tests and measurements).
+int dp_warp_mode_from_env();
 // keys[h] = (rows_max - rows of hit h) << 32 | h, rows = q_len[hs[h]] - l + 1:
 // ascending keys take the hits longest first.
 void dp_order_keys(const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l, int rows_max, uint64_t* keys,

@@ -238,6 +238,14 @@ int clast_format_tsv(clast_ctx* ctx, const clast_targets* t, const clast_map_res
                      int32_t num_out, clast_tsv* out);
 void clast_tsv_free(clast_tsv* t);
 
+/* Writes n bytes of buf as a new file at path (created or truncated, as
+ * std::ofstream opens printResult's output), with `threads` host threads:
+ * the file is sized, mapped, and each thread makes its own range's pages
+ * and copies into them (a single write() call holds the file's lock for the
+ * whole copy).  Files that cannot be mapped (pipes, devices) get positional
+ * writes.  CLAST_ERR_ARG when the file cannot be opened or written. */
+int clast_write_file(const char* path, const char* buf, int64_t n, int32_t threads);
+
 /* Hands back the device memory a context keeps for reuse between calls: its
  * scratch buffers, the device copies of released results, and the blocks
  * the device's memory pool holds after stream-ordered frees.  Results and
@@ -280,6 +288,7 @@ typedef struct clast_stats {
   int32_t dp_order_kind;     /* DP order used last: 0 none, 1 sorted by rows, 2 length buckets */
   int32_t dp_queue_chunk;    /* 0: one thread per hit over a full grid; k: persistent grid taking
                                 k x 32 hits per warp from a queue              */
+  int64_t dp_warp_hits;      /* hits extended one per warp (the longest of their batch) */
 } clast_stats;
 int clast_get_stats(const clast_ctx* ctx, clast_stats* out);
 
