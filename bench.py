@@ -389,9 +389,14 @@ def served_leg(eng, s, t, t_loads, args):
         return done
 
     run(1, 50, backlog=True)  # warm-up: lane scratch and pinned buffers
-    bl = run(1, args.serve_backlog, backlog=True)
-    span = (max(x[3] for x in bl) - min(x[2] for x in bl)) / 1e9
-    peak_bps = sum(x[1] for x in bl) / span
+    # the peak: the better of two saturating backlogs (one host hiccup during
+    # a backlog lowers that run's rate)
+    peaks = []
+    for _ in range(2):
+        bl = run(1, args.serve_backlog, backlog=True)
+        span = (max(x[3] for x in bl) - min(x[2] for x in bl)) / 1e9
+        peaks.append(sum(x[1] for x in bl) / span)
+    peak_bps = max(peaks)
     mean_b = float(req_bases.mean())
     levels = []
     for frac in (0.2, 0.4, 0.6, 0.8, 1.0):
@@ -413,11 +418,11 @@ def served_leg(eng, s, t, t_loads, args):
     srv.close()
     T.close()
     return {
-        "peak_mbps": round(peak_bps / 1e6, 1), "levels": levels,
+        "peak_mbps": round(peak_bps / 1e6, 1), "peak_runs_mbps": [round(x / 1e6, 1) for x in peaks], "levels": levels,
         "p99_ms_at_80pct": next(x["p99_ms"] for x in levels if x["offered_frac"] == 0.8),
         "config": "%s target resident (%d bp, %d windows); requests of 1-10,000 reads (log-uniform count) of "
                   "100-5,000 bp (log-uniform), 2 %% substitutions, 5 %% decoys, from a pool of %d reads; lanes %d, "
-                  "max batch %d bases; peak from a backlog of %d requests; %.0f s per level" % (
+                  "max batch %d bases; peak: the better of two backlogs of %d requests; %.0f s per level" % (
                       getattr(args, "workload", "medium"), int(t.offsets[-1]),
                       len(target_windows(np.diff(t.offsets), t_loads, s.lmer, int(T_VRAM))), args.serve_pool,
                       args.serve_lanes, args.serve_batch, args.serve_backlog, args.serve_seconds),

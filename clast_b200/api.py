@@ -535,7 +535,7 @@ class Server:
     of MAP_FIELDS (read = record index within the request) plus
     ``load_offsets``, copied out of the library."""
 
-    def __init__(self, engine: "Engine", targets: Targets, s: Setting, lanes: int = 2, q_vram: int = 2_000_000,
+    def __init__(self, engine: "Engine", targets: Targets, s: Setting, lanes: int = 4, q_vram: int = 2_000_000,
                  q_ram: int = 32_000_000, max_batch_bases: int = 8_000_000, hbm_budget: int = 0,
                  hbm_reserve: int = 0):
         self._lib = N.load()

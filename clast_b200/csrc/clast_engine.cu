@@ -435,6 +435,7 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
     m.aux = c->st_dp;
     m.ev_fork = c->ev_dp_fork;
     m.ev_join = c->ev_dp_join;
+    m.share = c->dp_share;
     if (!uneven) m.uniform_rows = std::max(0, qb.max_len - p->lmer);
     return m;
   };
@@ -1418,6 +1419,7 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
     m.aux = ctx->st_dp;
     m.ev_fork = ctx->ev_dp_fork;
     m.ev_join = ctx->ev_dp_join;
+    m.share = ctx->dp_share;
     if (lmin != lmax && H > 1) {
       uint64_t* ob = ws.get<uint64_t>("h_border", H);
       m.buckets = dp_bucket_order(ws, hs, qlen, H, p->lmer, ob, st);

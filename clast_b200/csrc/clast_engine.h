@@ -199,6 +199,7 @@ struct clast_ctx {
   // kernels on st (forked and joined by these events)
   cudaStream_t st_dp = nullptr;
   cudaEvent_t ev_dp_fork = nullptr, ev_dp_join = nullptr;
+  int dp_share = 1;  // batches sharing the GPU with this context's (a server's lanes)
 };
 
 struct clast_index {

@@ -162,6 +162,9 @@ struct DpLaunch {
   // from and joined back into the launch stream by the two events)
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // batches sharing the GPU: the split counts the GPU's issue time this many
+  // times over (the others' work runs beside this batch's)
+  int share = 1;
 };
 // order (may be null): the hits in the order the threads take them, as words
 // whose low 32 bits are hit indices; outputs stay at the hit's own index.

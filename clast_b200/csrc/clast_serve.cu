@@ -257,7 +257,7 @@ int clast_server_create(clast_ctx* ctx, const clast_targets* t, const clast_para
     s->p = *p;
     s->device = ctx->device;
     clast_server_config c = cfg ? *cfg : clast_server_config{};
-    if (c.lanes <= 0) c.lanes = 2;
+    if (c.lanes <= 0) c.lanes = 4;
     if (c.lanes > 16) throw std::invalid_argument("at most 16 lanes");
     if (c.q_vram <= 0) c.q_vram = 2000000;
     if (c.q_ram <= 0) c.q_ram = 32000000;
@@ -278,6 +278,7 @@ int clast_server_create(clast_ctx* ctx, const clast_targets* t, const clast_para
         for (clast_ctx* x : s->ctxs) clast_ctx_destroy(x);
         throw std::runtime_error("cannot create a lane context");
       }
+      lc->dp_share = c.lanes;  // the DP's warp / thread split counts the other lanes' work
       s->ctxs.push_back(lc);
     }
     clast_server* raw = s.get();

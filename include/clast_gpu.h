@@ -308,7 +308,7 @@ int clast_get_stats(const clast_ctx* ctx, clast_stats* out);
  * frees up, so their work overlaps the batches already on the GPU. */
 typedef struct clast_server clast_server;
 typedef struct clast_server_config {
-  int32_t lanes;           /* batches in flight at once; 0: 2                         */
+  int32_t lanes;           /* batches in flight at once; 0: 4                         */
   int32_t q_vram;          /* query window budget (bases, moveQueryWindow); 0: 2 MBase */
   int32_t q_ram;           /* RAM load budget per strand (bases); 0: 32 MBase         */
   int32_t reserved0;
