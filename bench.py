@@ -900,6 +900,10 @@ def main():
         args.no_plain = True  # per-window rebuilds of 3 Gbp of indexes: minutes per step
         args.no_cpu_baseline = True  # one CPU index build of 3 Gbp is far beyond a bounded sample
         args.no_tsv = True  # ~640 M result lines (38 GB of text) per step
+        # served requests here are GPU-throughput-bound (repeat families: ~160
+        # hits per read); fewer batches sharing the GPU finish each sooner
+        if args.serve_lanes == 4:
+            args.serve_lanes = 2
         if args.check == "load0":
             args.check = "off"  # the large-window parity is a test of its own
     if args.impl == "reference":
