@@ -762,7 +762,7 @@ def run_ours(args):
         "roofline": roofline,
         "counts_per_step": {k: st[k] for k in ("query_bases", "query_kmers", "seeds", "hits", "results",
                                                "dp_cells", "index_launches", "map_launches", "index_bases",
-                                               "index_keys")},
+                                               "index_keys", "dp_warp_hits")},
         "clocks": clk.summary(),
         "host_wall_ms_per_step": {"value_loop": hw_dev, "e2e_loop": hw_e2e},
     }
