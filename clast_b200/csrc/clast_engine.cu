@@ -401,7 +401,7 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
   // The longest hits of the order may run one per warp (banded_dp decides
   // from the length buckets, or for equal lengths from the row count).
   const bool uneven = qb.max_len != qb.min_len && H > 1;
-  const int warp_mode = dp_warp_mode_from_env();
+  const int warp_mode = dp_warp_mode_from_env(c->dp_warp);
   DpBuckets buckets;  // of the order last made
   auto make_order = [&](int kind) -> const uint64_t* {
     buckets = DpBuckets();
@@ -435,7 +435,6 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
     m.aux = c->st_dp;
     m.ev_fork = c->ev_dp_fork;
     m.ev_join = c->ev_dp_join;
-    m.share = c->dp_share;
     if (!uneven) m.uniform_rows = std::max(0, qb.max_len - p->lmer);
     return m;
   };
@@ -1415,11 +1414,10 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
       lmax = std::max(lmax, q_lengths[i]);
     }
     DpLaunch m;
-    m.warp = dp_warp_mode_from_env();
+    m.warp = dp_warp_mode_from_env(ctx->dp_warp);
     m.aux = ctx->st_dp;
     m.ev_fork = ctx->ev_dp_fork;
     m.ev_join = ctx->ev_dp_join;
-    m.share = ctx->dp_share;
     if (lmin != lmax && H > 1) {
       uint64_t* ob = ws.get<uint64_t>("h_border", H);
       m.buckets = dp_bucket_order(ws, hs, qlen, H, p->lmer, ob, st);

@@ -199,7 +199,10 @@ struct clast_ctx {
   // kernels on st (forked and joined by these events)
   cudaStream_t st_dp = nullptr;
   cudaEvent_t ev_dp_fork = nullptr, ev_dp_join = nullptr;
-  int dp_share = 1;  // batches sharing the GPU with this context's (a server's lanes)
+  // the DP's warp / thread split when CLAST_DP_WARP does not set it: a
+  // server's lanes run every hit one per thread (under load, other lanes'
+  // work shares the SMs, and one-per-warp hits lost more than they gained)
+  int dp_warp = clast::kDpWarpAuto;
 };
 
 struct clast_index {

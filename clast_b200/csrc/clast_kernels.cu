@@ -2348,20 +2348,19 @@ constexpr long long kDpWarpMinRows = 16;
 
 // Estimated time of the DP with the `s` longest hits (rows summed: sw, the
 // longest r1) one per warp and the rest (rows summed: rest, the longest rn)
-// one per thread, on a GPU shared by `share` such batches.
+// one per thread.
 __host__ __device__ __forceinline__ double dp_split_cycles(int W, long long s, double r1, double sw, double rn,
-                                                           double rest, int share) {
+                                                           double rest) {
   double lat = s > 0 ? r1 * kDpWarpRowCycles : 0.0;
   if (rest > 0) lat = fmax(lat, rn * W * kDpThreadCellCycles);
-  const double issue =
-      share * ((s > 0 ? sw / kDpWarpRowsPerCycle : 0.0) + rest * W / kDpThreadCellsPerCycle);
+  const double issue = (s > 0 ? sw / kDpWarpRowsPerCycle : 0.0) + rest * W / kDpThreadCellsPerCycle;
   return fmax(lat + 0.5 * issue, issue) + (s > 0 ? kDpLaunchCycles : 0.0);
 }
 
 // The split on the device: every bucket boundary (longest first) is a
 // candidate; the earliest estimated end wins.  One thread; ~500 buckets.
 __global__ void k_dp_warp_split(const unsigned int* __restrict__ count, const unsigned long long* __restrict__ rows,
-                                int W, long long cap, int share, long long* __restrict__ warp_n) {
+                                int W, long long cap, long long* __restrict__ warp_n) {
   if (threadIdx.x != 0) return;
   double total = 0;
   for (int b = 0; b < kDpBuckets; ++b) total += (double)rows[b];
@@ -2374,9 +2373,9 @@ __global__ void k_dp_warp_split(const unsigned int* __restrict__ count, const un
     // candidate: the buckets before b one per warp, b and the rest one per thread
     if (r1 < 0) {
       r1 = rn;
-      best = dp_split_cycles(W, 0, 0, 0, rn, total, share);
+      best = dp_split_cycles(W, 0, 0, 0, rn, total);
     } else {
-      const double t = dp_split_cycles(W, s, r1, sw, rn, total - sw, share);
+      const double t = dp_split_cycles(W, s, r1, sw, rn, total - sw);
       if (t < best) { best = t; best_s = s; }
     }
     if (dp_bucket_lo(b) < kDpWarpMinRows || s + count[b] > cap) {
@@ -2386,7 +2385,7 @@ __global__ void k_dp_warp_split(const unsigned int* __restrict__ count, const un
     s += count[b];
     sw += (double)rows[b];
   }
-  if (all_taken && s > 0 && dp_split_cycles(W, s, r1, sw, 0, 0, share) < best) best_s = s;  // every hit one per warp
+  if (all_taken && s > 0 && dp_split_cycles(W, s, r1, sw, 0, 0) < best) best_s = s;  // every hit one per warp
   *warp_n = best_s;
 }
 
@@ -2441,13 +2440,12 @@ long long launch_dp_mode(DpKernelArgs a, const DpLaunch& m, cudaStream_t st) {
     a.warp_fixed = a.n;
   } else if (m.warp == kDpWarpAuto) {
     if (m.buckets.count && m.warp_n) {
-      k_dp_warp_split<<<1, 32, 0, st>>>(m.buckets.count, m.buckets.rows, W, cap, std::max(1, m.share), m.warp_n);
+      k_dp_warp_split<<<1, 32, 0, st>>>(m.buckets.count, m.buckets.rows, W, cap, m.warp_n);
       CLAST_LAUNCHED();
       a.warp_n = m.warp_n;
     } else if (m.uniform_rows >= kDpWarpMinRows && a.n <= cap) {
       const double r = (double)m.uniform_rows, rows = r * (double)a.n;
-      const int sh = std::max(1, m.share);
-      if (dp_split_cycles(W, a.n, r, rows, 0, 0, sh) < dp_split_cycles(W, 0, 0, 0, r, rows, sh)) a.warp_fixed = a.n;
+      if (dp_split_cycles(W, a.n, r, rows, 0, 0) < dp_split_cycles(W, 0, 0, 0, r, rows)) a.warp_fixed = a.n;
     }
   }
   const int64_t rest = a.n - (a.warp_n ? 0 : a.warp_fixed);  // hits left for the one-per-thread kernels (at most)
@@ -2929,12 +2927,12 @@ DpBuckets dp_bucket_order(Workspace& ws, const int32_t* hs, const int32_t* q_len
   return b;
 }
 
-int dp_warp_mode_from_env() {
+int dp_warp_mode_from_env(int fallback) {
   const char* v = std::getenv("CLAST_DP_WARP");
-  if (!v) return kDpWarpAuto;
+  if (!v) return fallback;
   if (!std::strcmp(v, "off")) return kDpWarpOff;
   if (!std::strcmp(v, "all")) return kDpWarpAll;
-  return kDpWarpAuto;
+  return fallback;
 }
 
 long long banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk, const int32_t* hq,

@@ -162,9 +162,6 @@ struct DpLaunch {
   // from and joined back into the launch stream by the two events)
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  // batches sharing the GPU: the split counts the GPU's issue time this many
-  // times over (the others' work runs beside this batch's)
-  int share = 1;
 };
 // order (may be null): the hits in the order the threads take them, as words
 // whose low 32 bits are hit indices; outputs stay at the hit's own index.
@@ -181,8 +178,9 @@ DpBuckets dp_bucket_count(Workspace& ws, const int32_t* hs, const int32_t* q_len
 // instead of a sort (the counts of dp_bucket_count, which it runs).
 DpBuckets dp_bucket_order(Workspace& ws, const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l,
                           uint64_t* order, cudaStream_t st);
-// CLAST_DP_WARP=off|all overrides kDpWarpAuto (for tests and measurements).
-int dp_warp_mode_from_env();
+// CLAST_DP_WARP=off|all, else `fallback` (the environment overrides a
+// context's setting, for tests and measurements).
+int dp_warp_mode_from_env(int fallback);
 // keys[h] = (rows_max - rows of hit h) << 32 | h, rows = q_len[hs[h]] - l + 1:
 // ascending keys take the hits longest first.
 void dp_order_keys(const int32_t* hs, const int32_t* q_len, int64_t n_hits, int l, int rows_max, uint64_t* keys,

@@ -278,7 +278,7 @@ int clast_server_create(clast_ctx* ctx, const clast_targets* t, const clast_para
         for (clast_ctx* x : s->ctxs) clast_ctx_destroy(x);
         throw std::runtime_error("cannot create a lane context");
       }
-      lc->dp_share = c.lanes;  // the DP's warp / thread split counts the other lanes' work
+      lc->dp_warp = clast::kDpWarpOff;  // see clast_ctx::dp_warp
       s->ctxs.push_back(lc);
     }
     clast_server* raw = s.get();
