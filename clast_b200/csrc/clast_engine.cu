@@ -199,6 +199,8 @@ clast_index* make_index(clast_ctx* c, const clast_params* p, const char* bases, 
 }
 
 // Device-resident query strands of one batch, packed once for every index.
+struct QueryRef;
+
 struct QueryBatch {
   DevArray<char> bases;  // padded
   int64_t n = 0;
@@ -225,7 +227,29 @@ struct QueryBatch {
     nmask.alloc((size_t)(n / 64 + 4));
     pack_bases(bases.p + kPad, n, packed.p, nmask.p, st);
   }
+  QueryRef ref() const;
 };
+
+// A query batch as the seeding and search stages read it, without ownership
+// (a QueryBatch, or clast_search_noalloc's buffers in its fixed scratch).
+struct QueryRef {
+  QueryView q;
+  int64_t n = 0;                     // bases of the strands
+  const int32_t* wstart = nullptr;   // strand where each query window starts, plus the end
+  int32_t nwin = 0;
+  int32_t min_len = 0, max_len = 0;  // strand lengths (the DP orders hits by rows when they differ)
+};
+
+QueryRef QueryBatch::ref() const {
+  QueryRef r;
+  r.q = view();
+  r.n = n;
+  r.wstart = wstart.p;
+  r.nwin = nwin;
+  r.min_len = min_len;
+  r.max_len = max_len;
+  return r;
+}
 
 // Host copy of one batch's result (reference order within each query window).
 // One batch's hits on the device, reads ascending (reference order within
@@ -256,11 +280,11 @@ struct SeedSet {
 // windows are issued together.  A window whose seed partition overflowed is
 // seeded again (alone with the others that overflowed) with partitions sized
 // from the exact counts.
-void seed_windows(clast_ctx* c, const clast_params* p, const QueryBatch& qb, std::vector<SeedSet>& sets) {
+void seed_windows(clast_ctx* c, const clast_params* p, const QueryRef& qb, std::vector<SeedSet>& sets) {
   cudaStream_t st = c->st;
   Workspace& ws = c->ws;
-  const QueryView q = qb.view();
-  const int64_t ns = qb.nstrands;
+  const QueryView q = qb.q;
+  const int64_t ns = q.nstrands;
   const int parts = seed_parts();
   StageTimer& tm = c->timer;
   std::vector<int> todo;
@@ -324,17 +348,39 @@ void seed_windows(clast_ctx* c, const clast_params* p, const QueryBatch& qb, std
   if (!todo.empty()) throw std::runtime_error("seed partitions overflowed twice");
 }
 
+// Where search_seeded puts a window's final hits: take(F, foff, nr) returns
+// the arrays for its F hits (and may keep the nr + 1 per-read offsets), or
+// throws when they do not fit.
+struct HitSink {
+  virtual ~HitSink() = default;
+  virtual FinalOut take(int64_t F, const int64_t* foff, int64_t nr, cudaStream_t st) = 0;
+};
+
+// Device arrays of their own, with the per-read offsets (clast_search,
+// clast_map).
+struct DevHitsSink : HitSink {
+  DevHits& out;
+  explicit DevHitsSink(DevHits& o) : out(o) { out = DevHits(); }
+  FinalOut take(int64_t F, const int64_t* foff, int64_t nr, cudaStream_t st) override {
+    out.n = F;
+    out.t_id.alloc(F); out.t_idx.alloc(F); out.q_id.alloc(F); out.q_idx.alloc(F); out.t_len.alloc(F);
+    out.q_len.alloc(F); out.match.alloc(F); out.score.alloc(F); out.evalue.alloc(F);
+    out.foff.alloc(nr + 1);
+    CLAST_CK(cudaMemcpyAsync(out.foff.p, foff, (nr + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
+    return FinalOut{out.t_id.p, out.t_idx.p, out.q_id.p, out.q_idx.p, out.t_len.p, out.q_len.p, out.match.p,
+                    out.score.p, out.evalue.p};
+  }
+};
+
 // CDeviceHitList for every query window of `qb` against the window whose
 // seeds are in z: seed filters, DP, result order.
-void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, int32_t q_first, SeedSet& z,
-                   DevHits& out) {
+int64_t search_seeded(clast_ctx* c, Workspace& ws, const clast_params* p, const QueryRef& qb, int32_t q_first,
+                      SeedSet& z, bool tune, HitSink& sink) {
   cudaStream_t st = c->st;
-  Workspace& ws = c->ws;
   const clast_index* ix = z.ix;
-  const QueryView q = qb.view();
+  const QueryView q = qb.q;
   const TargetView tv = ix->tview();
-  const int64_t ns = qb.nstrands, nr = ns / 2;
-  out = DevHits();
+  const int64_t ns = q.nstrands, nr = ns / 2;
   StageTimer& tm = c->timer;
   const int64_t S = z.S;
   int64_t* off = z.off;
@@ -357,14 +403,14 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
   c->stats.seeds += S;
   if (S == 0) {
     add_counters();
-    return;
+    return 0;
   }
   int32_t* wfirst = ws.get<int32_t>("s_wfirst", qb.nwin);
-  window_first(nvalid, qb.wstart.p, qb.nwin, wfirst, st);
+  window_first(nvalid, qb.wstart, qb.nwin, wfirst, st);
   // sortSeeds, deletingIsolateSeeds, deleteDuplicateSeeds
   tm.begin(st);
   int32_t* hcnt = ws.get<int32_t>("s_hcnt", ns);
-  seed_sort_filter(ws, skey, sq, off, len32, nvalid, qb.wstart.p, qb.nwin, wfirst, p->width, p->gap, ns, hcnt, st);
+  seed_sort_filter(ws, skey, sq, off, len32, nvalid, qb.wstart, qb.nwin, wfirst, p->width, p->gap, ns, hcnt, st);
   tm.end(StageTimer::SORT, st, 4);
   int64_t* hoff = ws.get<int64_t>("s_hoff", ns + 1);
   scan_i32(ws, hcnt, ns, hoff, st);
@@ -373,12 +419,12 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
   c->stats.hits += H;
   if (H == 0) {
     add_counters();
-    return;
+    return 0;
   }
   uint64_t* hk = ws.get<uint64_t>("h_key", H);
   int32_t* hq = ws.get<int32_t>("h_q", H);
   int32_t* hs = ws.get<int32_t>("h_s", H);
-  gather_hits(skey, sq, off, hcnt, hoff, ns, hk, hq, hs, qb.len.p, p->lmer, 2 * p->gap + 1, counters + 1, st);
+  gather_hits(skey, sq, off, hcnt, hoff, ns, hk, hq, hs, q.len, p->lmer, 2 * p->gap + 1, counters + 1, st);
   // alignmentHits + calculateEvalue + deleteHits_lowEValue / _tooShort
   DpOut o;
   o.t_idx = ws.get<int32_t>("d_tidx", H);
@@ -412,13 +458,13 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
       while ((1ll << bits) <= rows_max) ++bits;
       uint64_t* ok = ws.get<uint64_t>("h_order", H);
       uint64_t* ok2 = ws.get<uint64_t>("h_order2", H);
-      dp_order_keys(hs, qb.len.p, H, p->lmer, rows_max, ok, st);
+      dp_order_keys(hs, q.len, H, p->lmer, rows_max, ok, st);
       const uint64_t* sorted = radix_sort_u64(ws, ok, nullptr, ok2, nullptr, H, 32, 32 + bits, st) ? ok2 : ok;
-      if (warp_mode == kDpWarpAuto) buckets = dp_bucket_count(ws, hs, qb.len.p, H, p->lmer, st);
+      if (warp_mode == kDpWarpAuto) buckets = dp_bucket_count(ws, hs, q.len, H, p->lmer, st);
       return sorted;
     }
     uint64_t* ob = ws.get<uint64_t>("h_border", H);
-    buckets = dp_bucket_order(ws, hs, qb.len.p, H, p->lmer, ob, st);
+    buckets = dp_bucket_order(ws, hs, q.len, H, p->lmer, ob, st);
     return ob;
   };
   unsigned long long* dp_head = ws.get<unsigned long long>("dp_head", 1);
@@ -440,7 +486,7 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
   };
   const int tune_key = (p->gap << 2) | (p->local ? 2 : 0) | (uneven ? 1 : 0);
   auto it = c->dp_tuned.find(tune_key);
-  if (it == c->dp_tuned.end() && H >= kDpTuneHits && !std::getenv("CLAST_DP_NO_TUNE")) {
+  if (tune && it == c->dp_tuned.end() && H >= kDpTuneHits && !std::getenv("CLAST_DP_NO_TUNE")) {
     std::vector<DpChoice> cands;
     for (int ord : (uneven ? std::vector<int>{1, 2} : std::vector<int>{0}))
       for (int q_ : {0, 1})
@@ -494,26 +540,21 @@ void search_seeded(clast_ctx* c, const clast_params* p, const QueryBatch& qb, in
   const int64_t F = read_scalar(foff + nr, st);
   c->stats.results += F;
   add_counters();
-  if (F == 0) return;
-  out.n = F;
-  out.t_id.alloc(F); out.t_idx.alloc(F); out.q_id.alloc(F); out.q_idx.alloc(F); out.t_len.alloc(F);
-  out.q_len.alloc(F); out.match.alloc(F); out.score.alloc(F); out.evalue.alloc(F);
-  out.foff.alloc(nr + 1);
-  CLAST_CK(cudaMemcpyAsync(out.foff.p, foff, (nr + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
-  FinalOut fo{out.t_id.p, out.t_idx.p, out.q_id.p, out.q_idx.p, out.t_len.p, out.q_len.p, out.match.p,
-              out.score.p, out.evalue.p};
+  if (F == 0) return 0;
+  const FinalOut fo = sink.take(F, foff, nr, st);
   final_compact(fsel, roff, fcnt, foff, nr, hk, hs, o, ix->t_begin, q_first, fo, st);
+  return F;
 }
 
 // CDeviceHitList for every query window of `qb` against one index.
-void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, const QueryBatch& qb,
+void search_batch(clast_ctx* c, const clast_index* ix, const clast_params* p, const QueryRef& qb,
                   int32_t q_first, DevHits& out) {
-  out = DevHits();
-  if (qb.nstrands == 0 || ix->n_keys == 0) return;
+  DevHitsSink sink(out);
+  if (qb.q.nstrands == 0 || ix->n_keys == 0) return;
   std::vector<SeedSet> sets(1);
   sets[0].ix = ix;
   seed_windows(c, p, qb, sets);
-  search_seeded(c, p, qb, q_first, sets[0], out);
+  search_seeded(c, c->ws, p, qb, q_first, sets[0], true, sink);
 }
 
 template <class T>
@@ -727,7 +768,7 @@ int clast_search(clast_ctx* ctx, const clast_index* ix, const clast_params* p, c
     CLAST_CK(cudaMemcpyAsync(qb.wstart.p, ws2, sizeof(ws2), cudaMemcpyHostToDevice, st));
     qb.pack(st);
     DevHits h;
-    search_batch(ctx, ix, p, qb, q_begin, h);
+    search_batch(ctx, ix, p, qb.ref(), q_begin, h);
     const int64_t F = h.n;
     out->n = F;
     auto d2h32 = [&](int32_t*& dst, const DevArray<int32_t>& src) {
@@ -1030,6 +1071,7 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
     CLAST_CK(cudaStreamWaitEvent(st, T->ev_done, 0));
     // every target window, in holder order (target load, window)
     std::vector<DevHits> per_win(T->wins.size());
+    const QueryRef qr = qb.ref();
     // windows seeded per pass over the query (CLAST_SEED_WINDOWS, 1..4)
     int group = 2;
     if (const char* e = std::getenv("CLAST_SEED_WINDOWS")) group = std::max(1, std::min(kMaxSeedWins, std::atoi(e)));
@@ -1038,14 +1080,17 @@ static int map_impl(clast_ctx* ctx, const clast_targets* T, const clast_params* 
       std::vector<size_t> idx;
       for (size_t w = g0; w < std::min(T->wins.size(), g0 + (size_t)group); ++w) {
         const clast_index* ix = T->wins[w].ix.get();
-        if (qb.nstrands == 0 || ix->n_keys == 0) continue;
+        if (qr.q.nstrands == 0 || ix->n_keys == 0) continue;
         sets.emplace_back();
         sets.back().ix = ix;
         idx.push_back(w);
       }
       if (sets.empty()) continue;
-      seed_windows(ctx, p, qb, sets);
-      for (size_t j = 0; j < sets.size(); ++j) search_seeded(ctx, p, qb, 0, sets[j], per_win[idx[j]]);
+      seed_windows(ctx, p, qr, sets);
+      for (size_t j = 0; j < sets.size(); ++j) {
+        DevHitsSink sink(per_win[idx[j]]);
+        search_seeded(ctx, ctx->ws, p, qr, 0, sets[j], true, sink);
+      }
     }
     // fixResult: stable merge by (read, score desc) over the windows, on the device
     std::vector<WinHits> wh;
@@ -1211,9 +1256,10 @@ int clast_last_map_stats(const clast_ctx* ctx, double* device_ms, int64_t* kerne
 
 // ----------------------------------------------------------------------------
 // clast_search_noalloc: clast_search on a fixed scratch buffer, allocating
-// nothing.  The stage sequence is search_batch's for one query window; every
-// device buffer is a slot of the static scratch (Workspace arena mode) and
-// the hits go straight into the caller's host arrays.
+// nothing.  It seeds the one query window itself (partitions sized to fit
+// the scratch), then runs search_seeded, the stages clast_search runs, with
+// every device buffer a slot of the static scratch (Workspace arena mode);
+// the hits go from scratch slots straight into the caller's host arrays.
 // ----------------------------------------------------------------------------
 namespace {
 
@@ -1380,78 +1426,52 @@ extern "C" int clast_search_noalloc(clast_ctx* ctx, const clast_index* ix, const
       part_cap = most;
     }
     if (S == 0) return finish(0);
-    int32_t* wfirst = ws.get<int32_t>("s_wfirst", 1);
-    window_first(nvalid, wstart, 1, wfirst, st);
-    // sortSeeds, deletingIsolateSeeds, deleteDuplicateSeeds
-    int32_t* hcnt = ws.get<int32_t>("s_hcnt", ns);
-    seed_sort_filter(ws, skey, sq, off, len32, nvalid, wstart, 1, wfirst, p->width, p->gap, ns, hcnt, st);
-    int64_t* hoff = ws.get<int64_t>("s_hoff", ns + 1);
-    scan_i32(ws, hcnt, ns, hoff, st);
-    const int64_t H = read_scalar(hoff + ns, st);
-    if (H == 0) return finish(0);
-    uint64_t* hk = ws.get<uint64_t>("h_key", H);
-    int32_t* hq = ws.get<int32_t>("h_q", H);
-    int32_t* hs = ws.get<int32_t>("h_s", H);
-    gather_hits(skey, sq, off, hcnt, hoff, ns, hk, hq, hs, qlen, p->lmer, 2 * p->gap + 1, counters + 1, st);
-    // alignmentHits + calculateEvalue + deleteHits_lowEValue / _tooShort
-    DpOut o;
-    o.t_idx = ws.get<int32_t>("d_tidx", H);
-    o.q_idx = ws.get<int32_t>("d_qidx", H);
-    o.t_len = ws.get<int32_t>("d_tlen", H);
-    o.q_len = ws.get<int32_t>("d_qlen", H);
-    o.match = ws.get<int32_t>("d_match", H);
-    o.score = ws.get<int32_t>("d_score", H);
-    o.evalue = ws.get<double>("d_e", H);
-    o.keep = ws.get<uint8_t>("d_keep", H);
-    DpParams dp{p->lmer, p->stride, p->gap, p->local, p->cutoff, p->total_db, p->K, p->lambda};
-    // reads of different lengths: hits longest first (length buckets), as clast_search
-    // orders them, so that a warp's hits have about the same number of rows
-    // (and the longest one per warp, as there)
-    const uint64_t* order = nullptr;
+    // the stages after seeding are clast_search's, on the fixed scratch (no
+    // autotuner runs: its trial orders would need more of it); the hits go
+    // to slots of the scratch, then to the caller's arrays
     int32_t lmin = INT32_MAX, lmax = 0;
     for (int32_t i = 0; i < n_qseqs; ++i) {
       lmin = std::min(lmin, q_lengths[i]);
       lmax = std::max(lmax, q_lengths[i]);
     }
-    DpLaunch m;
-    m.warp = dp_warp_mode_from_env(ctx->dp_warp);
-    m.aux = ctx->st_dp;
-    m.ev_fork = ctx->ev_dp_fork;
-    m.ev_join = ctx->ev_dp_join;
-    if (lmin != lmax && H > 1) {
-      uint64_t* ob = ws.get<uint64_t>("h_border", H);
-      m.buckets = dp_bucket_order(ws, hs, qlen, H, p->lmer, ob, st);
-      m.warp_n = ws.get<long long>("dp_warp_n", 1);
-      order = ob;
-    } else {
-      m.uniform_rows = std::max(0, lmax - p->lmer);
-    }
-    banded_dp(tv, q, hk, hq, hs, order, H, dp, o, st, m);
-    // resultSorting + deleteHits_duplicateResult, per read
-    uint64_t* k1 = ws.get<uint64_t>("f_k1", H);
-    uint64_t* k2 = ws.get<uint64_t>("f_k2", H);
-    int32_t* idx = ws.get<int32_t>("f_idx", H);
-    final_keys(hk, hq, hs, o, H, k1, k2, idx, st);
-    int64_t* roff = ws.get<int64_t>("f_roff", nr);
-    int32_t* rlen = ws.get<int32_t>("f_rlen", nr);
-    read_ranges(hoff, nr, roff, rlen, st);
-    segmented_sort_u64(ws, k1, k2, idx, roff, rlen, nr, st, 1);
-    int32_t* fcnt = ws.get<int32_t>("f_cnt", nr);
-    int32_t* fsel = ws.get<int32_t>("f_sel", H);
-    final_dedupe(k1, k2, idx, hk, hs, o, roff, rlen, nr, fcnt, fsel, st);
-    int64_t* foff = ws.get<int64_t>("f_off", nr + 1);
-    scan_i32(ws, fcnt, nr, foff, st);
-    const int64_t F = read_scalar(foff + nr, st);
-    if (F > capacity) {
-      out->n = F;
-      throw std::invalid_argument("window has " + std::to_string(F) + " hits, capacity is " +
-                                  std::to_string(capacity));
-    }
+    QueryRef qr;
+    qr.q = q;
+    qr.n = n;
+    qr.wstart = wstart;
+    qr.nwin = 1;
+    qr.min_len = lmin;
+    qr.max_len = lmax;
+    SeedSet z;
+    z.ix = ix;
+    z.off = off;
+    z.len32 = len32;
+    z.nvalid = nvalid;
+    z.counters = counters;
+    z.skey = skey;
+    z.sq = sq;
+    z.part_cap = part_cap;
+    z.S = S;
+    struct ArenaSink : HitSink {
+      Workspace& ws;
+      int64_t capacity;
+      clast_hits* out;
+      FinalOut fo{};
+      ArenaSink(Workspace& w, int64_t cap, clast_hits* o) : ws(w), capacity(cap), out(o) {}
+      FinalOut take(int64_t F, const int64_t*, int64_t, cudaStream_t) override {
+        if (F > capacity) {
+          out->n = F;
+          throw std::invalid_argument("window has " + std::to_string(F) + " hits, capacity is " +
+                                      std::to_string(capacity));
+        }
+        fo = FinalOut{ws.get<int32_t>("o_tid", F), ws.get<int32_t>("o_tidx", F), ws.get<int32_t>("o_qid", F),
+                      ws.get<int32_t>("o_qidx", F), ws.get<int32_t>("o_tlen", F), ws.get<int32_t>("o_qlen", F),
+                      ws.get<int32_t>("o_match", F), ws.get<int32_t>("o_score", F), ws.get<double>("o_e", F)};
+        return fo;
+      }
+    } sink(ws, capacity, out);
+    const int64_t F = search_seeded(ctx, ws, p, qr, q_begin, z, false, sink);
     if (F == 0) return finish(0);
-    FinalOut fo{ws.get<int32_t>("o_tid", F), ws.get<int32_t>("o_tidx", F), ws.get<int32_t>("o_qid", F),
-                ws.get<int32_t>("o_qidx", F), ws.get<int32_t>("o_tlen", F), ws.get<int32_t>("o_qlen", F),
-                ws.get<int32_t>("o_match", F), ws.get<int32_t>("o_score", F), ws.get<double>("o_e", F)};
-    final_compact(fsel, roff, fcnt, foff, nr, hk, hs, o, ix->t_begin, q_begin, fo, st);
+    const FinalOut& fo = sink.fo;
     int32_t* const dst[8] = {out->t_id, out->t_idx, out->q_id, out->q_idx, out->t_len, out->q_len, out->match,
                              out->score};
     const int32_t* const src[8] = {fo.t_id, fo.t_idx, fo.q_id, fo.q_idx, fo.t_len, fo.q_len, fo.match, fo.score};
