@@ -1558,11 +1558,13 @@ __device__ __forceinline__ void filter_chunk(int c0, int n, uint64_t k, uint32_t
   }
 }
 
-// Seed-sort tiers by a strand's seed count: <= 32 (one warp, registers),
-// <= kWarpSmemCap (one warp, shared memory), <= kCtaSortCap (one CTA, shared
-// memory), longer (one CTA, global memory).  List entries are the strand index
-// with the window-first flag in bit 31.
-constexpr int kSortTiers = 4;
+// Seed-sort tiers by a strand's seed count: <= kThreadSortCap (one thread,
+// registers; most strands hold a few chance seeds), <= 32 (one warp,
+// registers), <= kWarpSmemCap (one warp, shared memory), <= kCtaSortCap (one
+// CTA, shared memory), longer (one CTA, global memory).  List entries are the
+// strand index with the window-first flag in bit 31.
+constexpr int kSortTiers = 5;
+constexpr int kThreadSortCap = 8;
 constexpr int kWarpSmemCap = 256;
 constexpr uint32_t kWinFirstBit = 0x80000000u;
 
@@ -1570,7 +1572,12 @@ __global__ void k_seed_classify(SeedFilterCtx c, int64_t ns, int32_t* __restrict
                                 int32_t* __restrict__ counts) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int n = (i < ns && c.nvalid[i] > 0) ? c.cnt[i] : 0;
-  const int tier = (n <= 0) ? -1 : (n <= 32 ? 0 : (n <= kWarpSmemCap ? 1 : (n <= kCtaSortCap ? 2 : 3)));
+  const int tier = (n <= 0)                ? -1
+                 : (n <= kThreadSortCap) ? 0
+                 : (n <= 32)             ? 1
+                 : (n <= kWarpSmemCap)   ? 2
+                 : (n <= kCtaSortCap)    ? 3
+                                         : 4;
   const int lane = threadIdx.x & 31;
   const uint32_t entry = (uint32_t)i | ((tier >= 0 && window_first_strand(i, c)) ? kWinFirstBit : 0u);
 #pragma unroll
@@ -1591,6 +1598,68 @@ __device__ __forceinline__ void warp_cx(uint64_t& a1, uint32_t& a2, int lane, in
   const uint32_t b2 = __shfl_sync(kFull, a2, partner);
   const bool b_less = less2(b1, b2, a1, a2);
   if (lane < partner ? b_less : !b_less && (b1 != a1 || b2 != a2)) { a1 = b1; a2 = b2; }
+}
+
+// 1..kThreadSortCap seeds: one thread per strand.  The seeds (padded with
+// keys above every seed) go through an odd-even transposition network in
+// registers unless they already ascend, then the isolate and duplicate
+// filters run in seed order, as filter_chunk applies them to a warp's chunk:
+// a seed survives the isolate filter when it is near its predecessor (the
+// strand's first seed only when the strand is its window's first), and the
+// duplicate filter then drops it when it is near the previous seed that
+// survived the isolate filter.
+__global__ void k_seed_sort_filter_thread(uint64_t* __restrict__ skey, uint32_t* __restrict__ sq, SeedFilterCtx c,
+                                          const int32_t* __restrict__ list, const int32_t* __restrict__ count) {
+  const int total = *count;
+  for (int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; li < total;
+       li += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t e = (uint32_t)list[li];
+    const int s = (int)(e & ~kWinFirstBit);
+    const int64_t o = c.off[s];
+    const int n = c.cnt[s];
+    uint64_t k[kThreadSortCap];
+    uint32_t q[kThreadSortCap];
+    bool sorted = true;
+#pragma unroll
+    for (int i = 0; i < kThreadSortCap; ++i) {
+      k[i] = i < n ? skey[o + i] : ~0ull;
+      q[i] = i < n ? sq[o + i] : ~0u;
+      if (i > 0 && less2(k[i], q[i], k[i - 1], q[i - 1])) sorted = false;
+    }
+    if (!sorted) {
+#pragma unroll
+      for (int pass = 0; pass < kThreadSortCap; ++pass)
+#pragma unroll
+        for (int i = pass & 1; i + 1 < kThreadSortCap; i += 2)
+          if (less2(k[i + 1], q[i + 1], k[i], q[i])) {
+            const uint64_t tk = k[i]; k[i] = k[i + 1]; k[i + 1] = tk;
+            const uint32_t tq = q[i]; q[i] = q[i + 1]; q[i + 1] = tq;
+          }
+    }
+    const bool wf = (e & kWinFirstBit) != 0;
+    int ptid = 0, ptidx = 0, pdiag = 0;  // previous seed
+    int stid = 0, stidx = 0, sdiag = 0;  // previous isolate-filter survivor
+    bool have = false;
+    int64_t out = o;
+#pragma unroll
+    for (int j = 0; j < kThreadSortCap; ++j) {
+      if (j < n) {
+        const int tid = (int)(k[j] >> 32);
+        const int diag = (int)((uint32_t)k[j] ^ 0x80000000u);
+        const int tidx = diag + (int)q[j];
+        const bool k8 = (j == 0) ? wf : near_pred(tid, tidx, diag, ptid, ptidx, pdiag, c.width, c.gap);
+        const bool k9 = k8 && !(have && near_pred(tid, tidx, diag, stid, stidx, sdiag, c.width, c.gap));
+        if (k9) {
+          skey[out] = k[j];
+          sq[out] = q[j];
+          ++out;
+        }
+        if (k8) { stid = tid; stidx = tidx; sdiag = diag; have = true; }
+        ptid = tid; ptidx = tidx; pdiag = diag;
+      }
+    }
+    c.hcnt[s] = (int32_t)(out - o);
+  }
 }
 
 // <= 32 seeds: one warp sorts in registers (network sized to the count,
@@ -2861,16 +2930,19 @@ void seed_sort_filter(Workspace& ws, uint64_t* skey, uint32_t* sq, const int64_t
   CLAST_CK(cudaMemsetAsync(hcnt, 0, nstrands * sizeof(int32_t), st));
   k_seed_classify<<<blocks_for(nstrands, 256), 256, 0, st>>>(c, nstrands, lists, counts);
   CLAST_LAUNCHED();
-  k_seed_sort_filter_warp<<<grid_cap((nstrands * 32 + 255) / 256), 256, 0, st>>>(skey, sq, c, lists, counts);
+  k_seed_sort_filter_thread<<<grid_cap((nstrands + 255) / 256), 256, 0, st>>>(skey, sq, c, lists, counts);
+  CLAST_LAUNCHED();
+  k_seed_sort_filter_warp<<<grid_cap((nstrands * 32 + 255) / 256), 256, 0, st>>>(skey, sq, c, lists + nstrands,
+                                                                                counts + 1);
   CLAST_LAUNCHED();
   k_seed_sort_filter_warp_smem<<<grid_cap(std::min<int64_t>(nstrands, 65536) * 32 / kWarpSmemThreads + 1),
-                                 kWarpSmemThreads, 0, st>>>(skey, sq, c, lists + nstrands, counts + 1);
+                                 kWarpSmemThreads, 0, st>>>(skey, sq, c, lists + 2 * nstrands, counts + 2);
   CLAST_LAUNCHED();
   k_seed_sort_filter_cta<<<grid_cap(nstrands < 4096 ? nstrands : 4096), 256, 0, st>>>(skey, sq, c,
-                                                                                     lists + 2 * nstrands, counts + 2);
+                                                                                     lists + 3 * nstrands, counts + 3);
   CLAST_LAUNCHED();
   k_seed_sort_filter_global<<<grid_cap(nstrands < 1024 ? nstrands : 1024), 1024, 0, st>>>(
-      skey, sq, c, lists + 3 * nstrands, counts + 3);
+      skey, sq, c, lists + 4 * nstrands, counts + 4);
   CLAST_LAUNCHED();
 }
 
