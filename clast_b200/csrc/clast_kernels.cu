@@ -1310,22 +1310,68 @@ __device__ __forceinline__ bool less2(uint64_t a1, K2 a2, uint64_t b1, K2 b2) {
   return a1 < b1 || (a1 == b1 && a2 < b2);
 }
 
+// Segments of 2..kThreadSegCap items are sorted one per thread (most reads
+// have one or two hits), up to 32 one per warp, up to 2048 per CTA, longer
+// in global memory.
+constexpr int kThreadSegCap = 8, kSegTiers = 4;
+
 template <class K2, bool PAY>
 __global__ void k_classify(const int32_t* __restrict__ len, int64_t nseg, int32_t* __restrict__ lists,
                            int32_t* __restrict__ counts) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int n = (i < nseg) ? len[i] : 0;
-  const int tier = (n <= 1) ? -1 : ((n <= 32) ? 0 : (n <= 2048 ? 1 : 2));
+  const int tier = (n <= 1) ? -1 : (n <= kThreadSegCap ? 0 : ((n <= 32) ? 1 : (n <= 2048 ? 2 : 3)));
   const int lane = threadIdx.x & 31;
   // one atomic per warp and tier
 #pragma unroll
-  for (int t = 0; t < 3; ++t) {
+  for (int t = 0; t < kSegTiers; ++t) {
     const unsigned m = __ballot_sync(kFull, tier == t);
     if (!m) continue;
     int base = 0;
     if (lane == __ffs(m) - 1) base = atomicAdd(&counts[t], __popc(m));
     base = __shfl_sync(kFull, base, __ffs(m) - 1);
     if (tier == t) lists[(int64_t)t * nseg + base + __popc(m & lanemask_lt())] = (int32_t)i;
+  }
+}
+
+// 2..kThreadSegCap items: one thread per segment, an odd-even transposition
+// network in registers over the segment's own items only (a compare-exchange
+// past its end is skipped, so nothing but its items moves).
+template <class K2, bool PAY>
+__global__ void k_sort_thread(uint64_t* __restrict__ k1, K2* __restrict__ k2, int32_t* __restrict__ pay,
+                              const int64_t* __restrict__ off, const int32_t* __restrict__ len,
+                              const int32_t* __restrict__ list, const int32_t* __restrict__ count) {
+  const int total = *count;
+  for (int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; li < total;
+       li += (int64_t)gridDim.x * blockDim.x) {
+    const int seg = list[li];
+    const int64_t o = off[seg];
+    const int n = len[seg];
+    uint64_t a[kThreadSegCap];
+    K2 b[kThreadSegCap];
+    int32_t p[kThreadSegCap];
+#pragma unroll
+    for (int i = 0; i < kThreadSegCap; ++i) {
+      a[i] = i < n ? k1[o + i] : 0ull;
+      b[i] = i < n ? k2[o + i] : (K2)0;
+      p[i] = (PAY && i < n) ? pay[o + i] : 0;
+    }
+#pragma unroll
+    for (int pass = 0; pass < kThreadSegCap; ++pass)
+#pragma unroll
+      for (int i = pass & 1; i + 1 < kThreadSegCap; i += 2)
+        if (i + 1 < n && less2(a[i + 1], b[i + 1], a[i], b[i])) {
+          const uint64_t ta = a[i]; a[i] = a[i + 1]; a[i + 1] = ta;
+          const K2 tb = b[i]; b[i] = b[i + 1]; b[i + 1] = tb;
+          const int32_t tp = p[i]; p[i] = p[i + 1]; p[i + 1] = tp;
+        }
+#pragma unroll
+    for (int i = 0; i < kThreadSegCap; ++i)
+      if (i < n) {
+        k1[o + i] = a[i];
+        k2[o + i] = b[i];
+        if (PAY) pay[o + i] = p[i];
+      }
   }
 }
 
@@ -1457,18 +1503,21 @@ void seg_sort(Workspace& ws, uint64_t* k1, K2* k2, int32_t* pay, const int64_t* 
               int64_t nseg, cudaStream_t st, int tag) {
   if (nseg <= 0) return;
   const std::string t = "segsort" + std::to_string(tag);
-  int32_t* lists = ws.get<int32_t>(t + "l", 3 * nseg);
-  int32_t* counts = ws.get<int32_t>(t + "c", 3);
-  CLAST_CK(cudaMemsetAsync(counts, 0, 3 * sizeof(int32_t), st));
+  int32_t* lists = ws.get<int32_t>(t + "l", kSegTiers * nseg);
+  int32_t* counts = ws.get<int32_t>(t + "c", kSegTiers);
+  CLAST_CK(cudaMemsetAsync(counts, 0, kSegTiers * sizeof(int32_t), st));
   k_classify<K2, PAY><<<blocks_for(nseg, 256), 256, 0, st>>>(len, nseg, lists, counts);
   CLAST_LAUNCHED();
-  k_sort_warp<K2, PAY><<<grid_cap((nseg * 32 + 255) / 256), 256, 0, st>>>(k1, k2, pay, off, len, lists, counts);
+  k_sort_thread<K2, PAY><<<grid_cap((nseg + 255) / 256), 256, 0, st>>>(k1, k2, pay, off, len, lists, counts);
   CLAST_LAUNCHED();
-  k_sort_cta<K2, PAY><<<grid_cap(nseg < 4096 ? nseg : 4096), 256, 0, st>>>(k1, k2, pay, off, len, lists + nseg,
-                                                                           counts + 1);
+  k_sort_warp<K2, PAY><<<grid_cap((nseg * 32 + 255) / 256), 256, 0, st>>>(k1, k2, pay, off, len, lists + nseg,
+                                                                          counts + 1);
+  CLAST_LAUNCHED();
+  k_sort_cta<K2, PAY><<<grid_cap(nseg < 4096 ? nseg : 4096), 256, 0, st>>>(k1, k2, pay, off, len, lists + 2 * nseg,
+                                                                           counts + 2);
   CLAST_LAUNCHED();
   k_sort_global<K2, PAY><<<grid_cap(nseg < 1024 ? nseg : 1024), 1024, 0, st>>>(k1, k2, pay, off, len,
-                                                                                lists + 2 * nseg, counts + 2);
+                                                                                lists + 3 * nseg, counts + 3);
   CLAST_LAUNCHED();
 }
 
