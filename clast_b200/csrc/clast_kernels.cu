@@ -1651,8 +1651,10 @@ __device__ __forceinline__ void warp_cx(uint64_t& a1, uint32_t& a2, int lane, in
 
 // 1..kThreadSortCap seeds: one thread per strand.  The seeds (padded with
 // keys above every seed) go through an odd-even transposition network in
-// registers unless they already ascend, then the isolate and duplicate
-// filters run in seed order, as filter_chunk applies them to a warp's chunk:
+// registers unless they already ascend; the strand's nvalid valid seeds then
+// come first (seeds the boundary filters dropped hold kDroppedSeed, above
+// every valid key) and only they are filtered, in seed order, as
+// filter_chunk applies the filters to a warp's chunk:
 // a seed survives the isolate filter when it is near its predecessor (the
 // strand's first seed only when the strand is its window's first), and the
 // duplicate filter then drops it when it is near the previous seed that
@@ -1666,6 +1668,7 @@ __global__ void k_seed_sort_filter_thread(uint64_t* __restrict__ skey, uint32_t*
     const int s = (int)(e & ~kWinFirstBit);
     const int64_t o = c.off[s];
     const int n = c.cnt[s];
+    const int nv = c.nvalid[s];
     uint64_t k[kThreadSortCap];
     uint32_t q[kThreadSortCap];
     bool sorted = true;
@@ -1692,7 +1695,7 @@ __global__ void k_seed_sort_filter_thread(uint64_t* __restrict__ skey, uint32_t*
     int64_t out = o;
 #pragma unroll
     for (int j = 0; j < kThreadSortCap; ++j) {
-      if (j < n) {
+      if (j < nv) {
         const int tid = (int)(k[j] >> 32);
         const int diag = (int)((uint32_t)k[j] ^ 0x80000000u);
         const int tidx = diag + (int)q[j];

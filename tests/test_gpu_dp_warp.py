@@ -134,3 +134,23 @@ def test_whole_job_split_matches_thread_kernel(engine):
     for mode in (None, "all"):
         for f in api.MAP_FIELDS:
             assert np.array_equal(out[mode][f], out["off"][f]), (mode, f)
+
+
+@pytest.mark.parametrize("lmer,gap,local", [(15, 8, 0), (15, 8, 1), (8, 4, 0), (11, 16, 0)])
+def test_hits_entering_the_dp_equal_oracle(engine, lmer, gap, local):
+    """The number of hits the seed filters pass to the DP equals the oracle's
+    count after its isolate and duplicate filters: reads at both ends of every
+    contig make the boundary filters drop seeds (stored as sentinels that
+    sort last and are never filtered), and strands of every seed-count tier
+    (one thread, one warp, shared memory) occur."""
+    s, tl, ql = uneven_case(500 + lmer + gap + local, api.Setting(lmer=lmer, stride=2, gap=gap, local=local))
+    tbases, tgw, tln = tl.window(0, len(tl.lengths))
+    qbases, qgw, qln = ql.window(0, len(ql.lengths))
+    want = O.window_search(s, tbases, tgw, tln, 0, qbases, qgw, qln, 0, stage=O.STAGE_FILTERED)
+    before = engine.stats()["hits"]
+    ix = engine.hash_table(s, tl, 0, len(tl.lengths))
+    engine.hit_list(s, ix, ql, 0, len(ql.lengths) // 2)
+    ix.close()
+    got = engine.stats()["hits"] - before
+    assert len(want["t_id"]) > 100
+    assert got == len(want["t_id"])
