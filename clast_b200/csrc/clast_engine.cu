@@ -390,15 +390,19 @@ int64_t search_seeded(clast_ctx* c, Workspace& ws, const clast_params* p, const 
   uint64_t* skey = z.skey;
   uint32_t* sq = z.sq;
   const long long* warp_dev = nullptr;  // the DP's split, when it was made on the device
+  const int* bad_dev = nullptr;         // the DP's flag of hits outside the window, once it ran
   auto add_counters = [&]() {
     unsigned long long cells = 0;
     long long warp = 0;
+    int bad = 0;
     CLAST_CK(cudaMemcpyAsync(&cells, counters + 1, sizeof(cells), cudaMemcpyDeviceToHost, st));
     if (warp_dev) CLAST_CK(cudaMemcpyAsync(&warp, warp_dev, sizeof(warp), cudaMemcpyDeviceToHost, st));
+    if (bad_dev) CLAST_CK(cudaMemcpyAsync(&bad, bad_dev, sizeof(bad), cudaMemcpyDeviceToHost, st));
     CLAST_CK(cudaStreamSynchronize(st));
     c->stats.dp_cells += (int64_t)cells;
     c->stats.dp_warp_hits += warp;
     tm.flush();
+    if (bad) throw std::runtime_error("internal: a hit named a target sequence or strand outside the window");
   };
   c->stats.seeds += S;
   if (S == 0) {
@@ -469,6 +473,8 @@ int64_t search_seeded(clast_ctx* c, Workspace& ws, const clast_params* p, const 
   };
   unsigned long long* dp_head = ws.get<unsigned long long>("dp_head", 1);
   long long* dp_warp_n = ws.get<long long>("dp_warp_n", 1);
+  int* dp_bad = ws.get<int>("dp_bad", 1);
+  CLAST_CK(cudaMemsetAsync(dp_bad, 0, sizeof(int), st));
   auto launch_of = [&](const DpChoice& ch) {
     DpLaunch m;
     if (ch.queue) {
@@ -481,6 +487,7 @@ int64_t search_seeded(clast_ctx* c, Workspace& ws, const clast_params* p, const 
     m.aux = c->st_dp;
     m.ev_fork = c->ev_dp_fork;
     m.ev_join = c->ev_dp_join;
+    m.bad = dp_bad;
     if (!uneven) m.uniform_rows = std::max(0, qb.max_len - p->lmer);
     return m;
   };
@@ -521,6 +528,7 @@ int64_t search_seeded(clast_ctx* c, Workspace& ws, const clast_params* p, const 
   tm.end(StageTimer::DP, st);
   if (warp_fixed >= 0) c->stats.dp_warp_hits += warp_fixed;
   else warp_dev = dl.warp_n;
+  bad_dev = dp_bad;
   // resultSorting + deleteHits_duplicateResult, per read
   uint64_t* k1 = ws.get<uint64_t>("f_k1", H);
   uint64_t* k2 = ws.get<uint64_t>("f_k2", H);

@@ -2281,7 +2281,15 @@ struct DpKernelArgs {
   // the others one per thread: n_warp = *warp_n when given, else warp_fixed
   const long long* warp_n;
   long long warp_fixed;
+  int* bad;  // see DpLaunch::bad
 };
+
+// A hit whose target sequence or strand lies outside the window cannot come
+// from the seeding stages; it is flagged and given empty outputs instead of
+// being read past the window.
+__device__ __forceinline__ bool dp_hit_outside(const DpKernelArgs& a, int tid, int s) {
+  return (unsigned)tid >= (unsigned)a.t.nseqs || (unsigned)s >= (unsigned)a.q.nstrands;
+}
 
 __device__ __forceinline__ int64_t dp_warp_hits(const DpKernelArgs& a) {
   const int64_t w = a.warp_n ? (int64_t)*a.warp_n : (int64_t)a.warp_fixed;
@@ -2314,6 +2322,13 @@ __device__ __forceinline__ void dp_store(const DpKernelArgs& a, int64_t h, int q
   a.o.keep[h] = keep ? 1 : 0;
 }
 
+__device__ __forceinline__ void dp_skip(const DpKernelArgs& a, int64_t h) {
+  a.o.t_idx[h] = a.o.q_idx[h] = a.o.t_len[h] = a.o.q_len[h] = a.o.match[h] = a.o.score[h] = 0;
+  a.o.evalue[h] = 0.0;
+  a.o.keep[h] = 0;
+  if (a.bad) atomicExch(a.bad, 1);
+}
+
 // Extension of the hit at position i of the order (alignmentHits +
 // calculateEvalue + the two hit filters of deleteBadHits).
 template <int GAP, bool LOCAL>
@@ -2323,6 +2338,10 @@ __device__ __forceinline__ void dp_one(const DpKernelArgs& a, const int2* tab, i
   const int qidx = a.hq[h];
   const int s = a.hs[h];
   const int tid = (int)(k >> 32);
+  if (dp_hit_outside(a, tid, s)) {
+    dp_skip(a, h);
+    return;
+  }
   const int tidx = (int)((uint32_t)k ^ 0x80000000u) + qidx;
   const int64_t tstart = a.t.gateway[tid];
   const int tlen = a.t.lengths[tid];
@@ -2387,6 +2406,10 @@ __global__ void __launch_bounds__(128) k_banded_dp_warp(DpKernelArgs a) {
     const int qidx = a.hq[h];
     const int s = a.hs[h];
     const int tid = (int)(k >> 32);
+    if (dp_hit_outside(a, tid, s)) {  // the same for every lane of the warp
+      if (lane == 0) dp_skip(a, h);
+      continue;
+    }
     const int tidx = (int)((uint32_t)k ^ 0x80000000u) + qidx;
     const int64_t tstart = a.t.gateway[tid];
     const int tlen = a.t.lengths[tid];
@@ -3063,7 +3086,7 @@ long long banded_dp(const TargetView& t, const QueryView& q, const uint64_t* hk,
                     const int32_t* hs, const uint64_t* order, int64_t n_hits, const DpParams& p, const DpOut& o,
                     cudaStream_t st, const DpLaunch& m) {
   if (n_hits <= 0) return 0;
-  DpKernelArgs a{t, q, hk, hq, hs, order, n_hits, p, o, nullptr, 0};
+  DpKernelArgs a{t, q, hk, hq, hs, order, n_hits, p, o, nullptr, 0, m.bad};
   const bool local = p.local != 0;
   switch (p.gap) {
     case 2: return launch_dp_gap<2>(a, local, m, st);

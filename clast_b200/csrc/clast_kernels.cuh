@@ -162,6 +162,9 @@ struct DpLaunch {
   // from and joined back into the launch stream by the two events)
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // device word set to 1 when a hit names a target sequence or strand outside
+  // the window (an internal error: the hit is skipped, never read past)
+  int* bad = nullptr;
 };
 // order (may be null): the hits in the order the threads take them, as words
 // whose low 32 bits are hit indices; outputs stay at the hit's own index.
